@@ -1,0 +1,352 @@
+"""Benchmark of the n=75 population search hot path on B200.
+
+One step = one cross-checked scoring pass over the n=75 population: 4096
+seeded two-per-row/column states (150 int16 points each, 551,300 triple tests
+per state), exact determinant count + independent gcd-normalised slope count
++ badness + on-device mismatch check, in one launch of n3_score_checked.
+``value`` is states scored per second over all ranks with the population
+resident in HBM; ``e2e`` is the same metric through the C ABI with host
+buffers (pinned H2D of the step's columns, D2H of its scores and flags).
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference]
+
+Under torchrun each rank scores its own population (weak scaling, no
+data-path collective); the step time is the max over ranks.
+``--impl reference`` times the reference's CPU algorithm (the C restatement
+in oracle/, all host threads) on the same workload and metric.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import shutil
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+METRIC = "n=75 states scored/s & swap deltas/s; time-to-E≤12, learned vs plain proposal"
+UNIT = "states/s"
+N = 75
+STATES = 4096
+TESTS_PER_STATE = math.comb(2 * N, 3)  # 551,300
+OPS_PER_TEST = 4                       # multiply, multiply-add, compare, count
+L2_FLUSH_BYTES = 256 << 20             # > 126 MB L2
+WORKLOAD = "n=75 population scoring, 4096 states, determinant + slope cross-check + badness"
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=200)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", choices=["b200", "reference"], default="b200")
+    ap.add_argument("--states", type=int, default=STATES)
+    ap.add_argument("--mode", choices=["checked", "det", "slope"], default="checked",
+                    help="kernel a step runs: fused checked scoring (default), determinant only, slope only")
+    return ap.parse_args()
+
+
+def dist_env():
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return rank, world, local
+
+
+def population(n: int, count: int, rank: int):
+    from no_three_in_line_b200 import state
+
+    p, q = state.seeded_population(n, count, base_seed=91001 + rank * count)
+    return p, q, state.pq_to_columns(p, q)
+
+
+class ClockSampler:
+    """nvidia-smi clocks / throttle reasons sampled during the timed region."""
+
+    QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index: int):
+        self.index = index
+        self.proc = None
+        self.path = None
+
+    def __enter__(self):
+        if shutil.which("nvidia-smi"):
+            fd, self.path = tempfile.mkstemp(suffix=".csv")
+            os.close(fd)
+            self.out = open(self.path, "w")
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.index), f"--query-gpu={self.QUERY}",
+                                          "--format=csv,noheader,nounits", "-lms", "50"],
+                                         stdout=self.out, stderr=subprocess.DEVNULL)
+            time.sleep(0.15)
+        return self
+
+    def __exit__(self, *exc):
+        if self.proc is not None:
+            time.sleep(0.06)
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+            self.out.close()
+
+    def summary(self):
+        if not self.path or not os.path.exists(self.path):
+            return None
+        rows = [r.split(",") for r in Path(self.path).read_text().strip().splitlines() if r.strip()]
+        os.unlink(self.path)
+        sm, mx, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for r in rows:
+            if len(r) < 9:
+                continue
+            try:
+                sm.append(float(r[1]))
+                mx.append(float(r[2]))
+            except ValueError:
+                continue
+            for name, flag in zip(names, r[5:9]):
+                if flag.strip().lower() == "active":
+                    reasons.add(name)
+        if not sm:
+            return None
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": max(mx), "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def measured_peaks():
+    p = ROOT / "MEASURED_PEAKS.json"
+    if p.exists():
+        return json.loads(p.read_text()), "measured"
+    return {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0}, "fallback"
+
+
+def cpu_baseline(p, q, threads: int):
+    """The reference's CPU scoring algorithm (accelerated.py:14-37, restated in
+    oracle/) over the same states on all host threads."""
+    from oracle import oracle
+
+    oracle.score_population(p[:8], q[:8], threads=1)  # load
+    sample = min(len(p), 4096)
+    t0 = time.perf_counter()
+    oracle.score_population(p[:sample], q[:sample], badness=True, threads=threads)
+    dt = time.perf_counter() - t0
+    return {"value": sample / dt, "unit": UNIT, "cores": threads, "kind": "port",
+            "sample": f"{sample} n=75 states, determinant count + badness (accelerated.py:14-37 restated in C), "
+                      f"{threads} threads, {dt:.2f} s"}
+
+
+def run_reference(args):
+    """CPU arm: the reference algorithm (oracle port) on all host threads."""
+    rank, world, _ = dist_env()
+    if rank != 0:
+        return 0
+    from oracle import oracle
+
+    threads = oracle.max_threads()
+    p, q, _ = population(N, args.states, 0)
+    oracle.score_population(p[:8], q[:8], threads=1)
+    # bounded sample per step: ~0.5 s of wall time at this host's thread count
+    t0 = time.perf_counter()
+    oracle.score_population(p[:64], q[:64], badness=True, threads=threads)
+    per_state = (time.perf_counter() - t0) / 64
+    sample = int(max(threads, min(args.states, 0.5 / max(per_state, 1e-9))))
+    for _ in range(args.warmup):
+        oracle.score_population(p[:sample], q[:sample], badness=True, threads=threads)
+    times = []
+    for k in range(args.steps):
+        lo = (k * sample) % max(1, args.states - sample + 1)
+        t0 = time.perf_counter()
+        oracle.score_population(p[lo:lo + sample], q[lo:lo + sample], badness=True, threads=threads)
+        times.append(time.perf_counter() - t0)
+    total = sum(times)
+    value = sample * args.steps / total
+    line = {"metric": METRIC, "value": value, "unit": UNIT, "impl": "reference", "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * total / args.steps,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "int32",
+            "data": "synthetic: random_state(75, Random(91001+i)) states",
+            "config": {"workload": WORKLOAD, "n": N, "states": args.states, "sample_states_per_step": sample},
+            "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "port",
+                             "sample": f"{sample} states per step, determinant count + badness "
+                                       f"(accelerated.py:14-37 restated in C), {threads} threads"},
+            "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def run_b200(args):
+    import torch
+    import torch.distributed as dist
+
+    from no_three_in_line_b200 import _lib
+
+    rank, world, local = dist_env()
+    if world > 1:
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", init_method="env://", timeout=__import__("datetime").timedelta(seconds=120))
+    dev = torch.device("cuda", torch.cuda.current_device())
+    L = _lib.lib()
+    _lib.require_device()
+    B = args.states
+    p, q, cols_host = population(N, B, rank)
+    cols = torch.from_numpy(cols_host).to(dev)
+    scores = torch.empty(B, dtype=torch.int32, device=dev)
+    badness = torch.empty((B, 2 * N), dtype=torch.int32, device=dev)
+    flags = torch.zeros(2, dtype=torch.int32, device=dev)
+    flush = torch.empty(L2_FLUSH_BYTES // 4, dtype=torch.int32, device=dev)
+    stream = torch.cuda.current_stream()
+    sptr = int(stream.cuda_stream)
+
+    def step():
+        if args.mode == "det":
+            _lib.check(L.n3_score_columns(cols.data_ptr(), B, N, scores.data_ptr(), None, sptr), "n3_score_columns")
+        elif args.mode == "slope":
+            _lib.check(L.n3_score_slope(cols.data_ptr(), B, N, scores.data_ptr(), badness.data_ptr(), sptr),
+                       "n3_score_slope")
+        else:
+            _lib.check(L.n3_score_checked(cols.data_ptr(), B, N, scores.data_ptr(), badness.data_ptr(),
+                                          flags.data_ptr(), flags.data_ptr() + 4, sptr), "n3_score_checked")
+
+    for _ in range(max(args.warmup, 3)):
+        step()
+    torch.cuda.synchronize()
+    # correctness gate before timing: bit-exact against the oracle on a sample
+    from oracle import oracle
+
+    ref = oracle.score_population(p[:64], q[:64], threads=0)
+    got = scores[:64].cpu().numpy()
+    if not np.array_equal(ref, got) or int(flags[0].item()) != 0:
+        raise AssertionError("scores differ from the oracle; refusing to time")
+
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize()
+    with ClockSampler(dev.index) as clocks:
+        wall0 = time.perf_counter()
+        for k in range(args.steps):
+            flush.fill_(k)  # evict the population from L2 between steps
+            ev[k][0].record(stream)
+            step()
+            ev[k][1].record(stream)
+        torch.cuda.synchronize()
+        wall = time.perf_counter() - wall0
+    if world > 1:
+        dist.barrier()
+    step_ms = [a.elapsed_time(b) for a, b in ev]
+    local_total = sum(step_ms)
+    t_total = torch.tensor([local_total], dtype=torch.float64, device=dev)
+    if world > 1:
+        dist.all_reduce(t_total, op=dist.ReduceOp.MAX)
+    total_ms = float(t_total.item())
+    if int(flags[0].item()) != 0:
+        raise AssertionError("device cross-check reported a mismatch during timing")
+    value = world * B * args.steps / (total_ms / 1e3)
+
+    # end to end through the C ABI with host buffers
+    h_cols = torch.from_numpy(cols_host).pin_memory()
+    h_scores = torch.empty(B, dtype=torch.int32).pin_memory()
+    h_flags = torch.empty(2, dtype=torch.int32).pin_memory()
+    d_cols = torch.empty_like(cols)
+    e2e_steps = max(3, min(args.steps, 100))
+    for _ in range(2):
+        d_cols.copy_(h_cols, non_blocking=True)
+        step()
+    torch.cuda.synchronize()
+    e_start, e_end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e_start.record(stream)
+    for _ in range(e2e_steps):
+        d_cols.copy_(h_cols, non_blocking=True)
+        _lib.check(L.n3_score_checked(d_cols.data_ptr(), B, N, scores.data_ptr(), badness.data_ptr(),
+                                      flags.data_ptr(), flags.data_ptr() + 4, sptr), "n3_score_checked")
+        h_scores.copy_(scores, non_blocking=True)
+        h_flags.copy_(flags, non_blocking=True)
+    e_end.record(stream)
+    torch.cuda.synchronize()
+    e2e_ms = e_start.elapsed_time(e_end) / e2e_steps
+    t_e2e = torch.tensor([e2e_ms], dtype=torch.float64, device=dev)
+    if world > 1:
+        dist.all_reduce(t_e2e, op=dist.ReduceOp.MAX)
+    e2e_ms = float(t_e2e.item())
+
+    # integer-pipe ceiling of the same test expression
+    scratch = torch.zeros(2, dtype=torch.int64, device=dev)
+    sms = torch.cuda.get_device_properties(dev).multi_processor_count
+    blocks, iters = sms * 8, 4096
+    _lib.check(L.n3_calibrate_det_ceiling(blocks, iters, scratch.data_ptr(), sptr), "calibrate")
+    c0, c1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    c0.record(stream)
+    for _ in range(5):
+        _lib.check(L.n3_calibrate_det_ceiling(blocks, iters, scratch.data_ptr(), sptr), "calibrate")
+    c1.record(stream)
+    torch.cuda.synchronize()
+    ceiling_tests = blocks * 256 * iters * 16 * 5 / (c0.elapsed_time(c1) / 1e3)
+
+    line = None
+    if rank == 0:
+        ms_per_step = total_ms / args.steps
+        tests_per_s = value * TESTS_PER_STATE
+        achieved = tests_per_s / world * OPS_PER_TEST / 1e9
+        peak = ceiling_tests * OPS_PER_TEST / 1e9
+        peaks, peak_kind = measured_peaks()
+        line = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "int32",
+            "data": "synthetic: random_state(75, Random(91001+i)) states (the reference's seeding), resident in HBM",
+            "config": {"workload": WORKLOAD if args.mode == "checked" else f"{WORKLOAD} ({args.mode} kernel only)",
+                       "n": N, "states_per_gpu": B, "slots": 2 * N,
+                       "triple_tests_per_state": TESTS_PER_STATE, "parallelism": f"shard{world}",
+                       "l2": "256 MiB buffer written between steps, outside the per-step CUDA events"},
+            "triple_tests_per_s": tests_per_s,
+            "e2e": {"value": world * B / (e2e_ms / 1e3), "unit": UNIT,
+                    "h2d_bytes_per_step": int(cols_host.nbytes),
+                    "d2h_bytes_per_step": int(h_scores.numel() * 4 + h_flags.numel() * 4)},
+            "gpu_launches": args.steps,
+            "roofline": {"bound": "int32-alu",
+                         "kernel": {"checked": "n3::slope_kernel<1> (determinant + slope, checked)",
+                                    "det": "n3::det_kernel<ColSource,false>",
+                                    "slope": "n3::slope_kernel<0>"}[args.mode],
+                         "achieved": achieved, "peak": peak, "unit": "Gop/s", "frac": achieved / peak,
+                         "peak_source": "measured on this GPU: n3_calibrate_det_ceiling, the scorer's own "
+                                        "test expression on registers (4 int32 ops per triple test)",
+                         "traffic": None,
+                         "hbm_context": {"bytes_per_step": int(cols_host.nbytes + B * 4 + B * 2 * N * 4),
+                                         "hbm_gbs_peak": peaks.get("hbm_gbs"), "peak_kind": peak_kind}},
+            "wall_s_timed": wall,
+            "clocks": clocks.summary(),
+        }
+        line["cpu_baseline"] = cpu_baseline(p, q, threads=os.cpu_count() or 1)
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+    if line is not None:
+        print(json.dumps(line), flush=True)
+    return 0
+
+
+def main():
+    args = parse()
+    from __graft_entry__ import load_package
+
+    load_package()
+    if args.impl == "reference":
+        return run_reference(args)
+    return run_b200(args)
+
+
+if __name__ == "__main__":
+    raise SystemExit(main())

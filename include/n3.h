@@ -1,0 +1,142 @@
+/*
+ * n3: B200-native (sm_100a) engine for the no-three-in-line population search.
+ *
+ * Flat C ABI of libn3.so.  Every entry point takes device pointers (caller
+ * owned), plain sizes and a CUDA stream (cudaStream_t passed as void*; NULL is
+ * the legacy default stream), enqueues its work on that stream and returns an
+ * int status: N3_OK (0) or one of the N3_ERR_* codes below.  The message of
+ * the last failure on the calling host thread is returned by n3_last_error().
+ * Calls that report device-side findings (mismatch counts, error words) write
+ * them to device memory; read them after synchronising the stream.
+ *
+ * State layout: the reference's interleaved slot layout
+ * (src/no_three_75/accelerated.py:18-24, src/no_three_75/tempering.py:38).
+ * A state of an n x n grid has m = 2n slots; slot s = 2*row + layer lies in row
+ * s >> 1 and its column is cols[s].  P/Q arrays ([B][n] int32, the layout of
+ * src/no_three_75/gpu.py:69-77) are accepted where the reference used them.
+ * Columns must lie in [0, n); 2 <= n <= N3_MAX_N.
+ *
+ * Energies are exact integers everywhere: E = number of collinear triples.
+ */
+#ifndef N3_H_
+#define N3_H_
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define N3_MAX_N 75
+#define N3_SENTINEL (1 << 30) /* illegal move marker, src/no_three_75/gpu_delta.py:35 */
+
+enum {
+  N3_OK = 0,
+  N3_ERR_ARG = 1,      /* null pointer, bad size or shape (reference: ValueError) */
+  N3_ERR_RANGE = 2,    /* n outside [2, N3_MAX_N] or an index out of range */
+  N3_ERR_CUDA = 3,     /* CUDA runtime failure or no device (reference: RuntimeError) */
+  N3_ERR_MISMATCH = 4, /* incremental / cross-checked count differs (reference: AssertionError) */
+  N3_ERR_TIMEOUT = 5,  /* a bounded device wait expired */
+  N3_ERR_STATE = 6     /* the state is not a legal two-per-row/column state */
+};
+
+/* Library version (major*10000 + minor*100 + patch). */
+int n3_version(void);
+
+/* Message of the last failing call on this host thread ("" if none). */
+const char* n3_last_error(void);
+
+/* ---------------------------------------------------------------------------
+ * (a) Population scoring.
+ * ------------------------------------------------------------------------- */
+
+/* Exact collinear-triple count of B states given as P/Q, one warp per state,
+ * int32 cross-product determinants.  Replaces the reference kernel
+ * score_population (src/no_three_75/gpu.py:13-42, launched at gpu.py:76) and,
+ * with badness != NULL, score_population_badness
+ * (src/no_three_75/gpu_device_search.py:118-161): badness[b][s] is the number
+ * of collinear triples containing slot s.
+ *   p, q     int32 [B][n]      scores int32 [B]      badness int32 [B][2n] or NULL */
+int n3_score_population(const int32_t* p, const int32_t* q, int B, int n, int32_t* scores,
+                        int32_t* badness, void* stream);
+
+/* Same count over slot-layout columns (int16 [B][2n]). */
+int n3_score_columns(const int16_t* cols, int B, int n, int32_t* scores, int32_t* badness,
+                     void* stream);
+
+/* Independent normalised-slope line count: for each anchor the other points
+ * are grouped by gcd-reduced undirected direction (src/no_three_75/verifier_b.py:8-19);
+ * badness[s] = sum over directions of C(c,2) (src/no_three_75/conflicts.py:376-378)
+ * and E = sum(badness)/3 = sum over lines of C(k,3) (conflicts.py:373).
+ *   cols int16 [B][2n]     scores int32 [B]     badness int32 [B][2n] or NULL */
+int n3_score_slope(const int16_t* cols, int B, int n, int32_t* scores, int32_t* badness,
+                   void* stream);
+
+/* Fused, cross-checked scoring: determinant count and slope count per state,
+ * plus the column-range / duplicate-point checks.  scores = determinant E,
+ * badness = slope badness; *mismatch (device int32, accumulated, caller
+ * zeroes it) counts states whose two counts differ or whose badness does not
+ * sum to 3E; *error_word (device uint32, OR-ed, caller zeroes it, may be NULL)
+ * collects the device error bits (1: column range, 2: duplicate point,
+ * 4: mismatch).  The reference runs this audit on the host
+ * (src/no_three_75/gpu.py:131 exact_match, src/no_three_75/tempering.py:193-204). */
+int n3_score_checked(const int16_t* cols, int B, int n, int32_t* scores, int32_t* badness,
+                     int32_t* mismatch, uint32_t* error_word, void* stream);
+
+/* ---------------------------------------------------------------------------
+ * (b) Exact incremental swap deltas.
+ *
+ * A move (state, u, v) exchanges the columns of slots u and v (different
+ * rows); it is legal iff the columns differ and neither new point duplicates
+ * the other point of its row (src/no_three_75/tempering.py:58).  Illegal moves
+ * and out-of-range indices give N3_SENTINEL.
+ * ------------------------------------------------------------------------- */
+
+/* Exact dE of each move, counted through the moved points only (direction
+ * classes around u, v and their new positions); bit-exact against a full
+ * recompute.  Replaces the per-proposal delta of the reference walk kernel
+ * (src/no_three_75/tempering.py:68-89) for batches of moves.
+ *   cols int16 [B][2n]   moves int32 [M][3] (state, u, v)   dE int32 [M]
+ *   dbad int32 [M][2n] or NULL: change of every slot's badness (slot u / v
+ *   refer to the moved points' new positions). */
+int n3_swap_delta(const int16_t* cols, int B, int n, const int32_t* moves, int M, int32_t* dE,
+                  int32_t* dbad, void* stream);
+
+/* Same result by the reference's literal formulation (tempering.py:68-89:
+ * every pair outside {u,v} tested against u, u', v, v', every k against
+ * (u,v) and (u',v')); an independent device cross-check of n3_swap_delta. */
+int n3_swap_delta_pairs(const int16_t* cols, int B, int n, const int32_t* moves, int M,
+                        int32_t* dE, int32_t* dbad, void* stream);
+
+/* Full score after exchanging anchor slot u with every partner slot v, for A
+ * anchors (state, u): out[a][v] = current[state] - (bad[u] + bad[v] - joint)
+ * + new_affected, N3_SENTINEL where illegal.  Replaces the reference plugin
+ * kernel two_switch_scores (src/no_three_75/gpu_delta.py:19-75, one anchor per
+ * launch at gpu_delta.py:103-115) and accelerated.evaluate_two_switches
+ * (src/no_three_75/accelerated.py:122-195).
+ *   badness int32 [B][2n]   current int32 [B]   anchors int32 [A][2]   out int32 [A][2n] */
+int n3_two_switch_scores(const int16_t* cols, const int32_t* badness, const int32_t* current,
+                         int B, int n, const int32_t* anchors, int A, int32_t* out, void* stream);
+
+/* Same-layer row transpositions of anchor slot u = 2*row + layer with every
+ * partner row: out[a][row'] (int32 [A][n]), N3_SENTINEL where illegal or
+ * row' == row.  Replaces accelerated.evaluate_transpositions
+ * (src/no_three_75/accelerated.py:40-119). */
+int n3_transposition_scores(const int16_t* cols, const int32_t* badness, const int32_t* current,
+                            int B, int n, const int32_t* anchors, int A, int32_t* out, void* stream);
+
+/* ---------------------------------------------------------------------------
+ * Measurement helper (no reference counterpart).
+ * ------------------------------------------------------------------------- */
+
+/* Runs the scorer's determinant test expression on register operands only
+ * (no memory traffic): blocks x 256 threads x iters x 16 triple tests.  Its
+ * event-timed rate is the integer-pipe ceiling that bench.py reports the
+ * scorer's rate against.  scratch2: device uint64[2]. */
+int n3_calibrate_det_ceiling(int blocks, int iters, unsigned long long* scratch2, void* stream);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* N3_H_ */

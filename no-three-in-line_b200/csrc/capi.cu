@@ -1,0 +1,81 @@
+// Error reporting, per-device one-time set-up and small C-ABI utilities.
+#include <cstdarg>
+#include <cstdio>
+#include <mutex>
+#include <string>
+
+#include "n3_common.cuh"
+
+namespace n3host {
+
+static thread_local std::string g_last_error;
+
+int set_error(int code, const char* fmt, ...) {
+  char buf[512];
+  va_list ap;
+  va_start(ap, fmt);
+  vsnprintf(buf, sizeof(buf), fmt, ap);
+  va_end(ap);
+  g_last_error = buf;
+  return code;
+}
+
+int check_launch(const char* what) {
+  const cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return set_error(N3_ERR_CUDA, "%s: %s", what, cudaGetErrorString(e));
+  return N3_OK;
+}
+
+int build_dir_lut(cudaStream_t st);  // score.cu
+
+static std::mutex g_init_mutex;
+static bool g_tables_ready[64];
+static int g_sm_count[64];
+
+static int current_device(int* dev) {
+  const cudaError_t e = cudaGetDevice(dev);
+  if (e != cudaSuccess) return set_error(N3_ERR_CUDA, "cudaGetDevice: %s", cudaGetErrorString(e));
+  if (*dev < 0 || *dev >= 64) return set_error(N3_ERR_CUDA, "device ordinal %d unsupported", *dev);
+  return N3_OK;
+}
+
+// One-time, per-device construction of the device-resident lookup tables
+// (the gcd-reduced direction table used by the slope kernels).  Runs on a
+// private stream and waits for it, so the first call on a device must not be
+// made while a stream is being captured into a CUDA graph.
+int ensure_device_tables() {
+  int dev = 0;
+  N3_TRY(current_device(&dev));
+  std::lock_guard<std::mutex> lock(g_init_mutex);
+  if (g_tables_ready[dev]) return N3_OK;
+  cudaStream_t st;
+  if (cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking) != cudaSuccess) return check_launch("cudaStreamCreate");
+  int rc = build_dir_lut(st);
+  const cudaError_t e = cudaStreamSynchronize(st);
+  cudaStreamDestroy(st);
+  if (rc != N3_OK) return rc;
+  if (e != cudaSuccess) return set_error(N3_ERR_CUDA, "table set-up: %s", cudaGetErrorString(e));
+  g_tables_ready[dev] = true;
+  return N3_OK;
+}
+
+int sm_count() {
+  int dev = 0;
+  if (current_device(&dev) != N3_OK) return 148;
+  if (g_sm_count[dev] == 0) {
+    int v = 0;
+    if (cudaDeviceGetAttribute(&v, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || v <= 0) v = 148;
+    g_sm_count[dev] = v;
+  }
+  return g_sm_count[dev];
+}
+
+}  // namespace n3host
+
+extern "C" {
+
+int n3_version(void) { return 100; }
+
+const char* n3_last_error(void) { return n3host::g_last_error.c_str(); }
+
+}  // extern "C"

@@ -1,0 +1,404 @@
+// (a) Population scoring: exact collinear-triple counts, one warp per state.
+//
+// Two independent kernels and a fused, cross-checked one:
+//
+// * Determinant count (replaces src/no_three_75/gpu.py:13-42 and
+//   src/no_three_75/gpu_device_search.py:118-161).  Every triple i<j<k is
+//   tested once with an exact int32 cross product, at its middle slot j.  The
+//   two slots of j's row are pivots together; the triple's other two points
+//   lie in rows above and below that row.  The larger side sits in lane
+//   registers, the smaller side is broadcast from shared memory one row (two
+//   slots) at a time, so one pair of products serves four tests.  Triples
+//   holding j's row partner are skipped: two points of a row and a third point
+//   in another row are never collinear.
+//
+// * Normalised-slope line count (the counting form of
+//   src/no_three_75/verifier_b.py:8-33).  For every anchor a, the other points
+//   are binned by gcd-reduced undirected direction in an 8-bit shared-memory
+//   histogram; sum over bins of C(c,2) is the anchor's badness and
+//   E = sum(badness) / 3 (a line of k points gives each member C(k-1,2) pairs,
+//   src/no_three_75/conflicts.py:373-378).  The gcd reduction is tabulated once
+//   per device by build_dir_lut_kernel.
+//
+// * Checked scoring runs both per state and flags disagreement on device.
+#include <cstdio>
+
+#include "dirs.cuh"
+#include "n3_common.cuh"
+
+namespace n3 {
+
+__device__ uint16_t g_dir_lut[kLutSize];
+__device__ int g_dir_count;
+
+__device__ __forceinline__ int gcd_dev(int a, int b) {
+  a = a < 0 ? -a : a;
+  b = b < 0 ? -b : b;
+  while (b) {
+    const int t = a % b;
+    a = b;
+    b = t;
+  }
+  return a;
+}
+
+// Entry e = p * kLutW + (q + kMaxN - 1) names a primitive direction iff
+// gcd(p, |q|) == 1 with p > 0, or (p, q) == (0, 1).
+__device__ __forceinline__ bool is_primitive(int e) {
+  const int p = e / kLutW, q = e % kLutW - (kMaxN - 1);
+  return p == 0 ? q == 1 : gcd_dev(p, q) == 1;
+}
+
+// One block: numbers the primitive directions in (p, q) order, then maps every
+// difference vector to the id of its gcd-reduced direction.
+__global__ void __launch_bounds__(1024) build_dir_lut_kernel() {
+  __shared__ uint16_t prim[kLutSize];
+  __shared__ int scan[1024];
+  const int tid = threadIdx.x;
+  constexpr int per = (kLutSize + 1023) / 1024;
+  const int lo = tid * per, hi = min(lo + per, kLutSize);
+  int c = 0;
+  for (int e = lo; e < hi; ++e) c += is_primitive(e);
+  scan[tid] = c;
+  __syncthreads();
+  for (int off = 1; off < 1024; off <<= 1) {  // inclusive Hillis-Steele scan
+    const int v = tid >= off ? scan[tid - off] : 0;
+    __syncthreads();
+    scan[tid] += v;
+    __syncthreads();
+  }
+  int id = scan[tid] - c;
+  for (int e = lo; e < hi; ++e) prim[e] = is_primitive(e) ? (uint16_t)id++ : (uint16_t)0xFFFFu;
+  if (tid == 1023) g_dir_count = scan[1023];
+  __syncthreads();
+  for (int e = tid; e < kLutSize; e += 1024) {
+    const int dx = e / kLutW, dy = e % kLutW - (kMaxN - 1);
+    const int g = gcd_dev(dx, dy);
+    uint16_t v = 0xFFFFu;  // (0, 0) has no direction
+    if (g) {
+      const int p = dx / g;
+      const int q = p == 0 ? 1 : dy / g;  // (0, -1) ~ (0, 1)
+      v = prim[p * kLutW + q + (kMaxN - 1)];
+    }
+    g_dir_lut[e] = v;
+  }
+}
+
+struct PQSource {
+  const int32_t* p;
+  const int32_t* q;
+  __device__ __forceinline__ int col(int b, int n, int s) const {
+    const size_t base = (size_t)b * n + (s >> 1);
+    return (s & 1) ? q[base] : p[base];
+  }
+};
+
+struct ColSource {
+  const int16_t* c;
+  __device__ __forceinline__ int col(int b, int n, int s) const { return c[(size_t)b * 2 * n + s]; }
+};
+
+// Tests of the two pivots of row `rho` against all pairs (x, y) with x on the
+// larger side (R register slots per lane) and y on the smaller side.
+// X=(r_x,c_x), J=(rho,c_j), Y=(r_y,c_y) are collinear iff
+//   (r_x-rho)(c_y-c_j) == (c_x-c_j)(r_y-rho)
+//   <=>  a_x*c_y == a_y*b_x + a_x*c_j,   a = r - rho, b_x = c_x - c_j.
+template <int R, bool BAD>
+__device__ __forceinline__ int det_pivot_row(const int* __restrict__ cs, int n, int rho, int lane, int* bad) {
+  const int cj0 = cs[2 * rho], cj1 = cs[2 * rho + 1];
+  const int above = rho, below = n - 1 - rho;
+  const bool lanes_above = above >= below;
+  const int L = 2 * (lanes_above ? above : below);
+  const int lbase = lanes_above ? 0 : 2 * rho + 2;
+  const int rb0 = lanes_above ? rho + 1 : 0;
+  const int rb1 = lanes_above ? n : rho;
+  int ax[R], bx0[R], bx1[R], k0[R], k1[R], sx[R];
+#pragma unroll
+  for (int r = 0; r < R; ++r) {
+    const int x = lane + 32 * r;
+    if (x < L) {
+      const int s = lbase + x;
+      const int a = (s >> 1) - rho, c = cs[s];
+      ax[r] = a;
+      bx0[r] = c - cj0;
+      bx1[r] = c - cj1;
+      k0[r] = a * cj0;
+      k1[r] = a * cj1;
+      sx[r] = s;
+    } else {  // idle slot: products are 0, targets -1, never a hit
+      ax[r] = 0;
+      bx0[r] = 0;
+      bx1[r] = 0;
+      k0[r] = -1;
+      k1[r] = -1;
+      sx[r] = 0;
+    }
+  }
+  int cnt = 0;
+  const int2* rows2 = reinterpret_cast<const int2*>(cs);
+#pragma unroll 2
+  for (int row = rb0; row < rb1; ++row) {
+    const int2 cy = rows2[row];
+    const int ay = row - rho;
+#pragma unroll
+    for (int r = 0; r < R; ++r) {
+      const int P0 = ax[r] * cy.x, P1 = ax[r] * cy.y;
+      const int T0 = ay * bx0[r] + k0[r], T1 = ay * bx1[r] + k1[r];
+      const int h00 = P0 == T0, h10 = P1 == T0, h01 = P0 == T1, h11 = P1 == T1;
+      cnt += (h00 + h10) + (h01 + h11);
+      if (BAD) {
+        if (h00 | h10 | h01 | h11) {
+          const int hits[4] = {h00, h10, h01, h11};
+#pragma unroll
+          for (int t = 0; t < 4; ++t) {
+            if (hits[t]) {
+              atomicAdd(bad + sx[r], 1);
+              atomicAdd(bad + 2 * rho + (t >> 1), 1);
+              atomicAdd(bad + 2 * row + (t & 1), 1);
+            }
+          }
+        }
+      }
+    }
+  }
+  return cnt;
+}
+
+template <bool BAD>
+__device__ int det_state(const int* __restrict__ cs, int n, int lane, int* bad) {
+  int cnt = 0;
+  for (int rho = 1; rho < n - 1; ++rho) {
+    const int L = 2 * max(rho, n - 1 - rho);
+    switch ((L + 31) >> 5) {
+      case 1: cnt += det_pivot_row<1, BAD>(cs, n, rho, lane, bad); break;
+      case 2: cnt += det_pivot_row<2, BAD>(cs, n, rho, lane, bad); break;
+      case 3: cnt += det_pivot_row<3, BAD>(cs, n, rho, lane, bad); break;
+      case 4: cnt += det_pivot_row<4, BAD>(cs, n, rho, lane, bad); break;
+      default: cnt += det_pivot_row<5, BAD>(cs, n, rho, lane, bad); break;
+    }
+  }
+  return cnt;
+}
+
+constexpr int kDetWarps = 8;
+
+template <class Src, bool BAD>
+__global__ void __launch_bounds__(kDetWarps * 32) det_kernel(Src src, int B, int n, int32_t* __restrict__ scores,
+                                                               int32_t* __restrict__ badness) {
+  __shared__ __align__(16) int cs_all[kDetWarps][kMaxM];
+  __shared__ int bad_all[BAD ? kDetWarps : 1][BAD ? kMaxM : 1];
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int b = blockIdx.x * kDetWarps + warp;
+  if (b >= B) return;
+  const int m = 2 * n;
+  int* cs = cs_all[warp];
+  int* bad = BAD ? bad_all[warp] : nullptr;
+  for (int s = lane; s < m; s += 32) {
+    cs[s] = src.col(b, n, s);
+    if (BAD) bad[s] = 0;
+  }
+  __syncwarp();
+  const int cnt = warp_sum(det_state<BAD>(cs, n, lane, bad));
+  if (lane == 0) scores[b] = cnt;
+  if (BAD) {
+    __syncwarp();
+    for (int s = lane; s < m; s += 32) badness[(size_t)b * m + s] = bad[s];
+  }
+}
+
+// Slope line count of one state.  Returns sum over anchors of badness (3E).
+// hist: this warp's zeroed direction histogram (kDirWords words); it is left
+// zeroed on return.  bad_out (per slot) may be null.
+__device__ int slope_state(const int* __restrict__ cs, int n, const uint16_t* __restrict__ lut,
+                           uint32_t* __restrict__ hist, int lane, int* __restrict__ bad_out) {
+  const int m = 2 * n;
+  int total = 0;
+  for (int a = 0; a < m; ++a) {
+    const int ra = a >> 1, ca = cs[a];
+    int pairs = 0;
+    int ids[(kMaxM + 31) / 32];
+#pragma unroll
+    for (int t = 0; t < (kMaxM + 31) / 32; ++t) {
+      const int b = lane + 32 * t;
+      ids[t] = -1;
+      if (b < m && (b >> 1) != ra) {  // the row partner has the lone direction (0,1)
+        const int id = dir_id(lut, (b >> 1) - ra, cs[b] - ca);
+        ids[t] = id;
+        pairs += hist_add(hist, id);  // earlier points on this direction
+      }
+    }
+    __syncwarp();
+#pragma unroll
+    for (int t = 0; t < (kMaxM + 31) / 32; ++t)
+      if (ids[t] >= 0) hist_clear(hist, ids[t]);
+    __syncwarp();
+    pairs = warp_sum(pairs);
+    if (bad_out != nullptr && lane == (a & 31)) bad_out[a] = pairs;
+    total += pairs;
+  }
+  return total;
+}
+
+constexpr int kSlopeWarps = 4;
+constexpr size_t kSlopeSmem = sizeof(uint16_t) * kLutSize + sizeof(uint32_t) * kDirWords * kSlopeWarps +
+                              sizeof(int) * kMaxM * kSlopeWarps * 2 + 64;
+
+// Loads one state, validating columns (range, row duplicates).  Returns the
+// device error bits for this state (warp-uniform).
+template <class Src>
+__device__ __forceinline__ uint32_t load_checked(const Src& src, int b, int n, int* cs, int lane) {
+  const int m = 2 * n;
+  uint32_t err = 0;
+  for (int s = lane; s < m; s += 32) {
+    const int c = src.col(b, n, s);
+    if (c < 0 || c >= n) err |= kErrColumnRange;
+    cs[s] = min(max(c, 0), n - 1);
+  }
+  __syncwarp();
+  for (int r = lane; r < n; r += 32)
+    if (cs[2 * r] == cs[2 * r + 1]) err |= kErrDuplicate;
+  err = __reduce_or_sync(0xffffffffu, err);
+  return err;
+}
+
+// MODE 0: slope only (scores, badness).  MODE 1: determinant + slope, checked.
+template <int MODE>
+__global__ void __launch_bounds__(kSlopeWarps * 32) slope_kernel(ColSource src, int B, int n,
+                                                                   int32_t* __restrict__ scores,
+                                                                   int32_t* __restrict__ badness,
+                                                                   int32_t* __restrict__ mismatch,
+                                                                   uint32_t* __restrict__ error_word) {
+  extern __shared__ __align__(16) unsigned char smem[];
+  uint16_t* lut = reinterpret_cast<uint16_t*>(smem);
+  uint32_t* hist_all = reinterpret_cast<uint32_t*>(smem + ((sizeof(uint16_t) * kLutSize + 15) & ~size_t(15)));
+  int* cs_all = reinterpret_cast<int*>(hist_all + kDirWords * kSlopeWarps);
+  int* bad_all = cs_all + kMaxM * kSlopeWarps;
+  for (int i = threadIdx.x; i < kLutSize; i += blockDim.x) lut[i] = g_dir_lut[i];
+  for (int i = threadIdx.x; i < kDirWords * kSlopeWarps; i += blockDim.x) hist_all[i] = 0u;
+  __syncthreads();
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int m = 2 * n;
+  int* cs = cs_all + warp * kMaxM;
+  int* bad = bad_all + warp * kMaxM;
+  uint32_t* hist = hist_all + warp * kDirWords;
+  for (int b = blockIdx.x * kSlopeWarps + warp; b < B; b += gridDim.x * kSlopeWarps) {
+    const uint32_t err = load_checked(src, b, n, cs, lane);
+    if (err) {  // invalid state: no count is meaningful
+      if (lane == 0) {
+        scores[b] = -1;
+        if (error_word) atomicOr(error_word, err);
+        if (MODE == 1) atomicAdd(mismatch, 1);
+      }
+      if (badness)
+        for (int s = lane; s < m; s += 32) badness[(size_t)b * m + s] = -1;
+      __syncwarp();
+      continue;
+    }
+    const int total = slope_state(cs, n, lut, hist, lane, bad);
+    __syncwarp();
+    if (MODE == 0) {
+      if (lane == 0) scores[b] = total / 3;
+    } else {
+      const int e_det = warp_sum(det_state<false>(cs, n, lane, nullptr));
+      if (lane == 0) {
+        scores[b] = e_det;
+        if (total != 3 * e_det) {
+          atomicAdd(mismatch, 1);
+          if (error_word) atomicOr(error_word, kErrMismatch);
+        }
+      }
+    }
+    if (badness)
+      for (int s = lane; s < m; s += 32) badness[(size_t)b * m + s] = bad[s];
+    __syncwarp();
+  }
+}
+
+}  // namespace n3
+
+namespace n3host {
+
+int build_dir_lut(cudaStream_t st) {
+  n3::build_dir_lut_kernel<<<1, 1024, 0, st>>>();
+  N3_TRY(check_launch("build_dir_lut_kernel"));
+  int count = 0;
+  if (cudaMemcpyFromSymbolAsync(&count, n3::g_dir_count, sizeof(int), 0, cudaMemcpyDeviceToHost, st) != cudaSuccess ||
+      cudaStreamSynchronize(st) != cudaSuccess)
+    return check_launch("direction table read-back");
+  if (count != n3::kDirCount)
+    return set_error(N3_ERR_CUDA, "direction table has %d ids, expected %d", count, n3::kDirCount);
+  return N3_OK;
+}
+
+const uint16_t* dir_lut_device_ptr() {
+  void* p = nullptr;
+  if (cudaGetSymbolAddress(&p, n3::g_dir_lut) != cudaSuccess) return nullptr;
+  return static_cast<const uint16_t*>(p);
+}
+
+static int check_common(int B, int n, const void* a, const void* out) {
+  if (n < 2 || n > N3_MAX_N) return set_error(N3_ERR_RANGE, "n=%d outside [2, %d]", n, N3_MAX_N);
+  if (B < 0) return set_error(N3_ERR_ARG, "negative batch size %d", B);
+  if (B > 0 && (a == nullptr || out == nullptr)) return set_error(N3_ERR_ARG, "null device pointer");
+  return N3_OK;
+}
+
+template <class Src>
+static int launch_det(Src src, int B, int n, int32_t* scores, int32_t* badness, cudaStream_t st) {
+  if (B == 0) return N3_OK;
+  const int grid = (B + n3::kDetWarps - 1) / n3::kDetWarps;
+  if (badness)
+    n3::det_kernel<Src, true><<<grid, n3::kDetWarps * 32, 0, st>>>(src, B, n, scores, badness);
+  else
+    n3::det_kernel<Src, false><<<grid, n3::kDetWarps * 32, 0, st>>>(src, B, n, scores, nullptr);
+  return check_launch("det_kernel");
+}
+
+template <int MODE>
+static int launch_slope(const int16_t* cols, int B, int n, int32_t* scores, int32_t* badness, int32_t* mismatch,
+                        uint32_t* error_word, cudaStream_t st) {
+  if (B == 0) return N3_OK;
+  N3_TRY(ensure_device_tables());
+  static bool attr_set[2] = {false, false};
+  if (!attr_set[MODE]) {
+    if (cudaFuncSetAttribute(n3::slope_kernel<MODE>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)n3::kSlopeSmem) != cudaSuccess)
+      return check_launch("cudaFuncSetAttribute(slope_kernel)");
+    attr_set[MODE] = true;
+  }
+  const int blocks_needed = (B + n3::kSlopeWarps - 1) / n3::kSlopeWarps;
+  const int grid = blocks_needed < sm_count() * 3 ? blocks_needed : sm_count() * 3;
+  n3::slope_kernel<MODE><<<grid, n3::kSlopeWarps * 32, n3::kSlopeSmem, st>>>(n3::ColSource{cols}, B, n, scores,
+                                                                             badness, mismatch, error_word);
+  return check_launch("slope_kernel");
+}
+
+}  // namespace n3host
+
+extern "C" {
+
+int n3_score_population(const int32_t* p, const int32_t* q, int B, int n, int32_t* scores, int32_t* badness,
+                        void* stream) {
+  N3_TRY(n3host::check_common(B, n, p, scores));
+  if (B > 0 && q == nullptr) return n3host::set_error(N3_ERR_ARG, "null Q pointer");
+  return n3host::launch_det(n3::PQSource{p, q}, B, n, scores, badness, (cudaStream_t)stream);
+}
+
+int n3_score_columns(const int16_t* cols, int B, int n, int32_t* scores, int32_t* badness, void* stream) {
+  N3_TRY(n3host::check_common(B, n, cols, scores));
+  return n3host::launch_det(n3::ColSource{cols}, B, n, scores, badness, (cudaStream_t)stream);
+}
+
+int n3_score_slope(const int16_t* cols, int B, int n, int32_t* scores, int32_t* badness, void* stream) {
+  N3_TRY(n3host::check_common(B, n, cols, scores));
+  return n3host::launch_slope<0>(cols, B, n, scores, badness, nullptr, nullptr, (cudaStream_t)stream);
+}
+
+int n3_score_checked(const int16_t* cols, int B, int n, int32_t* scores, int32_t* badness, int32_t* mismatch,
+                     uint32_t* error_word, void* stream) {
+  N3_TRY(n3host::check_common(B, n, cols, scores));
+  if (B > 0 && mismatch == nullptr) return n3host::set_error(N3_ERR_ARG, "null mismatch counter");
+  return n3host::launch_slope<1>(cols, B, n, scores, badness, mismatch, error_word, (cudaStream_t)stream);
+}
+
+}  // extern "C"

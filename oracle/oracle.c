@@ -1,0 +1,390 @@
+/*
+ * CPU oracle for the no-three-in-line population search hot path.
+ *
+ * TEST INFRASTRUCTURE ONLY.  This file is a plain-C restatement of the
+ * reference's CPU algorithms (MilliganCo/no-three-in-line, package
+ * src/no_three_75).  Only tests/, __graft_entry__.smoke() and bench.py's CPU
+ * baseline / reference arm may load it, and only as the checker or as the
+ * timed CPU baseline.  The product path (the CUDA library) never calls it.
+ *
+ * Parity is pinned: tests/test_oracle_golden.py checks every function here
+ * against golden vectors produced by the reference itself
+ * (tests/golden/make_golden.py imports the reference and records its
+ * outputs), including the reference's own fixture
+ * results/best-near-solution-E10.json (E = 10).
+ *
+ * Slot layout used throughout (the reference's interleave,
+ * src/no_three_75/accelerated.py:18-24 and src/no_three_75/tempering.py:38):
+ *   slot s = 2*row + layer,  row(s) = s >> 1,  col[2r] = P[r], col[2r+1] = Q[r].
+ */
+#include <stdint.h>
+#include <stdlib.h>
+#include <string.h>
+
+#include <pthread.h>
+#include <unistd.h>
+
+#define N3O_SENTINEL64 (((int64_t)1) << 60)
+
+/* Minimal static-split parallel-for over [0, count) on `threads` pthreads
+ * (threads < 1: every online CPU). */
+typedef void (*n3o_body_fn)(int index, void* ctx);
+typedef struct {
+    n3o_body_fn body;
+    void* ctx;
+    int begin, end;
+} n3o_span;
+
+static void* n3o_run_span(void* arg) {
+    n3o_span* s = (n3o_span*)arg;
+    for (int i = s->begin; i < s->end; ++i) s->body(i, s->ctx);
+    return NULL;
+}
+
+int n3o_max_threads(void) {
+    const long c = sysconf(_SC_NPROCESSORS_ONLN);
+    return c > 0 ? (int)c : 1;
+}
+
+static void n3o_parallel_for(int count, int threads, n3o_body_fn body, void* ctx) {
+    if (threads < 1) threads = n3o_max_threads();
+    if (threads > count) threads = count;
+    if (threads <= 1) {
+        for (int i = 0; i < count; ++i) body(i, ctx);
+        return;
+    }
+    pthread_t tid[256];
+    n3o_span spans[256];
+    if (threads > 256) threads = 256;
+    for (int t = 0; t < threads; ++t) {
+        spans[t].body = body;
+        spans[t].ctx = ctx;
+        spans[t].begin = (int)((long long)count * t / threads);
+        spans[t].end = (int)((long long)count * (t + 1) / threads);
+        pthread_create(&tid[t], NULL, n3o_run_span, &spans[t]);
+    }
+    for (int t = 0; t < threads; ++t) pthread_join(tid[t], NULL);
+}
+
+static void interleave(const int32_t* p, const int32_t* q, int n, int32_t* rows, int32_t* cols) {
+    for (int r = 0; r < n; ++r) {
+        rows[2 * r] = r;
+        cols[2 * r] = p[r];
+        rows[2 * r + 1] = r;
+        cols[2 * r + 1] = q[r];
+    }
+}
+
+/* Restates src/no_three_75/accelerated.py:14-37 (score_and_badness): the
+ * i<j<k triple loop with the hoisted (dx1, dy1) of the pair (i, j) and the
+ * cross-product test dx1*(c_k-c_i) == dy1*(r_k-r_i). */
+int64_t n3o_score_and_badness(const int32_t* p, const int32_t* q, int n, int64_t* badness) {
+    const int m = 2 * n;
+    int32_t rows[512], cols[512];
+    if (m > 512) return -1;
+    interleave(p, q, n, rows, cols);
+    if (badness) memset(badness, 0, sizeof(int64_t) * (size_t)m);
+    int64_t score = 0;
+    for (int i = 0; i < m - 2; ++i) {
+        for (int j = i + 1; j < m - 1; ++j) {
+            const int32_t dx1 = rows[j] - rows[i];
+            const int32_t dy1 = cols[j] - cols[i];
+            for (int k = j + 1; k < m; ++k) {
+                if (dx1 * (cols[k] - cols[i]) == dy1 * (rows[k] - rows[i])) {
+                    ++score;
+                    if (badness) {
+                        ++badness[i];
+                        ++badness[j];
+                        ++badness[k];
+                    }
+                }
+            }
+        }
+    }
+    return score;
+}
+
+typedef struct {
+    const int32_t *p, *q;
+    int n;
+    int32_t *scores, *badness;
+    int slope;
+} n3o_pop_ctx;
+
+int64_t n3o_slope_score_points(const int32_t* rows, const int32_t* cols, int m, int64_t* badness);
+
+static void n3o_pop_body(int b, void* arg) {
+    const n3o_pop_ctx* c = (const n3o_pop_ctx*)arg;
+    const int n = c->n;
+    int64_t bad[512];
+    int64_t s;
+    if (c->slope) {
+        int32_t rows[512], cols[512];
+        interleave(c->p + (size_t)b * n, c->q + (size_t)b * n, n, rows, cols);
+        s = n3o_slope_score_points(rows, cols, 2 * n, bad);
+    } else {
+        s = n3o_score_and_badness(c->p + (size_t)b * n, c->q + (size_t)b * n, n, bad);
+    }
+    c->scores[b] = (int32_t)s;
+    if (c->badness)
+        for (int t = 0; t < 2 * n; ++t) c->badness[(size_t)b * 2 * n + t] = (int32_t)bad[t];
+}
+
+/* Batched form of the above over a population of P/Q states, the CPU side of
+ * src/no_three_75/gpu.py:99-109 (benchmark_gpu's serial loop), optionally
+ * spread over `threads` threads (< 1: all CPUs).  badness may be NULL. */
+void n3o_score_population(const int32_t* p, const int32_t* q, int B, int n, int32_t* scores,
+                          int32_t* badness, int threads) {
+    n3o_pop_ctx c = {p, q, n, scores, badness, 0};
+    n3o_parallel_for(B, threads, n3o_pop_body, &c);
+}
+
+static int igcd(int a, int b) {
+    if (a < 0) a = -a;
+    if (b < 0) b = -b;
+    while (b) {
+        const int t = a % b;
+        a = b;
+        b = t;
+    }
+    return a;
+}
+
+/* Primitive undirected direction of b - a: src/no_three_75/verifier_b.py:8-19
+ * (gcd-reduced, dx >= 0, and dy > 0 when dx == 0).  Packed into one int. */
+static int direction_key(int ra, int ca, int rb, int cb) {
+    int dx = rb - ra, dy = cb - ca;
+    const int g = igcd(dx, dy);
+    dx /= g;
+    dy /= g;
+    if (dx < 0 || (dx == 0 && dy < 0)) {
+        dx = -dx;
+        dy = -dy;
+    }
+    return (dx + 1024) * 4096 + (dy + 1024);
+}
+
+static int cmp_int(const void* a, const void* b) {
+    const int x = *(const int*)a, y = *(const int*)b;
+    return (x > y) - (x < y);
+}
+
+/* Normalised-slope line count over an arbitrary point list.  For each anchor a
+ * the other points are grouped by primitive direction (verifier_b.py:22-33
+ * stops at the first repeat; here every repeat is counted).  A line holding k
+ * points gives each member C(k-1,2) equal-direction pairs, so
+ *   badness[a] = sum_dir C(c_dir, 2)           (conflicts.py:376-378)
+ *   E          = (1/3) sum_a badness[a]        (= sum_lines C(k,3), conflicts.py:373)
+ * Returns E, or -1 when the points are not distinct or m is too large. */
+int64_t n3o_slope_score_points(const int32_t* rows, const int32_t* cols, int m, int64_t* badness) {
+    int keys[512];
+    if (m > 512) return -1;
+    int64_t total = 0;
+    for (int a = 0; a < m; ++a) {
+        int c = 0;
+        for (int b = 0; b < m; ++b) {
+            if (b == a) continue;
+            if (rows[a] == rows[b] && cols[a] == cols[b]) return -1;
+            keys[c++] = direction_key(rows[a], cols[a], rows[b], cols[b]);
+        }
+        qsort(keys, (size_t)c, sizeof(int), cmp_int);
+        int64_t pairs = 0;
+        int run = 1;
+        for (int t = 1; t <= c; ++t) {
+            if (t < c && keys[t] == keys[t - 1]) {
+                ++run;
+            } else {
+                pairs += (int64_t)run * (run - 1) / 2;
+                run = 1;
+            }
+        }
+        if (badness) badness[a] = pairs;
+        total += pairs;
+    }
+    if (total % 3) return -2;
+    return total / 3;
+}
+
+/* Batched slope line count over P/Q states (threads as above). */
+void n3o_slope_population(const int32_t* p, const int32_t* q, int B, int n, int32_t* scores,
+                          int32_t* badness, int threads) {
+    n3o_pop_ctx c = {p, q, n, scores, badness, 1};
+    n3o_parallel_for(B, threads, n3o_pop_body, &c);
+}
+
+/* Restates src/no_three_75/accelerated.py:122-195 (evaluate_two_switches):
+ * for the selected slot u, the full score after exchanging its column with
+ * every legal partner slot v, via current - (bad[u]+bad[v]-joint_old) +
+ * new_affected.  Illegal partners keep the sentinel 1<<60. */
+void n3o_two_switches(const int32_t* p, const int32_t* q, int n, int u, int64_t current,
+                      const int64_t* badness, int64_t* out) {
+    const int m = 2 * n;
+    int32_t rows[512], cols[512];
+    interleave(p, q, n, rows, cols);
+    for (int v = 0; v < m; ++v) out[v] = N3O_SENTINEL64;
+    const int srow = rows[u];
+    const int sother = 2 * srow + (1 - (u & 1));
+    for (int v = 0; v < m; ++v) {
+        if (v == u || rows[v] == srow) continue;
+        const int prow = rows[v];
+        const int pother = 2 * prow + (1 - (v & 1));
+        if (cols[v] == cols[sother] || cols[u] == cols[pother]) continue;
+        int64_t joint = 0;
+        for (int o = 0; o < m; ++o) {
+            if (o == u || o == v) continue;
+            if ((rows[v] - rows[u]) * (cols[o] - cols[u]) == (cols[v] - cols[u]) * (rows[o] - rows[u])) ++joint;
+        }
+        const int64_t old_aff = badness[u] + badness[v] - joint;
+        const int nur = rows[u], nuc = cols[v], nvr = rows[v], nvc = cols[u];
+        int64_t aff = 0;
+        for (int i = 0; i < m - 1; ++i) {
+            if (i == u) continue;
+            const int ir = rows[i], ic = (i == v) ? nvc : cols[i];
+            for (int j = i + 1; j < m; ++j) {
+                if (j == u) continue;
+                const int jr = rows[j], jc = (j == v) ? nvc : cols[j];
+                if ((ir - nur) * (jc - nuc) == (ic - nuc) * (jr - nur)) ++aff;
+            }
+        }
+        for (int i = 0; i < m - 1; ++i) {
+            if (i == u || i == v) continue;
+            for (int j = i + 1; j < m; ++j) {
+                if (j == u || j == v) continue;
+                if ((rows[i] - nvr) * (cols[j] - nvc) == (cols[i] - nvc) * (rows[j] - nvr)) ++aff;
+            }
+        }
+        out[v] = current - old_aff + aff;
+    }
+}
+
+/* Restates src/no_three_75/accelerated.py:40-119 (evaluate_transpositions):
+ * same-layer row transpositions of the selected (layer, row). */
+void n3o_transpositions(const int32_t* p, const int32_t* q, int n, int layer, int row, int64_t current,
+                        const int64_t* badness, int64_t* out) {
+    const int m = 2 * n;
+    int32_t rows[512], cols[512];
+    interleave(p, q, n, rows, cols);
+    for (int r = 0; r < n; ++r) out[r] = N3O_SENTINEL64;
+    const int u = 2 * row + layer;
+    for (int pr = 0; pr < n; ++pr) {
+        if (pr == row) continue;
+        if (layer == 0) {
+            if (p[pr] == q[row] || p[row] == q[pr]) continue;
+        } else {
+            if (q[pr] == p[row] || q[row] == p[pr]) continue;
+        }
+        const int v = 2 * pr + layer;
+        int64_t joint = 0;
+        for (int o = 0; o < m; ++o) {
+            if (o == u || o == v) continue;
+            if ((rows[v] - rows[u]) * (cols[o] - cols[u]) == (cols[v] - cols[u]) * (rows[o] - rows[u])) ++joint;
+        }
+        const int64_t old_aff = badness[u] + badness[v] - joint;
+        const int nur = rows[u], nuc = cols[v], nvr = rows[v], nvc = cols[u];
+        int64_t aff = 0;
+        for (int i = 0; i < m - 1; ++i) {
+            if (i == u) continue;
+            const int ir = rows[i], ic = (i == v) ? nvc : cols[i];
+            for (int j = i + 1; j < m; ++j) {
+                if (j == u) continue;
+                const int jr = rows[j], jc = (j == v) ? nvc : cols[j];
+                if ((ir - nur) * (jc - nuc) == (ic - nuc) * (jr - nur)) ++aff;
+            }
+        }
+        for (int i = 0; i < m - 1; ++i) {
+            if (i == u || i == v) continue;
+            for (int j = i + 1; j < m; ++j) {
+                if (j == u || j == v) continue;
+                if ((rows[i] - nvr) * (cols[j] - nvc) == (cols[i] - nvc) * (rows[j] - nvr)) ++aff;
+            }
+        }
+        out[pr] = current - old_aff + aff;
+    }
+}
+
+static int aligned3(int a, int ca, int b, int cb, int c, int cc) {
+    return (b - a) * (cc - ca) == (cb - ca) * (c - a);
+}
+
+/* Restates the exact move delta of the reference's persistent walk kernel,
+ * src/no_three_75/tempering.py:58 (legality) and :68-89 (delta): slot u takes
+ * column c_v and slot v takes c_u.  Every pair (i<j) outside {u,v} adds
+ * aligned(u',i,j)-aligned(u,i,j) + aligned(v',i,j)-aligned(v,i,j); every k
+ * outside {u,v} adds aligned(u',v',k)-aligned(u,v,k).  Each changed triple
+ * also moves the badness of its three members by the same +-1.
+ * cols is the slot-layout column array of one state (length 2n).
+ * Returns 1 for a legal move (dE / dbad written), 0 otherwise. */
+int n3o_walk_delta(const int32_t* cols, int n, int u, int v, int32_t* dE, int32_t* dbad) {
+    const int m = 2 * n;
+    if (dbad) memset(dbad, 0, sizeof(int32_t) * (size_t)m);
+    *dE = 0;
+    const int cu = cols[u], cv = cols[v];
+    if (!((u >> 1) != (v >> 1) && cu != cv && cols[u ^ 1] != cv && cols[v ^ 1] != cu)) return 0;
+    const int ru = u >> 1, rv = v >> 1;
+    int32_t delta = 0;
+    for (int i = 0; i < m - 1; ++i) {
+        if (i == u || i == v) continue;
+        const int ri = i >> 1, ci = cols[i];
+        for (int j = i + 1; j < m; ++j) {
+            if (j == u || j == v) continue;
+            const int rj = j >> 1, cj = cols[j];
+            int d = aligned3(ru, cv, ri, ci, rj, cj) - aligned3(ru, cu, ri, ci, rj, cj);
+            if (d) {
+                delta += d;
+                if (dbad) { dbad[u] += d; dbad[i] += d; dbad[j] += d; }
+            }
+            d = aligned3(rv, cu, ri, ci, rj, cj) - aligned3(rv, cv, ri, ci, rj, cj);
+            if (d) {
+                delta += d;
+                if (dbad) { dbad[v] += d; dbad[i] += d; dbad[j] += d; }
+            }
+        }
+    }
+    for (int k = 0; k < m; ++k) {
+        if (k == u || k == v) continue;
+        const int d = aligned3(ru, cv, rv, cu, k >> 1, cols[k]) - aligned3(ru, cu, rv, cv, k >> 1, cols[k]);
+        if (d) {
+            delta += d;
+            if (dbad) { dbad[u] += d; dbad[v] += d; dbad[k] += d; }
+        }
+    }
+    *dE = delta;
+    return 1;
+}
+
+/* Score + badness of one slot-layout column array (rows implicit). */
+int32_t n3o_score_columns(const int32_t* cols, int n, int32_t* badness) {
+    const int m = 2 * n;
+    int32_t p[256] = {0}, q[256] = {0};
+    int64_t bad[512];
+    if (n > 256) return -1;
+    for (int r = 0; r < n; ++r) {
+        p[r] = cols[2 * r];
+        q[r] = cols[2 * r + 1];
+    }
+    const int64_t s = n3o_score_and_badness(p, q, n, bad);
+    if (badness)
+        for (int t = 0; t < m; ++t) badness[t] = (int32_t)bad[t];
+    return (int32_t)s;
+}
+
+
+/* Determinant count over an arbitrary point list (the test of
+ * src/no_three_75/verifier_a.py:8-16, counted over all triples instead of
+ * stopping at the first witness).  badness may be NULL. */
+int64_t n3o_det_score_points(const int32_t* rows, const int32_t* cols, int m, int64_t* badness) {
+    if (badness) memset(badness, 0, sizeof(int64_t) * (size_t)m);
+    int64_t score = 0;
+    for (int i = 0; i < m - 2; ++i)
+        for (int j = i + 1; j < m - 1; ++j)
+            for (int k = j + 1; k < m; ++k)
+                if ((rows[j] - rows[i]) * (cols[k] - cols[i]) == (cols[j] - cols[i]) * (rows[k] - rows[i])) {
+                    ++score;
+                    if (badness) {
+                        ++badness[i];
+                        ++badness[j];
+                        ++badness[k];
+                    }
+                }
+    return score;
+}
