@@ -126,6 +126,82 @@ int n3_transposition_scores(const int16_t* cols, const int32_t* badness, const i
                             int B, int n, const int32_t* anchors, int A, int32_t* out, void* stream);
 
 /* ---------------------------------------------------------------------------
+ * (c) Replica-exchange tempering.
+ *
+ * Chains are grouped in ladders of L consecutive chains; chain c belongs to
+ * ladder c / L.  Every array below is device memory owned by the caller
+ * (the Python TemperingChains object); the kernel keeps each chain's state in
+ * shared memory for the whole launch and writes it back at the end.
+ * Replaces the reference's walk kernel and TemperingChains.advance/exchange
+ * (src/no_three_75/tempering.py:29-191), with the exchange on the device.
+ * ------------------------------------------------------------------------- */
+
+#define N3_SLOT_STRIDE 150 /* row stride of the per-chain arrays (2 * N3_MAX_N) */
+
+typedef struct n3_chains {
+  int n_chains;                 /* C, a positive multiple of ladder_size */
+  int ladder_size;              /* L, temperatures per ladder, 2..64 */
+  int16_t* cols;                /* [C][150] slot columns (first 2n used) */
+  int32_t* badness;             /* [C][150] triples through each slot, kept exact */
+  int32_t* energy;              /* [C] current E */
+  int32_t* best_energy;         /* [C] lowest E seen */
+  int16_t* best_cols;           /* [C][150] state at best_energy */
+  int32_t* temp_of;             /* [C] temperature index of chain c (ladder-major) */
+  int32_t* chain_at;            /* [C] chain_at[l*L + t]: ladder-local chain at temperature t */
+  uint64_t* counter;            /* [C] proposals made (Philox counter) */
+  uint32_t* accepted;           /* [C] accepted proposals */
+  const int32_t* ladder_n;      /* [C/L] grid size n of each ladder (mixed sizes allowed) */
+  uint32_t* ladder_round;       /* [C/L] exchange rounds done (even/odd parity) */
+  uint32_t* ladder_exchanges;   /* [C/L] accepted exchanges */
+  const uint32_t* acc_thresh;   /* [L][acc_width]: accept dE > 0 iff u32 < acc_thresh[t][dE] */
+  int acc_width;                /* dE >= acc_width is rejected */
+  const uint32_t* exch_thresh;  /* [L-1][exch_width]: swap (t,t+1) with energy gap -d iff u32 < thr[t][d] */
+  int exch_width;
+  int32_t* global_best;         /* [1] atomic minimum of best_energy, or NULL */
+  int32_t* hit;                 /* [4] first chain with E <= target: chain, counter, globaltimer lo/hi; or NULL */
+  int32_t* stop;                /* [1] nonzero: stop at the next exchange boundary; or NULL */
+  uint32_t* error_word;         /* [1] device error bits (16: incremental/full mismatch); or NULL */
+} n3_chains;
+
+typedef struct n3_temper_config {
+  uint64_t seed;                /* Philox key */
+  int chains_per_block;         /* warps (chains) per CTA: divides L (cluster of L/cpb CTAs) or a multiple of L */
+  int rounds;                   /* exchange rounds this launch (when ladder_rounds is NULL) */
+  const int32_t* ladder_rounds; /* [C/L] per-ladder rounds (device), equal within a CTA or cluster; or NULL */
+  int round_sweeps;             /* proposals per round = round_sweeps * 2n (one sweep = 2n proposals) ... */
+  int round_proposals;          /* ... unless round_proposals > 0 */
+  int exchange;                 /* 1: neighbour exchange after every round */
+  int target_energy;            /* >= 0: record the first chain reaching E <= target (and raise *stop) */
+} n3_temper_config;
+
+/* Runs cfg->rounds rounds (proposals, then an exchange) on every ladder in one
+ * persistent launch: grid C/cpb CTAs of cpb warps, clusters of L/cpb CTAs
+ * when a ladder spans several CTAs.  Capturable in a CUDA graph (fixed
+ * arguments; the per-device tables must have been set up by an earlier call). */
+int n3_temper_run(const n3_chains* chains, const n3_temper_config* config, void* stream);
+
+/* Recomputes every chain's E (determinant count) and badness (slope count)
+ * and adds the number of chains that differ from the maintained values to
+ * *mismatch (device int32).  The reference's TemperingChains.validate
+ * (src/no_three_75/tempering.py:193-204), on the device. */
+int n3_temper_audit(const n3_chains* chains, int32_t* mismatch, void* stream);
+
+/* Device clock (%globaltimer, ns) written to *out (device int64) in stream
+ * order; used to time a run to its first target hit on the device. */
+int n3_device_clock_ns(int64_t* out, void* stream);
+
+/* ---------------------------------------------------------------------------
+ * CUDA graphs (no reference counterpart: the reference launches every epoch
+ * from Python, src/no_three_75/tempering.py:275-278).  Capture the launches
+ * made on `stream` between n3_graph_begin and n3_graph_end (thread-local
+ * capture mode), then replay them with n3_graph_launch.
+ * ------------------------------------------------------------------------- */
+int n3_graph_begin(void* stream);
+int n3_graph_end(void* stream, void** graph_exec);
+int n3_graph_launch(void* graph_exec, void* stream);
+int n3_graph_destroy(void* graph_exec);
+
+/* ---------------------------------------------------------------------------
  * Measurement helper (no reference counterpart).
  * ------------------------------------------------------------------------- */
 

@@ -41,6 +41,10 @@ _SIGNATURES: dict[str, list] = {
     "n3_swap_delta_pairs": [_P, _I, _I, _P, _I, _P, _P, _P],
     "n3_two_switch_scores": [_P, _P, _P, _I, _I, _P, _I, _P, _P],
     "n3_transposition_scores": [_P, _P, _P, _I, _I, _P, _I, _P, _P],
+    "n3_graph_begin": [_P],
+    "n3_graph_end": [_P, ctypes.POINTER(ctypes.c_void_p)],
+    "n3_graph_launch": [_P, _P],
+    "n3_graph_destroy": [_P],
 }
 _RESTYPE = {"n3_last_error": ctypes.c_char_p}
 

@@ -2,7 +2,9 @@
 #include <cstdarg>
 #include <cstdio>
 #include <mutex>
+#include <set>
 #include <string>
+#include <utility>
 
 #include "n3_common.cuh"
 
@@ -59,6 +61,21 @@ int ensure_device_tables() {
   return N3_OK;
 }
 
+// Opts `kernel` into `bytes` of dynamic shared memory, once per (kernel, device).
+int allow_smem(const void* kernel, size_t bytes) {
+  static std::mutex mu;
+  static std::set<std::pair<const void*, int>> done;
+  int dev = 0;
+  N3_TRY(current_device(&dev));
+  std::lock_guard<std::mutex> lock(mu);
+  const auto key = std::make_pair(kernel, dev);
+  if (done.count(key)) return N3_OK;
+  const cudaError_t e = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+  if (e != cudaSuccess) return set_error(N3_ERR_CUDA, "cudaFuncSetAttribute: %s", cudaGetErrorString(e));
+  done.insert(key);
+  return N3_OK;
+}
+
 int sm_count() {
   int dev = 0;
   if (current_device(&dev) != N3_OK) return 148;
@@ -77,5 +94,44 @@ extern "C" {
 int n3_version(void) { return 100; }
 
 const char* n3_last_error(void) { return n3host::g_last_error.c_str(); }
+
+}  // extern "C"
+
+// ---------------------------------------------------------------------------
+// CUDA graphs: capture a fixed sequence of launches once, replay it cheaply.
+// ---------------------------------------------------------------------------
+extern "C" {
+
+int n3_graph_begin(void* stream) {
+  if (stream == nullptr) return n3host::set_error(N3_ERR_ARG, "graph capture needs a non-default stream");
+  const cudaError_t e = cudaStreamBeginCapture((cudaStream_t)stream, cudaStreamCaptureModeThreadLocal);
+  if (e != cudaSuccess) return n3host::set_error(N3_ERR_CUDA, "cudaStreamBeginCapture: %s", cudaGetErrorString(e));
+  return N3_OK;
+}
+
+int n3_graph_end(void* stream, void** graph_exec) {
+  if (graph_exec == nullptr) return n3host::set_error(N3_ERR_ARG, "null graph handle");
+  cudaGraph_t g = nullptr;
+  cudaError_t e = cudaStreamEndCapture((cudaStream_t)stream, &g);
+  if (e != cudaSuccess) return n3host::set_error(N3_ERR_CUDA, "cudaStreamEndCapture: %s", cudaGetErrorString(e));
+  cudaGraphExec_t x = nullptr;
+  e = cudaGraphInstantiate(&x, g, 0);
+  cudaGraphDestroy(g);
+  if (e != cudaSuccess) return n3host::set_error(N3_ERR_CUDA, "cudaGraphInstantiate: %s", cudaGetErrorString(e));
+  *graph_exec = (void*)x;
+  return N3_OK;
+}
+
+int n3_graph_launch(void* graph_exec, void* stream) {
+  if (graph_exec == nullptr) return n3host::set_error(N3_ERR_ARG, "null graph handle");
+  const cudaError_t e = cudaGraphLaunch((cudaGraphExec_t)graph_exec, (cudaStream_t)stream);
+  if (e != cudaSuccess) return n3host::set_error(N3_ERR_CUDA, "cudaGraphLaunch: %s", cudaGetErrorString(e));
+  return N3_OK;
+}
+
+int n3_graph_destroy(void* graph_exec) {
+  if (graph_exec != nullptr) cudaGraphExecDestroy((cudaGraphExec_t)graph_exec);
+  return N3_OK;
+}
 
 }  // extern "C"

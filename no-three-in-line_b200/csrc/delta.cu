@@ -29,40 +29,6 @@
 
 namespace n3 {
 
-constexpr int kSlotsPerLane = (kMaxM + 31) / 32;  // 5
-
-// Direction histogram around centre X = (rx, cx) over the slots of the state in
-// smem `cs` (m slots) except skip0, skip1 and except points in X's row (their
-// direction (0,1) is unique).  ids[t] receives the id of slot lane + 32 t
-// (-1 if not inserted).  Returns this lane's share of sum_dir C(count, 2).
-__device__ __forceinline__ int hist_build(const int* __restrict__ cs, int m, int rx, int cx, int skip0, int skip1,
-                                          const uint16_t* __restrict__ lut, uint32_t* __restrict__ hist, int lane,
-                                          int (&ids)[kSlotsPerLane]) {
-  int pairs = 0;
-#pragma unroll
-  for (int t = 0; t < kSlotsPerLane; ++t) {
-    const int k = lane + 32 * t;
-    ids[t] = -1;
-    if (k < m && k != skip0 && k != skip1 && (k >> 1) != rx) {
-      const int id = dir_id(lut, (k >> 1) - rx, cs[k] - cx);
-      ids[t] = id;
-      pairs += hist_add(hist, id);
-    }
-  }
-  return pairs;
-}
-
-__device__ __forceinline__ void hist_release(uint32_t* hist, const int (&ids)[kSlotsPerLane]) {
-#pragma unroll
-  for (int t = 0; t < kSlotsPerLane; ++t)
-    if (ids[t] >= 0) hist_clear(hist, ids[t]);
-}
-
-__device__ __forceinline__ bool legal_swap(const int* cs, int u, int v) {
-  const int cu = cs[u], cv = cs[v];
-  return (u >> 1) != (v >> 1) && cu != cv && cs[u ^ 1] != cv && cs[v ^ 1] != cu;
-}
-
 // Exact dE (and, if dbad != nullptr, this lane's badness changes for slots
 // lane + 32 t, plus the moved slots' changes in *dbad_u, *dbad_v) of a legal
 // move.  Uses the 4 centres u, v, u', v'; hist must be zeroed, is left zeroed.
@@ -277,7 +243,10 @@ __global__ void __launch_bounds__(kDeltaWarps * 32) partner_scores_kernel(
     const int bad_u = badness[(size_t)b * m + u];
     for (int w = warp; w < width; w += kDeltaWarps) {
       const int v = SAME_LAYER ? 2 * w + (u & 1) : w;
-      if (!legal_swap(cs, u, v)) {
+      // The reference's partner rule (accelerated.py:146-151, gpu_delta.py:175-180):
+      // another row, and neither new point duplicates its row partner.  Equal
+      // columns are allowed there (the move is then the identity, score = current).
+      if ((v >> 1) == ru || cs[v] == cs[u ^ 1] || cu == cs[v ^ 1]) {
         if (lane == 0) out[(size_t)a * width + w] = N3_SENTINEL;
         continue;
       }
@@ -314,15 +283,7 @@ namespace n3host {
 
 template <class K>
 static int prepare(K kernel) {
-  static int done[64];
-  int dev = 0;
-  cudaGetDevice(&dev);
-  if (dev >= 0 && dev < 64 && done[dev]) return N3_OK;
-  if (cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)n3::DeltaSmem::bytes) !=
-      cudaSuccess)
-    return check_launch("cudaFuncSetAttribute(delta kernel)");
-  if (dev >= 0 && dev < 64) done[dev] = 1;
-  return N3_OK;
+  return allow_smem(reinterpret_cast<const void*>(kernel), n3::DeltaSmem::bytes);
 }
 
 static int check_state_args(int B, int n, const void* cols) {

@@ -45,6 +45,41 @@ __device__ __forceinline__ int hist_get(const uint32_t* hist, int id) {
 
 __device__ __forceinline__ void hist_clear(uint32_t* hist, int id) { hist[id >> 2] = 0u; }
 
+constexpr int kSlotsPerLane = (kMaxM + 31) / 32;  // 5
+
+// Direction histogram around centre X = (rx, cx) over the slots of the state in
+// smem `cs` (m slots) except skip0, skip1 and except points in X's row (their
+// direction (0,1) is unique).  ids[t] receives the id of slot lane + 32 t
+// (-1 if not inserted).  Returns this lane's share of sum_dir C(count, 2).
+__device__ __forceinline__ int hist_build(const int* __restrict__ cs, int m, int rx, int cx, int skip0, int skip1,
+                                          const uint16_t* __restrict__ lut, uint32_t* __restrict__ hist, int lane,
+                                          int (&ids)[kSlotsPerLane]) {
+  int pairs = 0;
+#pragma unroll
+  for (int t = 0; t < kSlotsPerLane; ++t) {
+    const int k = lane + 32 * t;
+    ids[t] = -1;
+    if (k < m && k != skip0 && k != skip1 && (k >> 1) != rx) {
+      const int id = dir_id(lut, (k >> 1) - rx, cs[k] - cx);
+      ids[t] = id;
+      pairs += hist_add(hist, id);
+    }
+  }
+  return pairs;
+}
+
+__device__ __forceinline__ void hist_release(uint32_t* hist, const int (&ids)[kSlotsPerLane]) {
+#pragma unroll
+  for (int t = 0; t < kSlotsPerLane; ++t)
+    if (ids[t] >= 0) hist_clear(hist, ids[t]);
+}
+
+__device__ __forceinline__ bool legal_swap(const int* cs, int u, int v) {
+  const int cu = cs[u], cv = cs[v];
+  return (u >> 1) != (v >> 1) && cu != cv && cs[u ^ 1] != cv && cs[v ^ 1] != cu;
+}
+
+
 }  // namespace n3
 
 namespace n3host {

@@ -37,6 +37,7 @@ int set_error(int code, const char* fmt, ...);
 int check_launch(const char* what);
 int ensure_device_tables();
 int sm_count();
+int allow_smem(const void* kernel, size_t bytes);
 }  // namespace n3host
 
 #define N3_TRY(expr)                      \

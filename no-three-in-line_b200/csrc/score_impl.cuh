@@ -1,0 +1,126 @@
+// Device bodies of the two population scorers, shared by score.cu (the
+// scoring entry points) and tempering.cu (the on-device energy audit).
+// See score.cu for the method.
+#pragma once
+
+#include "dirs.cuh"
+#include "n3_common.cuh"
+
+namespace n3 {
+
+// Tests of the two pivots of row `rho` against all pairs (x, y) with x on the
+// larger side (R register slots per lane) and y on the smaller side.
+// X=(r_x,c_x), J=(rho,c_j), Y=(r_y,c_y) are collinear iff
+//   (r_x-rho)(c_y-c_j) == (c_x-c_j)(r_y-rho)
+//   <=>  a_x*c_y == a_y*b_x + a_x*c_j,   a = r - rho, b_x = c_x - c_j.
+template <int R, bool BAD>
+__device__ __forceinline__ int det_pivot_row(const int* __restrict__ cs, int n, int rho, int lane, int* bad) {
+  const int cj0 = cs[2 * rho], cj1 = cs[2 * rho + 1];
+  const int above = rho, below = n - 1 - rho;
+  const bool lanes_above = above >= below;
+  const int L = 2 * (lanes_above ? above : below);
+  const int lbase = lanes_above ? 0 : 2 * rho + 2;
+  const int rb0 = lanes_above ? rho + 1 : 0;
+  const int rb1 = lanes_above ? n : rho;
+  int ax[R], bx0[R], bx1[R], k0[R], k1[R], sx[R];
+#pragma unroll
+  for (int r = 0; r < R; ++r) {
+    const int x = lane + 32 * r;
+    if (x < L) {
+      const int s = lbase + x;
+      const int a = (s >> 1) - rho, c = cs[s];
+      ax[r] = a;
+      bx0[r] = c - cj0;
+      bx1[r] = c - cj1;
+      k0[r] = a * cj0;
+      k1[r] = a * cj1;
+      sx[r] = s;
+    } else {  // idle slot: products are 0, targets -1, never a hit
+      ax[r] = 0;
+      bx0[r] = 0;
+      bx1[r] = 0;
+      k0[r] = -1;
+      k1[r] = -1;
+      sx[r] = 0;
+    }
+  }
+  int cnt = 0;
+  const int2* rows2 = reinterpret_cast<const int2*>(cs);
+#pragma unroll 2
+  for (int row = rb0; row < rb1; ++row) {
+    const int2 cy = rows2[row];
+    const int ay = row - rho;
+#pragma unroll
+    for (int r = 0; r < R; ++r) {
+      const int P0 = ax[r] * cy.x, P1 = ax[r] * cy.y;
+      const int T0 = ay * bx0[r] + k0[r], T1 = ay * bx1[r] + k1[r];
+      const int h00 = P0 == T0, h10 = P1 == T0, h01 = P0 == T1, h11 = P1 == T1;
+      cnt += (h00 + h10) + (h01 + h11);
+      if (BAD) {
+        if (h00 | h10 | h01 | h11) {
+          const int hits[4] = {h00, h10, h01, h11};
+#pragma unroll
+          for (int t = 0; t < 4; ++t) {
+            if (hits[t]) {
+              atomicAdd(bad + sx[r], 1);
+              atomicAdd(bad + 2 * rho + (t >> 1), 1);
+              atomicAdd(bad + 2 * row + (t & 1), 1);
+            }
+          }
+        }
+      }
+    }
+  }
+  return cnt;
+}
+
+template <bool BAD>
+__device__ __forceinline__ int det_state(const int* __restrict__ cs, int n, int lane, int* bad) {
+  int cnt = 0;
+  for (int rho = 1; rho < n - 1; ++rho) {
+    const int L = 2 * max(rho, n - 1 - rho);
+    switch ((L + 31) >> 5) {
+      case 1: cnt += det_pivot_row<1, BAD>(cs, n, rho, lane, bad); break;
+      case 2: cnt += det_pivot_row<2, BAD>(cs, n, rho, lane, bad); break;
+      case 3: cnt += det_pivot_row<3, BAD>(cs, n, rho, lane, bad); break;
+      case 4: cnt += det_pivot_row<4, BAD>(cs, n, rho, lane, bad); break;
+      default: cnt += det_pivot_row<5, BAD>(cs, n, rho, lane, bad); break;
+    }
+  }
+  return cnt;
+}
+
+// Slope line count of one state.  Returns sum over anchors of badness (3E).
+// hist: this warp's zeroed direction histogram (kDirWords words); it is left
+// zeroed on return.  bad_out (per slot) may be null.
+__device__ __forceinline__ int slope_state(const int* __restrict__ cs, int n, const uint16_t* __restrict__ lut,
+                           uint32_t* __restrict__ hist, int lane, int* __restrict__ bad_out) {
+  const int m = 2 * n;
+  int total = 0;
+  for (int a = 0; a < m; ++a) {
+    const int ra = a >> 1, ca = cs[a];
+    int pairs = 0;
+    int ids[(kMaxM + 31) / 32];
+#pragma unroll
+    for (int t = 0; t < (kMaxM + 31) / 32; ++t) {
+      const int b = lane + 32 * t;
+      ids[t] = -1;
+      if (b < m && (b >> 1) != ra) {  // the row partner has the lone direction (0,1)
+        const int id = dir_id(lut, (b >> 1) - ra, cs[b] - ca);
+        ids[t] = id;
+        pairs += hist_add(hist, id);  // earlier points on this direction
+      }
+    }
+    __syncwarp();
+#pragma unroll
+    for (int t = 0; t < (kMaxM + 31) / 32; ++t)
+      if (ids[t] >= 0) hist_clear(hist, ids[t]);
+    __syncwarp();
+    pairs = warp_sum(pairs);
+    if (bad_out != nullptr && lane == (a & 31)) bad_out[a] = pairs;
+    total += pairs;
+  }
+  return total;
+}
+
+}  // namespace n3

@@ -1,0 +1,437 @@
+// (c) Replica-exchange tempering: one persistent kernel over thousands of
+// chains, ladders of neighbouring temperatures exchanged on the device.
+//
+// Reference: the per-replica walk kernel and host-side exchange of
+// src/no_three_75/tempering.py:29-191.  Layout and scheduling here:
+//
+// * One warp per chain.  A CTA holds `cpb` chains.  A ladder of L
+//   temperatures lives either inside one CTA (cpb a multiple of L) or across a
+//   thread-block cluster of L / cpb CTAs; its exchange step uses the CTA
+//   barrier or the cluster barrier and distributed shared memory, never a
+//   global spin-wait.
+// * Every chain keeps its columns and badness in shared memory and proposes
+//   uniform row-pair column swaps (slots u, v from Philox4x32-10 with counter
+//   (proposal index, chain), key = seed).  The exact dE uses the maintained
+//   badness for the old side (the reference identity bad[u]+bad[v]-joint,
+//   accelerated.py:78) and two direction histograms for the new side; an
+//   accepted move rebuilds the old-side histograms to update every point's
+//   badness exactly and checks the old side against the maintained badness.
+// * Metropolis acceptance compares a 32-bit uniform with a per-temperature
+//   integer threshold table floor(2^32 exp(-dE/T)) built on the host, so the
+//   CPU oracle replays every chain bit for bit.  Exchanges swap temperature
+//   labels (not states) between neighbours with the reference's rule
+//   (tempering.py:178-184, even/odd alternation), thresholds likewise tabled.
+// * Results depend only on the seed, the chain index and the round structure,
+//   not on cpb or on how rounds are split over launches.
+#include <cooperative_groups.h>
+
+#include "dirs.cuh"
+#include "n3_common.cuh"
+#include "philox.cuh"
+#include "score_impl.cuh"
+
+namespace cg = cooperative_groups;
+
+namespace n3 {
+
+struct TemperArgs {
+  n3_chains ch;
+  n3_temper_config cfg;
+  const uint16_t* lut;  // direction table (device)
+  int cluster;          // CTAs per ladder (1: whole ladders per CTA)
+};
+
+__device__ __forceinline__ uint64_t global_ns() {
+  uint64_t t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+  return t;
+}
+
+// Shared-memory layout of the tempering kernel (dynamic).
+struct TemperSmem {
+  static constexpr size_t lut_bytes = ((sizeof(uint16_t) * kLutSize + 15) / 16) * 16;
+  static __host__ __device__ size_t bytes(int cpb) {
+    return lut_bytes + (size_t)cpb * (sizeof(uint32_t) * kDirWords + 2 * sizeof(int) * kMaxM) +
+           3 * sizeof(int) * 64 + 16;
+  }
+};
+
+// One proposal of the chain held by this warp.  Returns 1 if accepted.
+__device__ __forceinline__ int propose(int* __restrict__ cs, int* __restrict__ bs, int m,
+                                       const uint16_t* __restrict__ lut, uint32_t* __restrict__ hist, int lane,
+                                       U4 rnd, const uint32_t* __restrict__ thr, int W, int& E,
+                                       uint32_t& err) {
+  const int u = (int)__umulhi(rnd.x, (unsigned)m);
+  const int v = (int)__umulhi(rnd.y, (unsigned)m);
+  if (!legal_swap(cs, u, v)) return 0;
+  const int ru = u >> 1, rv = v >> 1, cu = cs[u], cv = cs[v];
+  int ids[kSlotsPerLane], cnt_new[kSlotsPerLane];
+  // centre u' = (r_u, c_v)
+  const int part_a = hist_build(cs, m, ru, cv, u, v, lut, hist, lane, ids);
+  __syncwarp();
+  const int line_new = dir_id(lut, rv - ru, cu - cv);
+  const int j_new = hist_get(hist, line_new);
+#pragma unroll
+  for (int t = 0; t < kSlotsPerLane; ++t)
+    cnt_new[t] = ids[t] >= 0 ? hist_get(hist, ids[t]) - 1 + (ids[t] == line_new) : 0;
+  __syncwarp();
+  hist_release(hist, ids);
+  __syncwarp();
+  // centre v' = (r_v, c_u)
+  const int part_b = hist_build(cs, m, rv, cu, u, v, lut, hist, lane, ids);
+  __syncwarp();
+#pragma unroll
+  for (int t = 0; t < kSlotsPerLane; ++t) cnt_new[t] += ids[t] >= 0 ? hist_get(hist, ids[t]) - 1 : 0;
+  __syncwarp();
+  hist_release(hist, ids);
+  // points of A on the old line (u, v)
+  int joint = 0;
+#pragma unroll
+  for (int t = 0; t < kSlotsPerLane; ++t) {
+    const int k = lane + 32 * t;
+    if (k < m && k != u && k != v) joint += (rv - ru) * (cs[k] - cu) == (cv - cu) * ((k >> 1) - ru);
+  }
+  const int sum_ab = warp_sum(part_a + (part_b << 16));
+  const int sum_joint = warp_sum(joint);
+  const int t_a = sum_ab & 0xFFFF, t_b = sum_ab >> 16;
+  const int dE = (t_a + t_b + j_new) - (bs[u] + bs[v] - sum_joint);
+  const bool accept = dE <= 0 || (dE < W && rnd.z < thr[dE]);
+  if (!accept) {
+    __syncwarp();
+    return 0;
+  }
+  // Old-side histograms: exact badness change of every other point.
+  __syncwarp();
+  int dB[kSlotsPerLane];
+  const int part_c = hist_build(cs, m, ru, cu, u, v, lut, hist, lane, ids);
+  __syncwarp();
+  const int line_old = dir_id(lut, rv - ru, cv - cu);
+  const int j_old = hist_get(hist, line_old);
+#pragma unroll
+  for (int t = 0; t < kSlotsPerLane; ++t)
+    dB[t] = cnt_new[t] - (ids[t] >= 0 ? hist_get(hist, ids[t]) - 1 + (ids[t] == line_old) : 0);
+  __syncwarp();
+  hist_release(hist, ids);
+  __syncwarp();
+  const int part_d = hist_build(cs, m, rv, cv, u, v, lut, hist, lane, ids);
+  __syncwarp();
+#pragma unroll
+  for (int t = 0; t < kSlotsPerLane; ++t) dB[t] -= ids[t] >= 0 ? hist_get(hist, ids[t]) - 1 : 0;
+  __syncwarp();
+  hist_release(hist, ids);
+  const int sum_cd = warp_sum(part_c + (part_d << 16));
+  const int t_c = sum_cd & 0xFFFF, t_d = sum_cd >> 16;
+  if (bs[u] != t_c + j_old || bs[v] != t_d + j_old || j_old != sum_joint) err |= kErrAudit;
+  __syncwarp();
+#pragma unroll
+  for (int t = 0; t < kSlotsPerLane; ++t) {
+    const int k = lane + 32 * t;
+    if (k < m && k != u && k != v) bs[k] += dB[t];
+  }
+  if (lane == 0) {
+    bs[u] = t_a + j_new;
+    bs[v] = t_b + j_new;
+    cs[u] = cv;
+    cs[v] = cu;
+  }
+  __syncwarp();
+  E += dE;
+  return 1;
+}
+
+// Exchange step of one ladder (run by its leader thread).  tmp_chain[t] is the
+// ladder-local chain at temperature t, tmp_temp[i] the temperature of chain i,
+// e[i] the energy of chain i.
+__device__ void exchange_ladder(int* tmp_chain, int* tmp_temp, const int* e, int L, int ladder, uint32_t round,
+                                const uint32_t* __restrict__ xthr, int XW, uint32_t k0, uint32_t k1,
+                                uint32_t& accepted) {
+  for (int t = (int)(round & 1u); t < L - 1; t += 2) {
+    const int a = tmp_chain[t], b = tmp_chain[t + 1];
+    const int D = e[a] - e[b];  // chain a holds the lower temperature
+    bool swap = D >= 0;
+    if (!swap) {
+      const U4 r = philox4x32_10(U4{round, (uint32_t)t, (uint32_t)ladder, kTagExchange}, k0, k1);
+      const int d = -D;
+      swap = d < XW && r.x < xthr[(size_t)t * XW + d];
+    }
+    if (swap) {
+      tmp_chain[t] = b;
+      tmp_chain[t + 1] = a;
+      tmp_temp[a] = t + 1;
+      tmp_temp[b] = t;
+      ++accepted;
+    }
+  }
+}
+
+__global__ void __launch_bounds__(512, 1) temper_kernel(const TemperArgs A) {
+  extern __shared__ __align__(16) unsigned char smem[];
+  const n3_chains& ch = A.ch;
+  const n3_temper_config& cfg = A.cfg;
+  const int cpb = cfg.chains_per_block, L = ch.ladder_size, CS = A.cluster;
+  uint16_t* lut = reinterpret_cast<uint16_t*>(smem);
+  uint32_t* hist_all = reinterpret_cast<uint32_t*>(smem + TemperSmem::lut_bytes);
+  int* cs_all = reinterpret_cast<int*>(hist_all + (size_t)cpb * kDirWords);
+  int* bs_all = cs_all + cpb * kMaxM;
+  int* ld_e = bs_all + cpb * kMaxM;  // leader arrays (64 entries each)
+  int* ld_temp = ld_e + 64;
+  int* ld_chain = ld_temp + 64;
+  int* ld_stop = ld_chain + 64;
+
+  cg::cluster_group cluster = cg::this_cluster();
+  const int rank = CS > 1 ? (int)cluster.block_rank() : 0;
+  auto barrier = [&]() {
+    if (CS > 1)
+      cluster.sync();
+    else
+      __syncthreads();
+  };
+  // leader arrays: CTA rank 0 of the cluster (CS > 1) or this CTA (CS == 1)
+  int* L_e = CS > 1 ? cluster.map_shared_rank(ld_e, 0) : ld_e;
+  int* L_temp = CS > 1 ? cluster.map_shared_rank(ld_temp, 0) : ld_temp;
+  int* L_stop = CS > 1 ? cluster.map_shared_rank(ld_stop, 0) : ld_stop;
+
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int c = blockIdx.x * cpb + warp;
+  const int lad = c / L;
+  const int li = c % L;
+  const int lidx = CS > 1 ? li : warp;              // index into the leader arrays
+  const int lbase = CS > 1 ? 0 : (warp / L) * L;    // this ladder's block in them
+  const int n = ch.ladder_n[lad], m = 2 * n;
+  int* cs = cs_all + warp * kMaxM;
+  int* bs = bs_all + warp * kMaxM;
+  uint32_t* hist = hist_all + (size_t)warp * kDirWords;
+
+  for (int i = threadIdx.x; i < kLutSize; i += blockDim.x) lut[i] = A.lut[i];
+  for (int i = threadIdx.x; i < cpb * kDirWords; i += blockDim.x) hist_all[i] = 0u;
+  for (int s = lane; s < m; s += 32) {
+    cs[s] = ch.cols[(size_t)c * kMaxM + s];
+    bs[s] = ch.badness[(size_t)c * kMaxM + s];
+  }
+  int E = ch.energy[c], bestE = ch.best_energy[c];
+  uint64_t counter = ch.counter[c];
+  uint32_t accepted = ch.accepted[c];
+  uint32_t err = 0;
+  bool hit_done = false;
+
+  // The leader CTA loads the ladder bookkeeping of its ladder(s).
+  const bool leader_cta = rank == 0;
+  const int lad_first = (blockIdx.x * cpb) / L;          // first ladder of this CTA
+  const int n_lad_here = CS > 1 ? 1 : cpb / L;
+  if (leader_cta) {
+    for (int i = threadIdx.x; i < n_lad_here * L; i += blockDim.x) {
+      const int gl = lad_first + i / L;
+      ld_chain[i] = ch.chain_at[(size_t)gl * L + i % L];
+      ld_temp[i] = ch.temp_of[(size_t)gl * L + i % L];
+    }
+    if (threadIdx.x == 0) *ld_stop = 0;
+  }
+  uint32_t lround = 0, lexch = 0;  // leader-thread copies (one leader per ladder)
+  const bool ladder_leader = leader_cta && lane == 0 && (CS > 1 ? warp == 0 : (warp % L) == 0);
+  if (ladder_leader) {
+    lround = ch.ladder_round[lad];
+    lexch = ch.ladder_exchanges[lad];
+  }
+  barrier();
+
+  const int rounds = cfg.ladder_rounds ? cfg.ladder_rounds[lad] : cfg.rounds;
+  const int per_round = cfg.round_proposals > 0 ? cfg.round_proposals : cfg.round_sweeps * m;
+  const uint32_t k0 = (uint32_t)cfg.seed, k1 = (uint32_t)(cfg.seed >> 32);
+  const int W = ch.acc_width;
+  for (int r = 0; r < rounds; ++r) {
+    const int temp = L_temp[lidx];
+    const uint32_t* thr = ch.acc_thresh + (size_t)temp * W;
+    for (int p = 0; p < per_round; ++p) {
+      const U4 rnd = philox4x32_10(U4{(uint32_t)counter, (uint32_t)(counter >> 32), (uint32_t)c, kTagPropose},
+                                   k0, k1);
+      ++counter;
+      if (propose(cs, bs, m, lut, hist, lane, rnd, thr, W, E, err)) {
+        ++accepted;
+        if (E < bestE) {
+          bestE = E;
+          for (int s = lane; s < m; s += 32) ch.best_cols[(size_t)c * kMaxM + s] = (int16_t)cs[s];
+        }
+        if (cfg.target_energy >= 0 && E <= cfg.target_energy && !hit_done) {
+          hit_done = true;
+          if (lane == 0 && ch.hit != nullptr && atomicCAS(ch.hit, -1, c) == -1) {
+            const uint64_t now = global_ns();
+            ch.hit[1] = (int32_t)(uint32_t)counter;
+            ch.hit[2] = (int32_t)(uint32_t)now;
+            ch.hit[3] = (int32_t)(uint32_t)(now >> 32);
+            if (ch.stop) atomicExch(ch.stop, 1);
+          }
+        }
+      }
+    }
+    if (!cfg.exchange) continue;
+    if (lane == 0) L_e[lidx] = E;
+    barrier();
+    if (ladder_leader) {
+      exchange_ladder(ld_chain + lbase, ld_temp + lbase, ld_e + lbase, L, lad, lround, ch.exch_thresh,
+                      ch.exch_width, k0, k1, lexch);
+      ++lround;
+      if (ch.stop != nullptr && warp == 0) *ld_stop = *((volatile int*)ch.stop);
+    }
+    barrier();
+    if (*((volatile int*)L_stop)) break;
+  }
+
+  // write back
+  for (int s = lane; s < m; s += 32) {
+    ch.cols[(size_t)c * kMaxM + s] = (int16_t)cs[s];
+    ch.badness[(size_t)c * kMaxM + s] = bs[s];
+  }
+  if (lane == 0) {
+    ch.energy[c] = E;
+    ch.best_energy[c] = bestE;
+    ch.counter[c] = counter;
+    ch.accepted[c] = accepted;
+    if (err && ch.error_word) atomicOr(ch.error_word, err);
+    if (ch.global_best) atomicMin(ch.global_best, bestE);
+  }
+  if (ladder_leader) {
+    ch.ladder_round[lad] = lround;
+    ch.ladder_exchanges[lad] = lexch;
+  }
+  if (leader_cta) {
+    __syncthreads();  // leader threads finished their exchanges above
+    for (int i = threadIdx.x; i < n_lad_here * L; i += blockDim.x) {
+      const int gl = lad_first + i / L;
+      ch.chain_at[(size_t)gl * L + i % L] = ld_chain[i];
+      ch.temp_of[(size_t)gl * L + i % L] = ld_temp[i];
+    }
+  }
+  barrier();  // keep the leader's shared memory alive until every CTA is done with it
+}
+
+// Full recompute of every chain's energy (determinant count) and badness
+// (slope count) compared with the maintained values.  One warp per chain.
+constexpr int kAuditWarps = 4;
+
+__global__ void __launch_bounds__(kAuditWarps * 32) audit_kernel(const n3_chains ch, const uint16_t* __restrict__ g_lut,
+                                                                   int32_t* mismatch) {
+  extern __shared__ __align__(16) unsigned char smem[];
+  uint16_t* lut = reinterpret_cast<uint16_t*>(smem);
+  uint32_t* hist_all = reinterpret_cast<uint32_t*>(smem + TemperSmem::lut_bytes);
+  int* cs_all = reinterpret_cast<int*>(hist_all + kAuditWarps * kDirWords);
+  int* bs_all = cs_all + kAuditWarps * kMaxM;
+  for (int i = threadIdx.x; i < kLutSize; i += blockDim.x) lut[i] = g_lut[i];
+  for (int i = threadIdx.x; i < kAuditWarps * kDirWords; i += blockDim.x) hist_all[i] = 0u;
+  __syncthreads();
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  int* cs = cs_all + warp * kMaxM;
+  int* bs = bs_all + warp * kMaxM;
+  uint32_t* hist = hist_all + warp * kDirWords;
+  for (int c = blockIdx.x * kAuditWarps + warp; c < ch.n_chains; c += gridDim.x * kAuditWarps) {
+    const int n = ch.ladder_n[c / ch.ladder_size], m = 2 * n;
+    for (int s = lane; s < m; s += 32) cs[s] = ch.cols[(size_t)c * kMaxM + s];
+    __syncwarp();
+    const int e = warp_sum(det_state<false>(cs, n, lane, nullptr));
+    slope_state(cs, n, lut, hist, lane, bs);
+    __syncwarp();
+    int bad_ok = 1;
+    for (int s = lane; s < m; s += 32) bad_ok &= bs[s] == ch.badness[(size_t)c * kMaxM + s];
+    bad_ok = __all_sync(0xffffffffu, bad_ok);
+    if (lane == 0 && (e != ch.energy[c] || !bad_ok)) {
+      atomicAdd(mismatch, 1);
+      if (ch.error_word) atomicOr(ch.error_word, kErrAudit);
+    }
+    __syncwarp();
+  }
+}
+
+}  // namespace n3
+
+namespace n3host {
+
+static int check_chains(const n3_chains* ch) {
+  if (ch == nullptr) return set_error(N3_ERR_ARG, "null chains descriptor");
+  const int L = ch->ladder_size;
+  if (L < 2 || L > 64) return set_error(N3_ERR_ARG, "ladder_size %d outside [2, 64]", L);
+  if (ch->n_chains <= 0 || ch->n_chains % L)
+    return set_error(N3_ERR_ARG, "n_chains %d is not a positive multiple of ladder_size %d", ch->n_chains, L);
+  if (!ch->cols || !ch->badness || !ch->energy || !ch->best_energy || !ch->best_cols || !ch->temp_of ||
+      !ch->chain_at || !ch->counter || !ch->accepted || !ch->ladder_n || !ch->ladder_round ||
+      !ch->ladder_exchanges || !ch->acc_thresh || !ch->exch_thresh)
+    return set_error(N3_ERR_ARG, "null device pointer in chains descriptor");
+  if (ch->acc_width < 2 || ch->exch_width < 2) return set_error(N3_ERR_ARG, "threshold tables too narrow");
+  return N3_OK;
+}
+
+int temper_launch(const n3_chains* ch, const n3_temper_config* cfg, cudaStream_t st) {
+  N3_TRY(check_chains(ch));
+  if (cfg == nullptr) return set_error(N3_ERR_ARG, "null config");
+  const int L = ch->ladder_size, cpb = cfg->chains_per_block;
+  if (cpb < 1 || cpb > 16) return set_error(N3_ERR_ARG, "chains_per_block %d outside [1, 16]", cpb);
+  int cluster = 1;
+  if (cpb < L) {
+    if (L % cpb) return set_error(N3_ERR_ARG, "chains_per_block %d does not divide ladder_size %d", cpb, L);
+    cluster = L / cpb;
+    if (cluster > 8) return set_error(N3_ERR_ARG, "a ladder would span %d CTAs (max 8)", cluster);
+  } else if (cpb % L) {
+    return set_error(N3_ERR_ARG, "chains_per_block %d is not a multiple of ladder_size %d", cpb, L);
+  }
+  if (ch->n_chains % cpb) return set_error(N3_ERR_ARG, "n_chains not a multiple of chains_per_block");
+  if (cfg->rounds < 0 || cfg->round_proposals < 0 || cfg->round_sweeps < 0)
+    return set_error(N3_ERR_ARG, "negative round count or length");
+  if (!cfg->exchange && cfg->round_proposals == 0 && cfg->round_sweeps == 0)
+    return set_error(N3_ERR_ARG, "a round without exchange needs proposals");
+  N3_TRY(ensure_device_tables());
+  n3::TemperArgs args;
+  args.ch = *ch;
+  args.lut = dir_lut_device_ptr();
+  args.cfg = *cfg;
+  args.cluster = cluster;
+  const size_t smem = n3::TemperSmem::bytes(cpb);
+  N3_TRY(allow_smem(reinterpret_cast<const void*>(n3::temper_kernel), n3::TemperSmem::bytes(16)));
+  cudaLaunchConfig_t lc = {};
+  lc.gridDim = dim3(ch->n_chains / cpb);
+  lc.blockDim = dim3(cpb * 32);
+  lc.dynamicSmemBytes = smem;
+  lc.stream = st;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeClusterDimension;
+  attr[0].val.clusterDim.x = cluster;
+  attr[0].val.clusterDim.y = 1;
+  attr[0].val.clusterDim.z = 1;
+  lc.attrs = attr;
+  lc.numAttrs = 1;
+  const cudaError_t e = cudaLaunchKernelEx(&lc, n3::temper_kernel, args);
+  if (e != cudaSuccess) return set_error(N3_ERR_CUDA, "temper_kernel launch: %s", cudaGetErrorString(e));
+  return check_launch("temper_kernel");
+}
+
+}  // namespace n3host
+
+extern "C" {
+
+int n3_temper_run(const n3_chains* chains, const n3_temper_config* config, void* stream) {
+  return n3host::temper_launch(chains, config, (cudaStream_t)stream);
+}
+
+int n3_temper_audit(const n3_chains* chains, int32_t* mismatch, void* stream) {
+  N3_TRY(n3host::check_chains(chains));
+  if (mismatch == nullptr) return n3host::set_error(N3_ERR_ARG, "null mismatch counter");
+  N3_TRY(n3host::ensure_device_tables());
+  const n3_chains ch = *chains;
+  const size_t smem = n3::TemperSmem::lut_bytes +
+                      n3::kAuditWarps * (sizeof(uint32_t) * n3::kDirWords + 2 * sizeof(int) * n3::kMaxM);
+  N3_TRY(n3host::allow_smem(reinterpret_cast<const void*>(n3::audit_kernel), smem));
+  const int want = (ch.n_chains + n3::kAuditWarps - 1) / n3::kAuditWarps;
+  const int grid = want < n3host::sm_count() * 4 ? want : n3host::sm_count() * 4;
+  n3::audit_kernel<<<grid, n3::kAuditWarps * 32, smem, (cudaStream_t)stream>>>(ch, n3host::dir_lut_device_ptr(),
+                                                                                 mismatch);
+  return n3host::check_launch("audit_kernel");
+}
+
+}  // extern "C"
+
+namespace n3 {
+__global__ void clock_kernel(int64_t* out) { out[0] = (int64_t)global_ns(); }
+}  // namespace n3
+
+extern "C" int n3_device_clock_ns(int64_t* out, void* stream) {
+  if (out == nullptr) return n3host::set_error(N3_ERR_ARG, "null output");
+  n3::clock_kernel<<<1, 1, 0, (cudaStream_t)stream>>>(out);
+  return n3host::check_launch("clock_kernel");
+}

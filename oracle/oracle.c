@@ -388,3 +388,134 @@ int64_t n3o_det_score_points(const int32_t* rows, const int32_t* cols, int m, in
                 }
     return score;
 }
+
+/* ---------------------------------------------------------------------------
+ * Tempering replay (ladder_rounds, when given, is each ladder's round count).  Philox4x32-10 restated from Salmon et al., SC'11 (the
+ * paper's multipliers and Weyl constants), and the tempering schedule of the
+ * device kernel: per round, every chain makes `per_round` proposals (slots
+ * u = floor(r0*m/2^32), v = floor(r1*m/2^32) of the Philox block with counter
+ * (proposal index lo, hi, chain, 0x50000000) and key = seed), each scored by
+ * the reference's pair formulation (n3o_walk_delta, tempering.py:68-89) and
+ * accepted iff dE <= 0 or (dE < W and r2 < acc[temp][dE]); then each ladder
+ * exchanges neighbours (t, t+1) for t = round%2, round%2+2, ... with the
+ * reference's rule (tempering.py:178-184): swap when E(lower T) >= E(higher T),
+ * else iff the Philox word for (round, t, ladder, 0xE0000000) is below
+ * exch[t][E(higher T) - E(lower T)].
+ * ------------------------------------------------------------------------- */
+static void n3o_philox(uint32_t c[4], uint32_t k0, uint32_t k1) {
+    for (int r = 0; r < 10; ++r) {
+        const uint64_t p0 = (uint64_t)0xD2511F53u * c[0];
+        const uint64_t p1 = (uint64_t)0xCD9E8D57u * c[2];
+        const uint32_t y0 = (uint32_t)(p1 >> 32) ^ c[1] ^ k0, y1 = (uint32_t)p1;
+        const uint32_t y2 = (uint32_t)(p0 >> 32) ^ c[3] ^ k1, y3 = (uint32_t)p0;
+        c[0] = y0;
+        c[1] = y1;
+        c[2] = y2;
+        c[3] = y3;
+        k0 += 0x9E3779B9u;
+        k1 += 0xBB67AE85u;
+    }
+}
+
+void n3o_philox4x32_10(const uint32_t* ctr, uint32_t k0, uint32_t k1, uint32_t* out) {
+    uint32_t c[4] = {ctr[0], ctr[1], ctr[2], ctr[3]};
+    n3o_philox(c, k0, k1);
+    memcpy(out, c, sizeof(c));
+}
+
+typedef struct {
+    int C, L, stride;
+    int32_t *cols, *bad, *E, *bestE, *best_cols, *temp_of, *chain_at;
+    uint64_t* counter;
+    uint32_t* accepted;
+    const int32_t* ladder_n;
+    uint32_t *ladder_round, *ladder_exch;
+    const uint32_t* acc;
+    int W;
+    const uint32_t* exch;
+    int XW;
+    uint64_t seed;
+    int rounds, round_sweeps, round_proposals, exchange;
+    const int32_t* ladder_rounds;
+    int round;
+} n3o_temper_ctx;
+
+static void n3o_temper_chain_round(int c, void* arg) {
+    n3o_temper_ctx* T = (n3o_temper_ctx*)arg;
+    if (T->ladder_rounds && T->round >= T->ladder_rounds[c / T->L]) return;
+    const int n = T->ladder_n[c / T->L], m = 2 * n;
+    int32_t* cols = T->cols + (size_t)c * T->stride;
+    int32_t* bad = T->bad + (size_t)c * T->stride;
+    const int per = T->round_proposals > 0 ? T->round_proposals : T->round_sweeps * m;
+    const uint32_t* thr = T->acc + (size_t)T->temp_of[c] * T->W;
+    int32_t dbad[512];
+    for (int p = 0; p < per; ++p) {
+        const uint64_t k = T->counter[c]++;
+        uint32_t r[4] = {(uint32_t)k, (uint32_t)(k >> 32), (uint32_t)c, 0x50000000u};
+        n3o_philox(r, (uint32_t)T->seed, (uint32_t)(T->seed >> 32));
+        const int u = (int)(((uint64_t)r[0] * (uint32_t)m) >> 32);
+        const int v = (int)(((uint64_t)r[1] * (uint32_t)m) >> 32);
+        int32_t dE = 0;
+        if (!n3o_walk_delta(cols, n, u, v, &dE, dbad)) continue;
+        if (!(dE <= 0 || (dE < T->W && r[2] < thr[dE]))) continue;
+        const int32_t t = cols[u];
+        cols[u] = cols[v];
+        cols[v] = t;
+        for (int s = 0; s < m; ++s) bad[s] += dbad[s];
+        T->E[c] += dE;
+        T->accepted[c] += 1;
+        if (T->E[c] < T->bestE[c]) {
+            T->bestE[c] = T->E[c];
+            memcpy(T->best_cols + (size_t)c * T->stride, cols, sizeof(int32_t) * (size_t)m);
+        }
+    }
+}
+
+static void n3o_temper_exchange(n3o_temper_ctx* T, int lad) {
+    const int L = T->L;
+    int32_t* at = T->chain_at + (size_t)lad * L;
+    int32_t* tof = T->temp_of + (size_t)lad * L;
+    const int32_t* e = T->E + (size_t)lad * L;
+    const uint32_t round = T->ladder_round[lad];
+    for (int t = (int)(round & 1u); t < L - 1; t += 2) {
+        const int a = at[t], b = at[t + 1];
+        const int D = e[a] - e[b];
+        int swap = D >= 0;
+        if (!swap) {
+            uint32_t r[4] = {round, (uint32_t)t, (uint32_t)lad, 0xE0000000u};
+            n3o_philox(r, (uint32_t)T->seed, (uint32_t)(T->seed >> 32));
+            swap = -D < T->XW && r[0] < T->exch[(size_t)t * T->XW + (-D)];
+        }
+        if (swap) {
+            at[t] = b;
+            at[t + 1] = a;
+            tof[a] = t + 1;
+            tof[b] = t;
+            T->ladder_exch[lad] += 1;
+        }
+    }
+    T->ladder_round[lad] = round + 1;
+}
+
+/* Replays `rounds` rounds of the device tempering kernel on the CPU.  Arrays
+ * follow the n3_chains layout (columns widened to int32, row stride `stride`). */
+void n3o_temper_run(int C, int L, int stride, int32_t* cols, int32_t* bad, int32_t* E, int32_t* bestE,
+                    int32_t* best_cols, int32_t* temp_of, int32_t* chain_at, uint64_t* counter, uint32_t* accepted,
+                    const int32_t* ladder_n, uint32_t* ladder_round, uint32_t* ladder_exch, const uint32_t* acc,
+                    int W, const uint32_t* exch, int XW, uint64_t seed, int rounds, int round_sweeps,
+                    int round_proposals, int exchange, const int32_t* ladder_rounds, int threads) {
+    n3o_temper_ctx T = {C, L, stride, cols, bad, E, bestE, best_cols, temp_of, chain_at, counter, accepted,
+                        ladder_n, ladder_round, ladder_exch, acc, W, exch, XW, seed, rounds, round_sweeps,
+                        round_proposals, exchange, ladder_rounds, 0};
+    int max_rounds = rounds;
+    if (ladder_rounds)
+        for (int lad = 0; lad < C / L; ++lad)
+            if (ladder_rounds[lad] > max_rounds) max_rounds = ladder_rounds[lad];
+    for (int r = 0; r < max_rounds; ++r) {
+        T.round = r;
+        n3o_parallel_for(C, threads, n3o_temper_chain_round, &T);
+        if (exchange)
+            for (int lad = 0; lad < C / L; ++lad)
+                if (!ladder_rounds || r < ladder_rounds[lad]) n3o_temper_exchange(&T, lad);
+    }
+}

@@ -140,3 +140,45 @@ def score_columns(cols) -> tuple[int, np.ndarray]:
     c = _c32(cols)
     bad = np.zeros(len(c), np.int32)
     return int(lib().n3o_score_columns(c, len(c) // 2, bad.ctypes.data)), bad
+
+
+def philox4x32_10(ctr, key0: int, key1: int) -> list[int]:
+    """Philox4x32-10 (Salmon et al., SC'11) restated in oracle.c."""
+    L = lib()
+    f = L.n3o_philox4x32_10
+    f.restype = None
+    f.argtypes = [np.ctypeslib.ndpointer(dtype=np.uint32, flags="C_CONTIGUOUS"), ctypes.c_uint32, ctypes.c_uint32,
+                  np.ctypeslib.ndpointer(dtype=np.uint32, flags="C_CONTIGUOUS")]
+    out = np.zeros(4, np.uint32)
+    f(np.ascontiguousarray(ctr, dtype=np.uint32), key0 & 0xFFFFFFFF, key1 & 0xFFFFFFFF, out)
+    return [int(x) for x in out]
+
+
+def temper_run(state: dict, *, ladder_size: int, acc, exch, seed: int, rounds: int = 0, round_sweeps: int = 0,
+               round_proposals: int = 0, exchange: bool = True, ladder_rounds=None, threads: int = 0) -> dict:
+    """CPU replay of the device tempering kernel (see n3o_temper_run in oracle.c).
+
+    ``state`` holds numpy arrays in the layout of the device chains (columns
+    [C, stride]); a replayed copy is returned."""
+    L = lib()
+    f = L.n3o_temper_run
+    f.restype = None
+    P = ctypes.c_void_p
+    f.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_int] + [P] * 13 + [ctypes.c_int, P, ctypes.c_int,
+                                                                         ctypes.c_uint64] + [ctypes.c_int] * 4 + [P, ctypes.c_int]
+    s = {k: np.array(v, copy=True) for k, v in state.items()}
+    conv = {"cols": np.int32, "bad": np.int32, "E": np.int32, "bestE": np.int32, "best_cols": np.int32,
+            "temp_of": np.int32, "chain_at": np.int32, "counter": np.uint64, "accepted": np.uint32,
+            "ladder_n": np.int32, "ladder_round": np.uint32, "ladder_exch": np.uint32}
+    for k, dt in conv.items():
+        s[k] = np.ascontiguousarray(s[k], dtype=dt)
+    acc = np.ascontiguousarray(acc, dtype=np.uint32)
+    exch = np.ascontiguousarray(exch, dtype=np.uint32)
+    lr = None if ladder_rounds is None else np.ascontiguousarray(ladder_rounds, dtype=np.int32)
+    C, stride = s["cols"].shape
+    f(C, ladder_size, stride, *(s[k].ctypes.data for k in ["cols", "bad", "E", "bestE", "best_cols", "temp_of",
+                                                            "chain_at", "counter", "accepted", "ladder_n",
+                                                            "ladder_round", "ladder_exch"]),
+      acc.ctypes.data, acc.shape[1], exch.ctypes.data, exch.shape[1], seed & 0xFFFFFFFFFFFFFFFF, rounds,
+      round_sweeps, round_proposals, int(exchange), lr.ctypes.data if lr is not None else None, threads)
+    return s
