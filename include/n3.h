@@ -46,6 +46,12 @@ int n3_version(void);
 /* Message of the last failing call on this host thread ("" if none). */
 const char* n3_last_error(void);
 
+/* One-time set-up on the current device: builds the device-resident tables
+ * and opts the kernels into their shared-memory carve-outs.  Every entry
+ * point does what it needs of this lazily; call it once first when the
+ * first launches on a device are to be captured into a CUDA graph. */
+int n3_init_device(void);
+
 /* ---------------------------------------------------------------------------
  * (a) Population scoring.
  * ------------------------------------------------------------------------- */
@@ -185,6 +191,59 @@ int n3_temper_run(const n3_chains* chains, const n3_temper_config* config, void*
  * *mismatch (device int32).  The reference's TemperingChains.validate
  * (src/no_three_75/tempering.py:193-204), on the device. */
 int n3_temper_audit(const n3_chains* chains, int32_t* mismatch, void* stream);
+
+/* ---------------------------------------------------------------------------
+ * (d) Learned move proposal (no reference counterpart: the reference's walk
+ * proposes uniformly, src/no_three_75/tempering.py:50-56).
+ *
+ * A 192 -> 256 -> 256 -> 1 MLP (ReLU) with bf16 tensor-core weights and fp32
+ * accumulation ranks 128 candidate swaps per chain per step by predicted dE;
+ * one candidate is drawn from softmax(-pred / T) and accepted with the exact
+ * integer delta and the chain's Metropolis thresholds.  Every step pushes the
+ * chosen candidate's (features, exact dE) to a ring buffer; training draws
+ * batches from it (MSE on dE/16, Adam) with hand-written kernels.
+ * Feature layout (float): badness of u, v, u^1, v^1 (/16); their rows and
+ * columns (/n); the chain's 150 slot badness values (/16); zero padding.
+ * ------------------------------------------------------------------------- */
+typedef struct n3_mlp {
+  float* params;        /* [n3_mlp_param_count()] fp32: W1[256][192] b1[256] W2[256][256] b2[256] w3[256] b3 */
+  uint8_t* w2_img;      /* 131072 B: bf16 W2 in the tensor-core shared-memory layout (n3_mlp_pack) */
+  uint8_t* w1a_img;     /* 8192 B: bf16 candidate columns of W1, tensor-core layout */
+  uint8_t* a1_img;      /* [C][4096 B]: candidate features of each chain's 128 candidates (bf16) */
+  float* badn;          /* [C][150]: chain features (badness / 16) */
+  float* c1;            /* [C][256]: chain part of layer 1 (W1b x + b1) */
+  int32_t* cand;        /* [C][128]: u | v << 8 | legal << 31 */
+  float* pred;          /* [C][128]: predicted dE */
+  uint16_t* rb_feat;    /* [capacity][12] bf16 candidate features */
+  uint8_t* rb_bad;      /* [capacity][150] chain badness (clamped to 255) */
+  int16_t* rb_dE;       /* [capacity] exact dE */
+  int64_t rb_capacity;
+  float* stats;         /* [4]: sum |pred - dE|, proposals, accepted, sum of accepted dE */
+  uint64_t* counters;   /* [2]: learned steps taken (ring position, candidate stream), Adam steps taken */
+  float* loss_out;      /* [1] sum of squared errors of the last training batch, or NULL */
+  uint32_t* error_word; /* device error bits (8: a bounded tensor-core wait expired) */
+} n3_mlp;
+
+int n3_mlp_param_count(void);
+/* Floats of training scratch needed for a batch of `batch` tuples. */
+int n3_mlp_scratch_floats(int batch);
+/* Rebuilds w2_img and w1a_img from params. */
+int n3_mlp_pack(const n3_mlp* mlp, void* stream);
+/* Draws 128 candidates per chain for the current step (Philox keyed by seed,
+ * counter = step, chain, candidate), writes a1_img, badn, cand, and c1 (the
+ * chain part of layer 1, one GEMM over all chains). */
+int n3_mlp_candidates(const n3_chains* chains, const n3_mlp* mlp, uint64_t seed, void* stream);
+/* pred[t][j] for `tiles` tiles of 128 candidates from a1_img and c1 (tcgen05). */
+int n3_mlp_infer(const n3_mlp* mlp, int tiles, void* stream);
+/* Samples, scores exactly, accepts and records one move per chain, then
+ * advances the step counter.  temps: the ladder's L temperatures (device). */
+int n3_mlp_step(const n3_chains* chains, const n3_mlp* mlp, const float* temps, uint64_t seed, void* stream);
+/* One Adam step on a batch drawn from the ring slots recorded so far (all
+ * counters live on the device, so the call is graph-capturable); scratch
+ * holds n3_mlp_scratch_floats(batch) floats, grads/adam_m/adam_v
+ * n3_mlp_param_count() floats each. */
+int n3_mlp_train(const n3_mlp* mlp, int n_chains, int batch, float lr, uint64_t seed, float* scratch, float* grads,
+                 float* adam_m, float* adam_v, void* stream);
 
 /* Device clock (%globaltimer, ns) written to *out (device int64) in stream
  * order; used to time a run to its first target hit on the device. */

@@ -32,6 +32,7 @@ _F = ctypes.c_float
 _SIGNATURES: dict[str, list] = {
     "n3_version": [],
     "n3_last_error": [],
+    "n3_init_device": [],
     "n3_score_population": [_P, _P, _I, _I, _P, _P, _P],
     "n3_score_columns": [_P, _I, _I, _P, _P, _P],
     "n3_score_slope": [_P, _I, _I, _P, _P, _P],
@@ -49,6 +50,7 @@ _SIGNATURES: dict[str, list] = {
 _RESTYPE = {"n3_last_error": ctypes.c_char_p}
 
 _lib = None
+_ready: set[int] = set()
 
 
 def build(force: bool = False) -> Path:
@@ -130,8 +132,12 @@ def require_device():
     t = torch()
     if not t.cuda.is_available() or t.cuda.device_count() < 1:
         raise RuntimeError("no CUDA device is available")
-    lib()
-    return t.device("cuda", t.cuda.current_device())
+    L = lib()
+    dev = t.cuda.current_device()
+    if dev not in _ready:
+        check(L.n3_init_device(), "n3_init_device")
+        _ready.add(dev)
+    return t.device("cuda", dev)
 
 
 def stream_ptr(stream=None) -> int:

@@ -89,9 +89,24 @@ int sm_count() {
 
 }  // namespace n3host
 
+namespace n3host {
+int prepare_score();
+int prepare_delta();
+int prepare_tempering();
+int prepare_mlp();
+}  // namespace n3host
+
 extern "C" {
 
 int n3_version(void) { return 100; }
+
+int n3_init_device(void) {
+  N3_TRY(n3host::ensure_device_tables());
+  N3_TRY(n3host::prepare_score());
+  N3_TRY(n3host::prepare_delta());
+  N3_TRY(n3host::prepare_tempering());
+  return n3host::prepare_mlp();
+}
 
 const char* n3_last_error(void) { return n3host::g_last_error.c_str(); }
 

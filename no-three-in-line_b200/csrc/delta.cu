@@ -286,6 +286,13 @@ static int prepare(K kernel) {
   return allow_smem(reinterpret_cast<const void*>(kernel), n3::DeltaSmem::bytes);
 }
 
+int prepare_delta() {
+  N3_TRY(prepare(n3::swap_delta_kernel<true>));
+  N3_TRY(prepare(n3::swap_delta_kernel<false>));
+  N3_TRY(prepare(n3::partner_scores_kernel<true>));
+  return prepare(n3::partner_scores_kernel<false>);
+}
+
 static int check_state_args(int B, int n, const void* cols) {
   if (n < 2 || n > N3_MAX_N) return set_error(N3_ERR_RANGE, "n=%d outside [2, %d]", n, N3_MAX_N);
   if (B < 0) return set_error(N3_ERR_ARG, "negative batch size %d", B);

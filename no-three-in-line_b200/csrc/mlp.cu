@@ -1,0 +1,771 @@
+// (d) Learned move proposal: a 192 -> 256 -> 256 -> 1 MLP (bf16 weights,
+// fp32 accumulation) that ranks candidate swaps by predicted dE, trained online
+// on (features, exact dE) tuples emitted by the run.  No reference counterpart
+// (the reference proposes uniformly, src/no_three_75/tempering.py:50-56).
+//
+// Features of a candidate (u, v) of a chain, all float, 192 wide:
+//   [0..3]    badness of u, v, u^1, v^1, / 16
+//   [4..7]    rows of u, v, u^1, v^1, / n
+//   [8..11]   columns of u, v, u^1, v^1, / n
+//   [12..161] the chain's per-slot badness (150 slots, zero beyond 2n), / 16
+//   [162..191] zero
+// Layer 1 is split accordingly: W1 = [W1a | W1b].  The 150 chain features are
+// shared by all 128 candidates of a chain, so W1b x + b1 is computed once per
+// chain (candidates_kernel) and added in the epilogue of the per-candidate
+// K = 16 tensor-core product.  Inference per chain is one M = 128 tile:
+//   D1 = A1 (128 x 16) W1a^T  -> + chain part, ReLU, bf16 -> A2 (shared memory)
+//   D2 = A2 (128 x 256) W2^T  -> + b2, ReLU, . w3 + b3 -> predicted dE
+// both on tcgen05 with fp32 accumulators in tensor memory.
+// Training (SIMT fp32, hand-written GEMMs) uses MSE on dE / kTargetScale with
+// Adam; the packed bf16 images are rebuilt after each update.
+#include <cuda_bf16.h>
+#include <math.h>
+
+#include "chain_move.cuh"
+#include "dirs.cuh"
+#include "n3_common.cuh"
+#include "philox.cuh"
+#include "umma.cuh"
+
+namespace n3 {
+namespace mlp {
+
+constexpr int kCand = 128;    // candidates per chain per step (one M tile)
+constexpr int kIn = 192;      // input width
+constexpr int kCandFeat = 12; // per-candidate features
+constexpr int kChainFeat = 150;
+constexpr int kH = 256;
+constexpr float kTargetScale = 16.0f;
+// Parameter buffer layout (fp32): W1 [256][192], b1, W2 [256][256], b2, w3, b3.
+constexpr int oW1 = 0;
+constexpr int oB1 = oW1 + kH * kIn;
+constexpr int oW2 = oB1 + kH;
+constexpr int oB2 = oW2 + kH * kH;
+constexpr int oW3 = oB2 + kH;
+constexpr int oB3 = oW3 + kH;
+constexpr int kParams = oB3 + 4;  // padded to a multiple of 4
+
+// Inference shared-memory map (offsets from a 1024-aligned base).
+constexpr uint32_t sW2 = 0;                       // SW128 image, 4 x [256 x 128 B]
+constexpr uint32_t sA2 = sW2 + 4 * kH * 128;      // SW128, 4 x [128 x 128 B]
+constexpr uint32_t sW1a = sA2 + 4 * kCand * 128;  // INTERLEAVE K=16, 256 rows
+constexpr uint32_t sA1 = sW1a + kH * 32;          // INTERLEAVE K=16, 128 rows
+constexpr uint32_t sC1 = sA1 + kCand * 32;        // fp32[256] chain part of layer 1
+constexpr uint32_t sB2 = sC1 + kH * 4;
+constexpr uint32_t sW3 = sB2 + kH * 4;
+constexpr uint32_t sBar = sW3 + kH * 4;           // mbarrier (8 B) + TMEM address (4 B) + abort flag
+constexpr uint32_t kInferSmem = sBar + 64 + 1024; // + alignment slack
+constexpr uint32_t kWaitTries = 1u << 24;
+
+__device__ __forceinline__ uint16_t bf16_bits(float x) {
+  const __nv_bfloat16 h = __float2bfloat16_rn(x);
+  return *reinterpret_cast<const uint16_t*>(&h);
+}
+
+// ---------------------------------------------------------------------------
+// Packing: fp32 parameters -> bf16 tensor-core images + transposed W1b.
+// ---------------------------------------------------------------------------
+__global__ void pack_kernel(const float* __restrict__ P, uint8_t* __restrict__ w2_img, uint8_t* __restrict__ w1a_img) {
+  const int tid = blockIdx.x * blockDim.x + threadIdx.x;
+  const int stride = gridDim.x * blockDim.x;
+  for (int i = tid; i < kH * kH; i += stride) {  // W2[n][k]: row n of the B operand, K index k
+    const int n = i / kH, k = i % kH;
+    *reinterpret_cast<uint16_t*>(w2_img + umma::sw128_offset(n, k, kH)) = bf16_bits(P[oW2 + n * kH + k]);
+  }
+  for (int i = tid; i < kH * 16; i += stride) {
+    const int n = i / 16, k = i % 16;
+    const float w = k < kCandFeat ? P[oW1 + n * kIn + k] : 0.0f;
+    *reinterpret_cast<uint16_t*>(w1a_img + umma::inter16_offset(n, k)) = bf16_bits(w);
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Candidates: per chain, 128 Philox-drawn (u, v) slot pairs and their features
+// as the INTERLEAVE A1 image, plus the chain's scaled badness row (the input
+// of the chain part of layer 1, computed for all chains by one GEMM).
+// ---------------------------------------------------------------------------
+struct CandArgs {
+  const int16_t* cols;     // [C][150]
+  const int32_t* badness;  // [C][150]
+  const int32_t* ladder_n; // [C/L]
+  int ladder_size, n_chains;
+  uint8_t* a1_img;         // [C][128 rows x 32 B]
+  float* badn;             // [C][150] badness / 16
+  int32_t* cand;           // [C][128]: u | v << 8 | legal << 31
+  const uint64_t* step;    // device step counter
+  uint32_t k0, k1;
+};
+
+__device__ __forceinline__ void candidate_features(const int16_t* cols, const int32_t* bad, int n, int u, int v,
+                                                   float (&f)[kCandFeat]) {
+  const float inv_n = 1.0f / (float)n;
+  const int s[4] = {u, v, u ^ 1, v ^ 1};
+#pragma unroll
+  for (int i = 0; i < 4; ++i) {
+    f[i] = (float)bad[s[i]] * (1.0f / 16.0f);
+    f[4 + i] = (float)(s[i] >> 1) * inv_n;
+    f[8 + i] = (float)cols[s[i]] * inv_n;
+  }
+}
+
+__global__ void __launch_bounds__(kCand) candidates_kernel(const CandArgs A) {
+  const int c = blockIdx.x;
+  const int n = A.ladder_n[c / A.ladder_size], m = 2 * n;
+  const int16_t* cols = A.cols + (size_t)c * kChainFeat;
+  const int32_t* bad = A.badness + (size_t)c * kChainFeat;
+  for (int s = threadIdx.x; s < kChainFeat; s += blockDim.x)
+    A.badn[(size_t)c * kChainFeat + s] = s < m ? (float)bad[s] * (1.0f / 16.0f) : 0.f;
+  {
+    const int j = threadIdx.x;
+    const uint64_t step = *A.step;
+    const U4 r = philox4x32_10(U4{(uint32_t)step, (uint32_t)(step >> 32), (uint32_t)c, kTagCandidate | (uint32_t)j},
+                               A.k0, A.k1);
+    const int u = (int)__umulhi(r.x, (unsigned)m), v = (int)__umulhi(r.y, (unsigned)m);
+    const int cu = cols[u], cv = cols[v];
+    const bool legal = (u >> 1) != (v >> 1) && cu != cv && cols[u ^ 1] != cv && cols[v ^ 1] != cu;
+    float f[kCandFeat];
+    candidate_features(cols, bad, n, u, v, f);
+    uint8_t* img = A.a1_img + (size_t)c * (kCand * 32);
+#pragma unroll
+    for (int k = 0; k < 16; ++k)
+      *reinterpret_cast<uint16_t*>(img + umma::inter16_offset(j, k)) = bf16_bits(k < kCandFeat ? f[k] : 0.0f);
+    A.cand[(size_t)c * kCand + j] = u | (v << 8) | (legal ? (1 << 31) : 0);
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Tensor-core inference: one persistent CTA per SM, 4 warps, one chain tile
+// (128 candidates) per iteration.
+// ---------------------------------------------------------------------------
+struct InferArgs {
+  const uint8_t* a1_img;  // [T][4096 B]
+  const float* c1;        // [T][256]
+  const uint8_t* w2_img;  // 128 KB
+  const uint8_t* w1a_img; // 8 KB
+  const float* P;         // b2, w3, b3
+  float* pred;            // [T][128]
+  int tiles;
+  uint32_t* error_word;
+};
+
+__device__ __forceinline__ void copy16(uint8_t* dst, const uint8_t* src, int bytes, int tid, int nthreads) {
+  const uint4* s = reinterpret_cast<const uint4*>(src);
+  uint4* d = reinterpret_cast<uint4*>(dst);
+  for (int i = tid; i < bytes / 16; i += nthreads) d[i] = s[i];
+}
+
+__global__ void __launch_bounds__(128, 1) infer_kernel(const InferArgs A) {
+  extern __shared__ uint8_t smem_raw[];
+  const uint32_t raw = umma::smem_addr(smem_raw);
+  uint8_t* sm = smem_raw + ((1024u - (raw & 1023u)) & 1023u);  // 1024-aligned base
+  const uint32_t base = umma::smem_addr(sm);
+  const int tid = threadIdx.x, warp = tid >> 5;
+  float* c1s = reinterpret_cast<float*>(sm + sC1);
+  float* b2s = reinterpret_cast<float*>(sm + sB2);
+  float* w3s = reinterpret_cast<float*>(sm + sW3);
+  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(sm + sBar + 8);
+  int* abort_flag = reinterpret_cast<int*>(sm + sBar + 16);
+  const uint32_t mbar = base + sBar;
+
+  copy16(sm + sW2, A.w2_img, 4 * kH * 128, tid, blockDim.x);
+  copy16(sm + sW1a, A.w1a_img, kH * 32, tid, blockDim.x);
+  for (int i = tid; i < kH; i += blockDim.x) {
+    b2s[i] = A.P[oB2 + i];
+    w3s[i] = A.P[oW3 + i];
+  }
+  const float b3 = A.P[oB3];
+  if (warp == 0) {
+    umma::tmem_alloc(base + sBar + 8, 256);
+    umma::tmem_relinquish();
+  }
+  if (tid == 0) {
+    umma::mbar_init(mbar, 1);
+    umma::mbar_fence_init();
+    *abort_flag = 0;
+  }
+  umma::fence_before_sync();
+  __syncthreads();
+  umma::fence_after_sync();
+  const uint32_t tmem = *tmem_slot;
+  const uint32_t lane_base = tmem + ((uint32_t)(32 * warp) << 16);
+  const uint32_t idesc = umma::idesc_bf16_f32(128, 256);
+  uint32_t phase = 0;
+  const int row = tid;  // candidate row = TMEM lane
+
+  for (int t = blockIdx.x; t < A.tiles; t += gridDim.x) {
+    copy16(sm + sA1, A.a1_img + (size_t)t * (kCand * 32), kCand * 32, tid, blockDim.x);
+    for (int i = tid; i < kH; i += blockDim.x) c1s[i] = A.c1[(size_t)t * kH + i];
+    umma::fence_async_smem();
+    umma::fence_before_sync();
+    __syncthreads();
+    umma::fence_after_sync();
+    if (tid == 0) {
+      umma::mma_bf16(tmem, umma::desc_interleave(base + sA1, 128, 256), umma::desc_interleave(base + sW1a, 128, 256),
+                     idesc, 0u);
+      umma::commit(mbar);
+    }
+    if (!umma::mbar_wait(mbar, phase, kWaitTries)) atomicExch(abort_flag, 1);
+    phase ^= 1u;
+    umma::fence_after_sync();
+    __syncthreads();
+    if (*abort_flag) break;
+    // epilogue 1: h1 = relu(D1 + chain part) -> bf16 -> A2 (SW128)
+#pragma unroll 1
+    for (int j = 0; j < kH / 32; ++j) {
+      float v[32];
+      umma::tmem_ld32(lane_base + 32 * j, v);
+#pragma unroll
+      for (int q = 0; q < 4; ++q) {  // 8 values -> one 16-byte chunk
+        uint32_t w[4];
+#pragma unroll
+        for (int e = 0; e < 4; ++e) {
+          const int k0 = 32 * j + 8 * q + 2 * e;
+          const float h0 = fmaxf(v[8 * q + 2 * e] + c1s[k0], 0.f);
+          const float h1 = fmaxf(v[8 * q + 2 * e + 1] + c1s[k0 + 1], 0.f);
+          w[e] = (uint32_t)bf16_bits(h0) | ((uint32_t)bf16_bits(h1) << 16);
+        }
+        *reinterpret_cast<uint4*>(sm + sA2 + umma::sw128_offset(row, 32 * j + 8 * q, kCand)) =
+            make_uint4(w[0], w[1], w[2], w[3]);
+      }
+    }
+    umma::fence_async_smem();
+    umma::fence_before_sync();
+    __syncthreads();
+    umma::fence_after_sync();
+    if (tid == 0) {
+#pragma unroll
+      for (int s = 0; s < kH / 16; ++s) {
+        const uint32_t koff = (uint32_t)(s & 3) * 32u;  // K = 16 step inside a 64-wide slice
+        const uint64_t ad = umma::desc_sw128(base + sA2 + (uint32_t)(s >> 2) * (kCand * 128) + koff);
+        const uint64_t bd = umma::desc_sw128(base + sW2 + (uint32_t)(s >> 2) * (kH * 128) + koff);
+        umma::mma_bf16(tmem, ad, bd, idesc, s > 0 ? 1u : 0u);
+      }
+      umma::commit(mbar);
+    }
+    if (!umma::mbar_wait(mbar, phase, kWaitTries)) atomicExch(abort_flag, 1);
+    phase ^= 1u;
+    umma::fence_after_sync();
+    __syncthreads();
+    if (*abort_flag) break;
+    // epilogue 2: relu(D2 + b2) . w3 + b3
+    float acc = b3;
+#pragma unroll 1
+    for (int j = 0; j < kH / 32; ++j) {
+      float v[32];
+      umma::tmem_ld32(lane_base + 32 * j, v);
+#pragma unroll
+      for (int e = 0; e < 32; ++e) acc = fmaf(fmaxf(v[e] + b2s[32 * j + e], 0.f), w3s[32 * j + e], acc);
+    }
+    A.pred[(size_t)t * kCand + row] = acc * kTargetScale;
+    umma::fence_before_sync();
+    __syncthreads();
+  }
+  if (*abort_flag && tid == 0) {
+    if (A.error_word) atomicOr(A.error_word, kErrTimeout);
+    umma::mbar_wait(mbar, phase ^ 1u, kWaitTries);  // bounded wait for the MMA still in flight
+  }
+  umma::fence_before_sync();
+  __syncthreads();
+  if (warp == 0) {
+    umma::fence_after_sync();
+    umma::tmem_dealloc(tmem, 256);
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Learned step: sample one candidate per chain from softmax(-pred / T), score
+// it exactly, Metropolis-accept with the chain's threshold row, update the
+// state and badness, and push the (features, exact dE) tuple to the ring.
+// One warp per chain, state in shared memory (as in the tempering kernel).
+// ---------------------------------------------------------------------------
+struct StepArgs {
+  n3_chains ch;
+  const uint16_t* lut;
+  const float* temps;     // [L] ladder temperatures
+  const int32_t* cand;    // [C][128]
+  const float* pred;      // [C][128]
+  const uint64_t* step;   // device step counter
+  uint32_t k0, k1;
+  // ring buffer
+  uint16_t* rb_feat;      // [cap][12] bf16
+  uint8_t* rb_bad;        // [cap][150]
+  int16_t* rb_dE;         // [cap]
+  int64_t rb_cap;
+  float* stats;           // [4]: sum |pred - dE|, count, accepted, sum dE accepted
+};
+
+constexpr int kStepWarps = 16;
+
+__global__ void __launch_bounds__(kStepWarps * 32, 1) learned_step_kernel(const StepArgs A) {
+  extern __shared__ __align__(16) unsigned char smem[];
+  const n3_chains& ch = A.ch;
+  uint16_t* lut = reinterpret_cast<uint16_t*>(smem);
+  uint32_t* hist_all = reinterpret_cast<uint32_t*>(smem + ((sizeof(uint16_t) * kLutSize + 15) / 16) * 16);
+  int* cs_all = reinterpret_cast<int*>(hist_all + kStepWarps * kDirWords);
+  int* bs_all = cs_all + kStepWarps * kMaxM;
+  for (int i = threadIdx.x; i < kLutSize; i += blockDim.x) lut[i] = A.lut[i];
+  for (int i = threadIdx.x; i < kStepWarps * kDirWords; i += blockDim.x) hist_all[i] = 0u;
+  __syncthreads();
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int c = blockIdx.x * kStepWarps + warp;
+  if (c >= ch.n_chains) return;  // no block-level barrier follows
+  const int L = ch.ladder_size;
+  const int n = ch.ladder_n[c / L], m = 2 * n;
+  int* cs = cs_all + warp * kMaxM;
+  int* bs = bs_all + warp * kMaxM;
+  uint32_t* hist = hist_all + warp * kDirWords;
+  for (int s = lane; s < m; s += 32) {
+    cs[s] = ch.cols[(size_t)c * kMaxM + s];
+    bs[s] = ch.badness[(size_t)c * kMaxM + s];
+  }
+  const int temp = ch.temp_of[c];
+  const float T = A.temps[temp];
+  // softmax(-pred / T) over the legal candidates, sampled by inverse CDF
+  float logit[kCand / 32];
+  float mx = -INFINITY;
+#pragma unroll
+  for (int q = 0; q < kCand / 32; ++q) {
+    const int j = lane + 32 * q;
+    const int cw = A.cand[(size_t)c * kCand + j];
+    logit[q] = cw < 0 ? -A.pred[(size_t)c * kCand + j] / T : -INFINITY;
+    mx = fmaxf(mx, logit[q]);
+  }
+#pragma unroll
+  for (int o = 16; o; o >>= 1) mx = fmaxf(mx, __shfl_xor_sync(0xffffffffu, mx, o));
+  const uint64_t step = *A.step;
+  const U4 r = philox4x32_10(U4{(uint32_t)step, (uint32_t)(step >> 32), (uint32_t)c, kTagCandidate | 0xFFFFu},
+                             A.k0, A.k1);
+  int chosen = -1;
+  if (mx > -INFINITY) {
+    float w[kCand / 32], tot = 0.f;
+#pragma unroll
+    for (int q = 0; q < kCand / 32; ++q) {
+      w[q] = logit[q] > -INFINITY ? __expf(logit[q] - mx) : 0.f;
+      tot += w[q];
+    }
+    // inclusive prefix over lanes of the per-lane totals (candidate order j = lane + 32 q, by q then lane)
+    float laneq[kCand / 32];
+#pragma unroll
+    for (int q = 0; q < kCand / 32; ++q) {
+      float x = w[q];
+#pragma unroll
+      for (int o = 1; o < 32; o <<= 1) {
+        const float y = __shfl_up_sync(0xffffffffu, x, o);
+        if (lane >= o) x += y;
+      }
+      laneq[q] = x;  // prefix within block q
+    }
+    float qtot[kCand / 32], acc = 0.f;
+#pragma unroll
+    for (int q = 0; q < kCand / 32; ++q) {
+      qtot[q] = __shfl_sync(0xffffffffu, laneq[q], 31);
+      acc += qtot[q];
+    }
+    const float target = ((float)(r.x >> 8) + 0.5f) * (1.0f / 16777216.0f) * acc;
+    float before = 0.f;
+    int pick = -1;
+#pragma unroll
+    for (int q = 0; q < kCand / 32; ++q) {
+      if (pick < 0 && target < before + qtot[q]) {
+        const unsigned hit = __ballot_sync(0xffffffffu, w[q] > 0.f && before + laneq[q] > target);
+        if (hit) pick = 32 * q + (__ffs(hit) - 1);
+      }
+      before += qtot[q];
+    }
+    if (pick < 0) {  // rounding at the top end: take the last legal candidate
+#pragma unroll
+      for (int q = 0; q < kCand / 32; ++q) {
+        const unsigned hit = __ballot_sync(0xffffffffu, w[q] > 0.f);
+        if (hit) pick = 32 * q + (31 - __clz(hit));
+      }
+    }
+    chosen = pick;
+  }
+  __syncwarp();
+  int E = ch.energy[c];
+  uint32_t err = 0;
+  if (chosen >= 0) {
+    const int cw = A.cand[(size_t)c * kCand + chosen];
+    const int u = cw & 0xFF, v = (cw >> 8) & 0xFF;
+    const float p = A.pred[(size_t)c * kCand + chosen];
+    // tuple: features of the state before the move
+    const int64_t slot = (int64_t)((step * (uint64_t)ch.n_chains + (uint64_t)c) % (uint64_t)A.rb_cap);
+    if (lane == 0) {
+      float f[kCandFeat];
+      const int sidx[4] = {u, v, u ^ 1, v ^ 1};
+      const float inv_n = 1.0f / (float)n;
+#pragma unroll
+      for (int i = 0; i < 4; ++i) {
+        f[i] = (float)bs[sidx[i]] * (1.0f / 16.0f);
+        f[4 + i] = (float)(sidx[i] >> 1) * inv_n;
+        f[8 + i] = (float)cs[sidx[i]] * inv_n;
+      }
+#pragma unroll
+      for (int i = 0; i < kCandFeat; ++i) A.rb_feat[slot * kCandFeat + i] = bf16_bits(f[i]);
+    }
+    for (int s = lane; s < kChainFeat; s += 32)
+      A.rb_bad[slot * kChainFeat + s] = (uint8_t)(s < m ? min(bs[s], 255) : 0);
+    __syncwarp();
+    const uint32_t* thr = ch.acc_thresh + (size_t)temp * ch.acc_width;
+    int dE = 0;
+    const int acc = move_exact(cs, bs, m, lut, hist, lane, u, v, r.y, thr, ch.acc_width, E, err, &dE);
+    if (lane == 0) {
+      A.rb_dE[slot] = (int16_t)max(-32768, min(32767, dE));
+      atomicAdd(A.stats + 0, fabsf(p - (float)dE));
+      atomicAdd(A.stats + 1, 1.0f);
+      if (acc) {
+        atomicAdd(A.stats + 2, 1.0f);
+        atomicAdd(A.stats + 3, (float)dE);
+        ch.accepted[c] += 1;
+      }
+    }
+    if (acc && E < ch.best_energy[c]) {
+      if (lane == 0) ch.best_energy[c] = E;
+      for (int s = lane; s < m; s += 32) ch.best_cols[(size_t)c * kMaxM + s] = (int16_t)cs[s];
+    }
+  }
+  for (int s = lane; s < m; s += 32) {
+    ch.cols[(size_t)c * kMaxM + s] = (int16_t)cs[s];
+    ch.badness[(size_t)c * kMaxM + s] = bs[s];
+  }
+  if (lane == 0) {
+    ch.energy[c] = E;
+    if (err && ch.error_word) atomicOr(ch.error_word, err);
+    if (ch.global_best) atomicMin(ch.global_best, E);
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Training (SIMT fp32).
+// ---------------------------------------------------------------------------
+struct Batch {
+  float* X;   // [B][192]
+  float* y;   // [B]
+};
+
+// Draws batch row b from the first `filled` ring slots, filled =
+// min(capacity, steps recorded * chains); the draw is keyed by the training
+// step counter.
+__global__ void gather_kernel(const uint16_t* __restrict__ rb_feat, const uint8_t* __restrict__ rb_bad,
+                              const int16_t* __restrict__ rb_dE, const uint64_t* __restrict__ counters,
+                              int64_t capacity, int n_chains, int B, uint32_t k0, uint32_t k1, float* __restrict__ X,
+                              float* __restrict__ y) {
+  const int b = blockIdx.x;
+  __shared__ int64_t slot_s;
+  if (threadIdx.x == 0) {
+    const uint64_t steps = counters[0], t = counters[1];
+    const uint64_t recorded = steps * (uint64_t)n_chains;
+    const uint64_t filled = recorded < (uint64_t)capacity ? (recorded ? recorded : 1) : (uint64_t)capacity;
+    const U4 r = philox4x32_10(U4{(uint32_t)t, (uint32_t)(t >> 32), (uint32_t)b, 0x7A000000u}, k0, k1);
+    const uint64_t x = ((uint64_t)r.x << 32) | r.y;
+    slot_s = (int64_t)(x % filled);
+    y[b] = (float)rb_dE[slot_s] / kTargetScale;
+  }
+  __syncthreads();
+  const int64_t s = slot_s;
+  for (int k = threadIdx.x; k < kIn; k += blockDim.x) {
+    float v = 0.f;
+    if (k < kCandFeat) {
+      const uint16_t h = rb_feat[s * kCandFeat + k];
+      v = __uint_as_float((uint32_t)h << 16);
+    } else if (k < kCandFeat + kChainFeat) {
+      v = (float)rb_bad[s * kChainFeat + (k - kCandFeat)] * (1.0f / 16.0f);
+    }
+    X[(size_t)b * kIn + k] = v;
+  }
+}
+
+// C[M x N] = sum_k A(m, k) B(k, n), A(m,k) = A[m*sam + k*sak], B(k,n) = B[k*sbk + n*sbn].
+// EPI 0: C = acc (+ atomically when split over gridDim.z)
+// EPI 1: Z = acc + bias[n]; C = relu(Z); aux = Z
+// EPI 2: C = acc * (aux[m, n] > 0)
+// EPI 3: C = acc + bias[n]
+template <int EPI>
+__global__ void __launch_bounds__(256) gemm_kernel(int M, int N, int K, const float* __restrict__ A, int sam, int sak,
+                                                   const float* __restrict__ Bm, int sbk, int sbn,
+                                                   float* __restrict__ C, int ldc, const float* __restrict__ bias,
+                                                   float* __restrict__ aux) {
+  __shared__ float As[16][64 + 4];
+  __shared__ float Bs[16][64 + 4];
+  const int tx = threadIdx.x % 16, ty = threadIdx.x / 16;
+  const int m0 = blockIdx.y * 64, n0 = blockIdx.x * 64;
+  const int kchunk = (K + gridDim.z - 1) / gridDim.z;
+  const int kb = blockIdx.z * kchunk, ke = min(K, kb + kchunk);
+  float acc[4][4] = {};
+  for (int k0 = kb; k0 < ke; k0 += 16) {
+    for (int i = threadIdx.x; i < 16 * 64; i += 256) {
+      const int kk = i / 64, mm = i % 64;
+      const int gk = k0 + kk;
+      As[kk][mm] = (m0 + mm < M && gk < ke) ? A[(size_t)(m0 + mm) * sam + (size_t)gk * sak] : 0.f;
+      Bs[kk][mm] = (n0 + mm < N && gk < ke) ? Bm[(size_t)gk * sbk + (size_t)(n0 + mm) * sbn] : 0.f;
+    }
+    __syncthreads();
+#pragma unroll
+    for (int kk = 0; kk < 16; ++kk) {
+      float a[4], b[4];
+#pragma unroll
+      for (int i = 0; i < 4; ++i) {
+        a[i] = As[kk][ty * 4 + i];
+        b[i] = Bs[kk][tx * 4 + i];
+      }
+#pragma unroll
+      for (int i = 0; i < 4; ++i)
+#pragma unroll
+        for (int j = 0; j < 4; ++j) acc[i][j] = fmaf(a[i], b[j], acc[i][j]);
+    }
+    __syncthreads();
+  }
+#pragma unroll
+  for (int i = 0; i < 4; ++i) {
+    const int mm = m0 + ty * 4 + i;
+    if (mm >= M) continue;
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {
+      const int nn = n0 + tx * 4 + j;
+      if (nn >= N) continue;
+      float v = acc[i][j];
+      const size_t o = (size_t)mm * ldc + nn;
+      if (EPI == 0) {
+        if (gridDim.z > 1)
+          atomicAdd(C + o, v);
+        else
+          C[o] = v;
+      } else if (EPI == 1) {
+        v += bias[nn];
+        aux[o] = v;
+        C[o] = fmaxf(v, 0.f);
+      } else if (EPI == 2) {
+        C[o] = aux[o] > 0.f ? v : 0.f;
+      } else {
+        C[o] = v + bias[nn];
+      }
+    }
+  }
+}
+
+// out = H2 . w3 + b3, d = 2 (out - y) / B, dZ2 = d w3 (Z2 > 0), loss += (out - y)^2
+__global__ void head_kernel(int B, const float* __restrict__ H2, const float* __restrict__ Z2,
+                            const float* __restrict__ P, const float* __restrict__ y, float* __restrict__ d,
+                            float* __restrict__ dZ2, float* __restrict__ loss) {
+  const int b = blockIdx.x * (blockDim.x / 32) + threadIdx.x / 32;
+  const int lane = threadIdx.x & 31;
+  if (b >= B) return;
+  float acc = 0.f;
+  for (int k = lane; k < kH; k += 32) acc = fmaf(H2[(size_t)b * kH + k], P[oW3 + k], acc);
+#pragma unroll
+  for (int o = 16; o; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
+  const float out = acc + P[oB3];
+  const float e = out - y[b];
+  const float g = 2.f * e / (float)B;
+  if (lane == 0) {
+    d[b] = g;
+    atomicAdd(loss, e * e);
+  }
+  for (int k = lane; k < kH; k += 32) dZ2[(size_t)b * kH + k] = Z2[(size_t)b * kH + k] > 0.f ? g * P[oW3 + k] : 0.f;
+}
+
+// column sums: out[n] = sum_b M[b][n] (+ for gw3: sum_b H2[b][n] d[b])
+__global__ void colsum_kernel(int B, int N, const float* __restrict__ Mx, const float* __restrict__ scale,
+                              float* __restrict__ out) {
+  const int n = blockIdx.x * blockDim.x + threadIdx.x;
+  if (n >= N) return;
+  float acc = 0.f;
+  for (int b = 0; b < B; ++b) acc = fmaf(Mx[(size_t)b * N + n], scale ? scale[b] : 1.f, acc);
+  out[n] = acc;
+}
+
+__global__ void sum_kernel(int B, const float* __restrict__ v, float* __restrict__ out) {
+  float acc = 0.f;
+  for (int b = threadIdx.x; b < B; b += blockDim.x) acc += v[b];
+#pragma unroll
+  for (int o = 16; o; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
+  __shared__ float part[32];
+  if ((threadIdx.x & 31) == 0) part[threadIdx.x / 32] = acc;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    float t = 0.f;
+    for (int i = 0; i < (int)(blockDim.x / 32); ++i) t += part[i];
+    *out = t;
+  }
+}
+
+// Adam (Kingma & Ba) with bias correction; the step number is counters[1] + 1.
+__global__ void adam_kernel(int count, float* __restrict__ P, const float* __restrict__ G, float* __restrict__ Mo,
+                            float* __restrict__ V, float lr, float b1, float b2, float eps,
+                            const uint64_t* __restrict__ counters) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= count) return;
+  const float t = (float)(counters[1] + 1);
+  const float c1 = 1.f - powf(b1, t), c2 = 1.f - powf(b2, t);
+  const float g = G[i];
+  const float m = b1 * Mo[i] + (1.f - b1) * g;
+  const float v = b2 * V[i] + (1.f - b2) * g * g;
+  Mo[i] = m;
+  V[i] = v;
+  P[i] -= lr * (m / c1) / (sqrtf(v / c2) + eps);
+}
+
+__global__ void bump_kernel(uint64_t* counters, int which) { counters[which] += 1; }
+
+}  // namespace mlp
+}  // namespace n3
+
+// ---------------------------------------------------------------------------
+// Host side.
+// ---------------------------------------------------------------------------
+namespace n3host {
+using namespace n3::mlp;
+
+static int launch_pack(const n3_mlp* M, cudaStream_t st) {
+  pack_kernel<<<148, 256, 0, st>>>(M->params, M->w2_img, M->w1a_img);
+  return check_launch("mlp pack_kernel");
+}
+
+static size_t step_smem() {
+  return ((sizeof(uint16_t) * n3::kLutSize + 15) / 16) * 16 +
+         kStepWarps * (sizeof(uint32_t) * n3::kDirWords + 2 * sizeof(int) * n3::kMaxM);
+}
+
+int prepare_mlp() {
+  N3_TRY(allow_smem(reinterpret_cast<const void*>(infer_kernel), kInferSmem));
+  return allow_smem(reinterpret_cast<const void*>(learned_step_kernel), step_smem());
+}
+
+}  // namespace n3host
+
+extern "C" {
+
+int n3_mlp_param_count(void) { return n3::mlp::kParams; }
+
+int n3_mlp_scratch_floats(int batch) {
+  // X [B][192], y, d, Z1, H1, Z2, H2, dZ2, dZ1 [B][256] each, loss
+  return batch * (n3::mlp::kIn + 2) + 6 * batch * n3::mlp::kH + 4;
+}
+
+int n3_mlp_pack(const n3_mlp* M, void* stream) {
+  if (!M || !M->params || !M->w2_img || !M->w1a_img) return n3host::set_error(N3_ERR_ARG, "null MLP buffer");
+  return n3host::launch_pack(M, (cudaStream_t)stream);
+}
+
+int n3_mlp_candidates(const n3_chains* ch, const n3_mlp* M, uint64_t seed, void* stream) {
+  using namespace n3::mlp;
+  if (!ch || !M) return n3host::set_error(N3_ERR_ARG, "null descriptor");
+  CandArgs A;
+  A.cols = ch->cols;
+  A.badness = ch->badness;
+  A.ladder_n = ch->ladder_n;
+  A.ladder_size = ch->ladder_size;
+  A.n_chains = ch->n_chains;
+  A.a1_img = M->a1_img;
+  A.badn = M->badn;
+  A.cand = M->cand;
+  A.step = M->counters;
+  A.k0 = (uint32_t)seed;
+  A.k1 = (uint32_t)(seed >> 32);
+  cudaStream_t st = (cudaStream_t)stream;
+  candidates_kernel<<<ch->n_chains, kCand, 0, st>>>(A);
+  N3_TRY(n3host::check_launch("candidates_kernel"));
+  // chain part of layer 1 for every chain: c1 = badn W1b^T + b1   (B(k, n) = W1[n*192 + 12 + k])
+  const int C = ch->n_chains;
+  gemm_kernel<3><<<dim3(kH / 64, (C + 63) / 64, 1), 256, 0, st>>>(C, kH, kChainFeat, M->badn, kChainFeat, 1,
+                                                                  M->params + oW1 + kCandFeat, 1, kIn, M->c1, kH,
+                                                                  M->params + oB1, nullptr);
+  return n3host::check_launch("chain layer-1 gemm");
+}
+
+int n3_mlp_infer(const n3_mlp* M, int tiles, void* stream) {
+  using namespace n3::mlp;
+  if (!M || tiles < 0) return n3host::set_error(N3_ERR_ARG, "bad MLP inference arguments");
+  if (tiles == 0) return N3_OK;
+  N3_TRY(n3host::allow_smem(reinterpret_cast<const void*>(infer_kernel), kInferSmem));
+  InferArgs A;
+  A.a1_img = M->a1_img;
+  A.c1 = M->c1;
+  A.w2_img = M->w2_img;
+  A.w1a_img = M->w1a_img;
+  A.P = M->params;
+  A.pred = M->pred;
+  A.tiles = tiles;
+  A.error_word = M->error_word;
+  const int grid = tiles < n3host::sm_count() ? tiles : n3host::sm_count();
+  infer_kernel<<<grid, 128, kInferSmem, (cudaStream_t)stream>>>(A);
+  return n3host::check_launch("infer_kernel");
+}
+
+int n3_mlp_step(const n3_chains* ch, const n3_mlp* M, const float* temps, uint64_t seed, void* stream) {
+  using namespace n3::mlp;
+  if (!ch || !M || !temps) return n3host::set_error(N3_ERR_ARG, "null descriptor");
+  N3_TRY(n3host::ensure_device_tables());
+  const size_t smem = n3host::step_smem();
+  N3_TRY(n3host::allow_smem(reinterpret_cast<const void*>(learned_step_kernel), smem));
+  StepArgs A;
+  A.ch = *ch;
+  A.lut = n3host::dir_lut_device_ptr();
+  A.temps = temps;
+  A.cand = M->cand;
+  A.pred = M->pred;
+  A.step = M->counters;
+  A.k0 = (uint32_t)seed;
+  A.k1 = (uint32_t)(seed >> 32);
+  A.rb_feat = M->rb_feat;
+  A.rb_bad = M->rb_bad;
+  A.rb_dE = M->rb_dE;
+  A.rb_cap = M->rb_capacity;
+  A.stats = M->stats;
+  const int grid = (ch->n_chains + kStepWarps - 1) / kStepWarps;
+  learned_step_kernel<<<grid, kStepWarps * 32, smem, (cudaStream_t)stream>>>(A);
+  N3_TRY(n3host::check_launch("learned_step_kernel"));
+  bump_kernel<<<1, 1, 0, (cudaStream_t)stream>>>(M->counters, 0);
+  return n3host::check_launch("bump_kernel");
+}
+
+int n3_mlp_train(const n3_mlp* M, int n_chains, int batch, float lr, uint64_t seed, float* scratch, float* grads,
+                 float* adam_m, float* adam_v, void* stream) {
+  using namespace n3::mlp;
+  cudaStream_t st = (cudaStream_t)stream;
+  if (!M || !scratch || !grads || !adam_m || !adam_v || batch < 64 || n_chains < 1)
+    return n3host::set_error(N3_ERR_ARG, "bad MLP training arguments");
+  const int B = batch;
+  float* X = scratch;
+  float* y = X + (size_t)B * kIn;
+  float* d = y + B;
+  float* Z1 = d + B;
+  float* H1 = Z1 + (size_t)B * kH;
+  float* Z2 = H1 + (size_t)B * kH;
+  float* H2 = Z2 + (size_t)B * kH;
+  float* dZ2 = H2 + (size_t)B * kH;
+  float* dZ1 = dZ2 + (size_t)B * kH;
+  float* loss = dZ1 + (size_t)B * kH;
+  float* P = M->params;
+  cudaMemsetAsync(grads, 0, sizeof(float) * kParams, st);
+  cudaMemsetAsync(loss, 0, sizeof(float), st);
+  gather_kernel<<<B, 64, 0, st>>>(M->rb_feat, M->rb_bad, M->rb_dE, M->counters, M->rb_capacity, n_chains, B,
+                                  (uint32_t)seed, (uint32_t)(seed >> 32), X, y);
+  const dim3 g_fwd(kH / 64, (B + 63) / 64, 1);
+  // Z1 = X W1^T + b1 ; H1 = relu(Z1)     (W1 [256][192]: B(k, n) = W1[n*192 + k])
+  gemm_kernel<1><<<g_fwd, 256, 0, st>>>(B, kH, kIn, X, kIn, 1, P + oW1, 1, kIn, H1, kH, P + oB1, Z1);
+  gemm_kernel<1><<<g_fwd, 256, 0, st>>>(B, kH, kH, H1, kH, 1, P + oW2, 1, kH, H2, kH, P + oB2, Z2);
+  head_kernel<<<(B + 7) / 8, 256, 0, st>>>(B, H2, Z2, P, y, d, dZ2, loss);
+  // gradients of the head and layer 2
+  colsum_kernel<<<(kH + 127) / 128, 128, 0, st>>>(B, kH, H2, d, grads + oW3);
+  sum_kernel<<<1, 1024, 0, st>>>(B, d, grads + oB3);
+  const int splits = B >= 2048 ? 16 : 4;
+  // gW2[n][k] = sum_b dZ2[b][n] H1[b][k]
+  gemm_kernel<0><<<dim3(kH / 64, kH / 64, splits), 256, 0, st>>>(kH, kH, B, dZ2, 1, kH, H1, kH, 1, grads + oW2, kH,
+                                                                   nullptr, nullptr);
+  colsum_kernel<<<(kH + 127) / 128, 128, 0, st>>>(B, kH, dZ2, nullptr, grads + oB2);
+  // dZ1 = (dZ2 W2) * (Z1 > 0)            (B(k, n) = W2[k*256 + n])
+  gemm_kernel<2><<<g_fwd, 256, 0, st>>>(B, kH, kH, dZ2, kH, 1, P + oW2, kH, 1, dZ1, kH, nullptr, Z1);
+  // gW1[n][k] = sum_b dZ1[b][n] X[b][k]
+  gemm_kernel<0><<<dim3(kIn / 64, kH / 64, splits), 256, 0, st>>>(kH, kIn, B, dZ1, 1, kH, X, kIn, 1, grads + oW1,
+                                                                    kIn, nullptr, nullptr);
+  colsum_kernel<<<(kH + 127) / 128, 128, 0, st>>>(B, kH, dZ1, nullptr, grads + oB1);
+  adam_kernel<<<(kParams + 255) / 256, 256, 0, st>>>(kParams, P, grads, adam_m, adam_v, lr, 0.9f, 0.999f, 1e-8f,
+                                                     M->counters);
+  bump_kernel<<<1, 1, 0, st>>>(M->counters, 1);
+  if (M->loss_out) cudaMemcpyAsync(M->loss_out, loss, sizeof(float), cudaMemcpyDeviceToDevice, st);
+  N3_TRY(n3host::check_launch("mlp training kernels"));
+  return n3host::launch_pack(M, st);
+}
+
+}  // extern "C"

@@ -227,6 +227,11 @@ static int check_common(int B, int n, const void* a, const void* out) {
   return N3_OK;
 }
 
+int prepare_score() {
+  N3_TRY(allow_smem(reinterpret_cast<const void*>(n3::slope_kernel<0>), n3::kSlopeSmem));
+  return allow_smem(reinterpret_cast<const void*>(n3::slope_kernel<1>), n3::kSlopeSmem);
+}
+
 template <class Src>
 static int launch_det(Src src, int B, int n, int32_t* scores, int32_t* badness, cudaStream_t st) {
   if (B == 0) return N3_OK;

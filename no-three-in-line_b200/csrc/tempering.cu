@@ -28,6 +28,7 @@
 #include "dirs.cuh"
 #include "n3_common.cuh"
 #include "philox.cuh"
+#include "chain_move.cuh"
 #include "score_impl.cuh"
 
 namespace cg = cooperative_groups;
@@ -55,89 +56,6 @@ struct TemperSmem {
            3 * sizeof(int) * 64 + 16;
   }
 };
-
-// One proposal of the chain held by this warp.  Returns 1 if accepted.
-__device__ __forceinline__ int propose(int* __restrict__ cs, int* __restrict__ bs, int m,
-                                       const uint16_t* __restrict__ lut, uint32_t* __restrict__ hist, int lane,
-                                       U4 rnd, const uint32_t* __restrict__ thr, int W, int& E,
-                                       uint32_t& err) {
-  const int u = (int)__umulhi(rnd.x, (unsigned)m);
-  const int v = (int)__umulhi(rnd.y, (unsigned)m);
-  if (!legal_swap(cs, u, v)) return 0;
-  const int ru = u >> 1, rv = v >> 1, cu = cs[u], cv = cs[v];
-  int ids[kSlotsPerLane], cnt_new[kSlotsPerLane];
-  // centre u' = (r_u, c_v)
-  const int part_a = hist_build(cs, m, ru, cv, u, v, lut, hist, lane, ids);
-  __syncwarp();
-  const int line_new = dir_id(lut, rv - ru, cu - cv);
-  const int j_new = hist_get(hist, line_new);
-#pragma unroll
-  for (int t = 0; t < kSlotsPerLane; ++t)
-    cnt_new[t] = ids[t] >= 0 ? hist_get(hist, ids[t]) - 1 + (ids[t] == line_new) : 0;
-  __syncwarp();
-  hist_release(hist, ids);
-  __syncwarp();
-  // centre v' = (r_v, c_u)
-  const int part_b = hist_build(cs, m, rv, cu, u, v, lut, hist, lane, ids);
-  __syncwarp();
-#pragma unroll
-  for (int t = 0; t < kSlotsPerLane; ++t) cnt_new[t] += ids[t] >= 0 ? hist_get(hist, ids[t]) - 1 : 0;
-  __syncwarp();
-  hist_release(hist, ids);
-  // points of A on the old line (u, v)
-  int joint = 0;
-#pragma unroll
-  for (int t = 0; t < kSlotsPerLane; ++t) {
-    const int k = lane + 32 * t;
-    if (k < m && k != u && k != v) joint += (rv - ru) * (cs[k] - cu) == (cv - cu) * ((k >> 1) - ru);
-  }
-  const int sum_ab = warp_sum(part_a + (part_b << 16));
-  const int sum_joint = warp_sum(joint);
-  const int t_a = sum_ab & 0xFFFF, t_b = sum_ab >> 16;
-  const int dE = (t_a + t_b + j_new) - (bs[u] + bs[v] - sum_joint);
-  const bool accept = dE <= 0 || (dE < W && rnd.z < thr[dE]);
-  if (!accept) {
-    __syncwarp();
-    return 0;
-  }
-  // Old-side histograms: exact badness change of every other point.
-  __syncwarp();
-  int dB[kSlotsPerLane];
-  const int part_c = hist_build(cs, m, ru, cu, u, v, lut, hist, lane, ids);
-  __syncwarp();
-  const int line_old = dir_id(lut, rv - ru, cv - cu);
-  const int j_old = hist_get(hist, line_old);
-#pragma unroll
-  for (int t = 0; t < kSlotsPerLane; ++t)
-    dB[t] = cnt_new[t] - (ids[t] >= 0 ? hist_get(hist, ids[t]) - 1 + (ids[t] == line_old) : 0);
-  __syncwarp();
-  hist_release(hist, ids);
-  __syncwarp();
-  const int part_d = hist_build(cs, m, rv, cv, u, v, lut, hist, lane, ids);
-  __syncwarp();
-#pragma unroll
-  for (int t = 0; t < kSlotsPerLane; ++t) dB[t] -= ids[t] >= 0 ? hist_get(hist, ids[t]) - 1 : 0;
-  __syncwarp();
-  hist_release(hist, ids);
-  const int sum_cd = warp_sum(part_c + (part_d << 16));
-  const int t_c = sum_cd & 0xFFFF, t_d = sum_cd >> 16;
-  if (bs[u] != t_c + j_old || bs[v] != t_d + j_old || j_old != sum_joint) err |= kErrAudit;
-  __syncwarp();
-#pragma unroll
-  for (int t = 0; t < kSlotsPerLane; ++t) {
-    const int k = lane + 32 * t;
-    if (k < m && k != u && k != v) bs[k] += dB[t];
-  }
-  if (lane == 0) {
-    bs[u] = t_a + j_new;
-    bs[v] = t_b + j_new;
-    cs[u] = cv;
-    cs[v] = cu;
-  }
-  __syncwarp();
-  E += dE;
-  return 1;
-}
 
 // Exchange step of one ladder (run by its leader thread).  tmp_chain[t] is the
 // ladder-local chain at temperature t, tmp_temp[i] the temperature of chain i,
@@ -401,6 +319,15 @@ int temper_launch(const n3_chains* ch, const n3_temper_config* cfg, cudaStream_t
   return check_launch("temper_kernel");
 }
 
+}  // namespace n3host
+
+namespace n3host {
+int prepare_tempering() {
+  N3_TRY(allow_smem(reinterpret_cast<const void*>(n3::temper_kernel), n3::TemperSmem::bytes(16)));
+  const size_t audit = n3::TemperSmem::lut_bytes +
+                       n3::kAuditWarps * (sizeof(uint32_t) * n3::kDirWords + 2 * sizeof(int) * n3::kMaxM);
+  return allow_smem(reinterpret_cast<const void*>(n3::audit_kernel), audit);
+}
 }  // namespace n3host
 
 extern "C" {

@@ -1,0 +1,132 @@
+"""(d) Learned proposal: tcgen05 MLP inference against an fp64 reference of
+the same bf16-rounded network, training gradients against torch autograd,
+and exact energies through learned steps."""
+from __future__ import annotations
+
+import numpy as np
+import pytest
+
+from no_three_in_line_b200 import learned, state, tempering
+
+pytestmark = pytest.mark.gpu
+
+
+def bf16(x):
+    """Round-to-nearest-even to bfloat16, returned as float64."""
+    a = np.asarray(x, dtype=np.float32)
+    b = a.view(np.uint32).astype(np.uint64)
+    b = ((b + 0x7FFF + ((b >> 16) & 1)) >> 16) << 16
+    return b.astype(np.uint32).view(np.float32).astype(np.float64)
+
+
+def inter16_offset(row, k):
+    return (row >> 3) * 256 + (k >> 3) * 128 + (row & 7) * 16 + (k & 7) * 2
+
+
+def make(n=75, chains=32, L=16, seed=4):
+    p, q = state.seeded_population(n, chains)
+    temps = np.tile(tempering.geometric_ladder(0.05, 5.0, L), chains // L)
+    ch = tempering.TemperingChains(state.pq_to_columns(p, q), temps, seed, ladder_size=L)
+    return ch
+
+
+def features(cols, bad, n, u, v):
+    s = [u, v, u ^ 1, v ^ 1]
+    return np.array([bad[x] / 16 for x in s] + [(x >> 1) / n for x in s] + [cols[x] / n for x in s])
+
+
+def test_inference_matches_bf16_reference(cuda):
+    ch = make()
+    lp = learned.LearnedProposal(ch, seed=9, ring_capacity=1 << 12, batch=256)
+    lp.propose_scores()
+    P = lp.params.cpu().numpy().astype(np.float64)
+    W1 = P[learned.O_W1:learned.O_B1].reshape(256, 192)
+    b1 = P[learned.O_B1:learned.O_W2]
+    W2 = P[learned.O_W2:learned.O_B2].reshape(256, 256)
+    b2 = P[learned.O_B2:learned.O_W3]
+    w3 = P[learned.O_W3:learned.O_B3]
+    b3 = P[learned.O_B3]
+    cols = ch.cols.cpu().numpy()
+    bad = ch.badness_dev.cpu().numpy()
+    cand = lp.cand.cpu().numpy()
+    pred = lp.pred.cpu().numpy()
+    img = lp.a1_img.cpu().numpy().reshape(-1, 4096)
+    c1_dev = lp.c1.cpu().numpy()
+    for c in range(cols.shape[0]):
+        x_chain = bad[c] / 16.0
+        c1 = b1 + W1[:, 12:162] @ x_chain
+        assert np.allclose(c1_dev[c], c1, rtol=1e-5, atol=1e-5)
+        F = np.zeros((128, 16))
+        for j in range(128):
+            u, v = cand[c, j] & 0xFF, (cand[c, j] >> 8) & 0xFF
+            F[j, :12] = features(cols[c], bad[c], 75, u, v)
+            got = np.array([img[c, inter16_offset(j, k):inter16_offset(j, k) + 2].view(np.uint16)[0]
+                            for k in range(16)], np.uint32)
+            assert np.array_equal((got << 16).view(np.float32).astype(np.float64), bf16(F[j]))
+        h1 = np.maximum(bf16(F) @ bf16(np.pad(W1[:, :12], ((0, 0), (0, 4)))).T + c1, 0)
+        h2 = np.maximum(bf16(h1) @ bf16(W2).T + b2, 0)
+        ref = (h2 @ w3 + b3) * 16.0
+        assert np.allclose(pred[c], ref, rtol=1e-2, atol=5e-2), (c, np.abs(pred[c] - ref).max())
+
+
+def test_training_gradients_match_autograd(cuda):
+    import torch
+
+    ch = make(chains=64, L=16)
+    lp = learned.LearnedProposal(ch, seed=3, ring_capacity=1 << 14, batch=256, lr=1e-3)
+    for _ in range(20):
+        lp.step()
+    p0 = lp.params.clone()
+    lp.train()
+    torch.cuda.synchronize()
+    B = lp.batch
+    X = lp.scratch[:B * 192].view(B, 192).double().cpu()
+    y = lp.scratch[B * 192:B * 192 + B].double().cpu()
+    P = p0.double().cpu().requires_grad_(True)
+    W1 = P[learned.O_W1:learned.O_B1].view(256, 192)
+    b1 = P[learned.O_B1:learned.O_W2]
+    W2 = P[learned.O_W2:learned.O_B2].view(256, 256)
+    b2 = P[learned.O_B2:learned.O_W3]
+    w3 = P[learned.O_W3:learned.O_B3]
+    b3 = P[learned.O_B3]
+    h1 = torch.relu(X @ W1.T + b1)
+    h2 = torch.relu(h1 @ W2.T + b2)
+    out = h2 @ w3 + b3
+    loss = ((out - y) ** 2).mean()
+    loss.backward()
+    g_ref = P.grad.numpy()
+    g = lp.grads.cpu().numpy().astype(np.float64)
+    scale = np.abs(g_ref).max()
+    assert np.allclose(g[:learned.O_B3 + 1], g_ref[:learned.O_B3 + 1], rtol=1e-3, atol=1e-4 * scale)
+    # the applied update is Adam's first step from these gradients
+    m = 0.1 * g
+    v = 0.001 * g * g
+    p1_ref = p0.double().cpu().numpy() - 1e-3 * (m / 0.1) / (np.sqrt(v / 0.001) + 1e-8)
+    assert np.allclose(lp.params.cpu().numpy(), p1_ref, rtol=1e-5, atol=1e-6)
+    assert abs(float(lp.loss.item()) / B - float(loss)) < 1e-3 * (1 + float(loss))
+
+
+def test_learned_steps_keep_energies_exact(cuda):
+    ch = make(chains=64, L=16, seed=12)
+    e0 = int(ch.energy.min().item())
+    lp = learned.LearnedProposal(ch, seed=12, ring_capacity=1 << 16, batch=512)
+    res = lp.run(600, exchange_every=300, train_every=10, block=50)
+    ch.validate()
+    assert int(ch.error_word.item()) == 0 and int(lp.error_word.item()) == 0
+    st = lp.read_stats()
+    assert st.proposals >= 64 * 600 and st.accepted > 0 and np.isfinite(st.mae)
+    assert res.best < e0
+    from no_three_in_line_b200 import gpu
+
+    s = gpu.score_columns_gpu(ch.best_columns.cpu().numpy())
+    assert np.array_equal(s, ch.best_energy.cpu().numpy())
+
+
+def test_graph_and_eager_agree(cuda):
+    runs = []
+    for graph in (False, True):
+        ch = make(chains=32, L=16, seed=21)
+        lp = learned.LearnedProposal(ch, seed=21, ring_capacity=1 << 14, batch=256)
+        lp.run(100, exchange_every=100, train_every=0, block=50, graph=graph, warm=False)
+        runs.append((ch.cols.cpu().numpy(), ch.energy.cpu().numpy(), lp.params.cpu().numpy()))
+    assert np.array_equal(runs[0][0], runs[1][0]) and np.array_equal(runs[0][1], runs[1][1])
