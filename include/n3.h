@@ -245,6 +245,21 @@ int n3_mlp_step(const n3_chains* chains, const n3_mlp* mlp, const float* temps, 
 int n3_mlp_train(const n3_mlp* mlp, int n_chains, int batch, float lr, uint64_t seed, float* scratch, float* grads,
                  float* adam_m, float* adam_v, void* stream);
 
+/* The same training step without caller-provided scratch.  No counterpart in
+ * the reference.  For callers that cannot call cudaMalloc, such as a host
+ * application whose own allocator takes all device memory at start-up, or a
+ * plug-in whose host forbids allocations it does not make itself: the batch
+ * activations and the gradient live in a static device array inside libn3.so
+ * (about 4 MB, held by every GPU that loads the library until the process
+ * exits), so this call allocates nothing.  batch must lie in [64, 512]; larger
+ * batches are rejected with N3_ERR_RANGE.  The first call on a device looks up
+ * the array's device address; make that first call before any stream capture.
+ * All calls share the array, which keeps the last call's contents (the call
+ * clears what must start at zero): calls that overlap on the GPU, from several
+ * streams or threads, race on it and must be serialised by the caller. */
+int n3_mlp_train_noalloc(const n3_mlp* mlp, int n_chains, int batch, float lr, uint64_t seed, float* adam_m,
+                         float* adam_v, void* stream);
+
 /* Device clock (%globaltimer, ns) written to *out (device int64) in stream
  * order; used to time a run to its first target hit on the device. */
 int n3_device_clock_ns(int64_t* out, void* stream);

@@ -19,6 +19,7 @@
 // Training (SIMT fp32, hand-written GEMMs) uses MSE on dE / kTargetScale with
 // Adam; the packed bf16 images are rebuilt after each update.
 #include <cuda_bf16.h>
+#include <mutex>
 #include <math.h>
 
 #include "chain_move.cuh"
@@ -769,3 +770,100 @@ int n3_mlp_train(const n3_mlp* M, int n_chains, int batch, float lr, uint64_t se
 }
 
 }  // extern "C"
+
+// ---------------------------------------------------------------------------
+// Training step that allocates nothing.
+//
+// n3_mlp_train needs its caller to provide device memory for the batch
+// activations and the gradient.  Some callers cannot call cudaMalloc: an
+// application that hands all device memory to its own allocator at start-up,
+// or a plug-in loaded into a host whose memory manager forbids allocations it
+// does not make itself.  For them, n3_mlp_train_noalloc keeps that working
+// memory in the file-scope array below, sized for batches of at most
+// kNoAllocMaxBatch tuples (about 4 MB).  Every GPU that loads libn3.so holds
+// this array until the process exits.
+// ---------------------------------------------------------------------------
+namespace n3 {
+namespace mlp {
+constexpr int kNoAllocMaxBatch = 512;
+constexpr size_t kNoAllocScratchFloats =
+    (size_t)kNoAllocMaxBatch * (kIn + 2) + (size_t)6 * kNoAllocMaxBatch * kH + 4;
+constexpr size_t kNoAllocFloats = kNoAllocScratchFloats + kParams;  // scratch, then the gradient
+static __device__ __align__(256) float g_noalloc_work[kNoAllocFloats];
+}  // namespace mlp
+}  // namespace n3
+
+namespace n3host {
+
+// Device address of g_noalloc_work on the current device, looked up once per
+// device (the symbol's host-side name is not a device address).
+static int noalloc_work_ptr(float** out) {
+  static std::mutex mu;
+  static float* ptrs[64];
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64)
+    return set_error(N3_ERR_CUDA, "n3_mlp_train_noalloc: no usable current device");
+  std::lock_guard<std::mutex> lock(mu);
+  if (ptrs[dev] == nullptr) {
+    float* p = nullptr;
+    const cudaError_t e = cudaGetSymbolAddress((void**)&p, n3::mlp::g_noalloc_work);
+    if (e != cudaSuccess || p == nullptr)
+      return set_error(N3_ERR_CUDA, "n3_mlp_train_noalloc: cudaGetSymbolAddress failed: %s", cudaGetErrorString(e));
+    ptrs[dev] = p;
+  }
+  *out = ptrs[dev];
+  return N3_OK;
+}
+
+}  // namespace n3host
+
+extern "C" int n3_mlp_train_noalloc(const n3_mlp* M, int n_chains, int batch, float lr, uint64_t seed,
+                                    float* adam_m, float* adam_v, void* stream) {
+  using namespace n3::mlp;
+  cudaStream_t st = (cudaStream_t)stream;
+  if (!M || !adam_m || !adam_v || n_chains < 1) return n3host::set_error(N3_ERR_ARG, "bad MLP training arguments");
+  if (batch < 64 || batch > kNoAllocMaxBatch)
+    return n3host::set_error(N3_ERR_RANGE, "n3_mlp_train_noalloc: batch %d outside [64, %d] (its static working "
+                             "memory holds at most %d tuples)", batch, kNoAllocMaxBatch, kNoAllocMaxBatch);
+  float* work = nullptr;
+  N3_TRY(n3host::noalloc_work_ptr(&work));
+  const int B = batch;
+  float* X = work;
+  float* y = X + (size_t)B * kIn;
+  float* d = y + B;
+  float* Z1 = d + B;
+  float* H1 = Z1 + (size_t)B * kH;
+  float* Z2 = H1 + (size_t)B * kH;
+  float* H2 = Z2 + (size_t)B * kH;
+  float* dZ2 = H2 + (size_t)B * kH;
+  float* dZ1 = dZ2 + (size_t)B * kH;
+  float* loss = dZ1 + (size_t)B * kH;
+  float* grads = work + kNoAllocScratchFloats;
+  float* P = M->params;
+  // The array keeps the previous call's contents: clear the accumulated parts.
+  if (cudaMemsetAsync(grads, 0, sizeof(float) * kParams, st) != cudaSuccess ||
+      cudaMemsetAsync(loss, 0, sizeof(float), st) != cudaSuccess)
+    return n3host::check_launch("n3_mlp_train_noalloc: clearing the gradient");
+  gather_kernel<<<B, 64, 0, st>>>(M->rb_feat, M->rb_bad, M->rb_dE, M->counters, M->rb_capacity, n_chains, B,
+                                  (uint32_t)seed, (uint32_t)(seed >> 32), X, y);
+  const dim3 g_fwd(kH / 64, (B + 63) / 64, 1);
+  gemm_kernel<1><<<g_fwd, 256, 0, st>>>(B, kH, kIn, X, kIn, 1, P + oW1, 1, kIn, H1, kH, P + oB1, Z1);
+  gemm_kernel<1><<<g_fwd, 256, 0, st>>>(B, kH, kH, H1, kH, 1, P + oW2, 1, kH, H2, kH, P + oB2, Z2);
+  head_kernel<<<(B + 7) / 8, 256, 0, st>>>(B, H2, Z2, P, y, d, dZ2, loss);
+  colsum_kernel<<<(kH + 127) / 128, 128, 0, st>>>(B, kH, H2, d, grads + oW3);
+  sum_kernel<<<1, 1024, 0, st>>>(B, d, grads + oB3);
+  const int splits = 4;
+  gemm_kernel<0><<<dim3(kH / 64, kH / 64, splits), 256, 0, st>>>(kH, kH, B, dZ2, 1, kH, H1, kH, 1, grads + oW2, kH,
+                                                                   nullptr, nullptr);
+  colsum_kernel<<<(kH + 127) / 128, 128, 0, st>>>(B, kH, dZ2, nullptr, grads + oB2);
+  gemm_kernel<2><<<g_fwd, 256, 0, st>>>(B, kH, kH, dZ2, kH, 1, P + oW2, kH, 1, dZ1, kH, nullptr, Z1);
+  gemm_kernel<0><<<dim3(kIn / 64, kH / 64, splits), 256, 0, st>>>(kH, kIn, B, dZ1, 1, kH, X, kIn, 1, grads + oW1,
+                                                                    kIn, nullptr, nullptr);
+  colsum_kernel<<<(kH + 127) / 128, 128, 0, st>>>(B, kH, dZ1, nullptr, grads + oB1);
+  adam_kernel<<<(kParams + 255) / 256, 256, 0, st>>>(kParams, P, grads, adam_m, adam_v, lr, 0.9f, 0.999f, 1e-8f,
+                                                     M->counters);
+  bump_kernel<<<1, 1, 0, st>>>(M->counters, 1);
+  if (M->loss_out) cudaMemcpyAsync(M->loss_out, loss, sizeof(float), cudaMemcpyDeviceToDevice, st);
+  N3_TRY(n3host::check_launch("n3_mlp_train_noalloc kernels"));
+  return n3host::launch_pack(M, st);
+}
