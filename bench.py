@@ -42,6 +42,10 @@ TESTS_PER_STATE = math.comb(2 * N, 3)  # 551,300
 OPS_PER_TEST = 4                       # multiply, multiply-add, compare, count
 L2_FLUSH_BYTES = 256 << 20             # > 126 MB L2
 WORKLOAD = "n=75 population scoring, 4096 states, determinant + slope cross-check + badness"
+# dram__bytes_read.sum + dram__bytes_write.sum of one det_kernel launch over the
+# 4096-state population, from an ncu capture (1,253,632 B read, 0 B written; the
+# algorithmic input is 1,228,800 B of int16 columns plus the 16 KB of counts).
+DET_TRAFFIC_BYTES = 1253632
 
 
 def parse():
@@ -51,8 +55,16 @@ def parse():
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", choices=["b200", "reference"], default="b200")
     ap.add_argument("--states", type=int, default=STATES)
-    ap.add_argument("--mode", choices=["checked", "det", "slope"], default="checked",
-                    help="kernel a step runs: fused checked scoring (default), determinant only, slope only")
+    ap.add_argument("--mode", choices=["checked", "det", "slope", "tempering", "learned", "time-to-target"],
+                    default="checked",
+                    help="kernel a step runs: fused checked scoring (default), determinant only, slope only; "
+                         "or the learned-vs-plain time-to-target comparison")
+    ap.add_argument("--no-secondary", action="store_true", help="skip the delta/tempering/MLP measurements")
+    ap.add_argument("--seeds", type=int, default=3, help="time-to-target: seeds per method")
+    ap.add_argument("--budget", type=float, default=30.0, help="time-to-target: device seconds per run")
+    ap.add_argument("--target", type=int, default=12, help="time-to-target: energy target")
+    ap.add_argument("--learned-moves", type=str, default="1",
+                    help="time-to-target: comma-separated moves per learned step to compare (1 = one move per step)")
     return ap.parse_args()
 
 
@@ -147,6 +159,153 @@ def cpu_baseline(p, q, threads: int):
     return {"value": sample / dt, "unit": UNIT, "cores": threads, "kind": "port",
             "sample": f"{sample} n=75 states, determinant count + badness (accelerated.py:14-37 restated in C), "
                       f"{threads} threads, {dt:.2f} s"}
+
+
+def secondary_measurements(dev, p, q):
+    """Swap deltas/s and tempering / learned-proposal throughput at the
+    configurations of the metric, each timed with CUDA events after warm-up."""
+    import torch
+
+    from no_three_in_line_b200 import _lib, autotune, gpu_delta, learned, state, tempering
+
+    out = {}
+    launches = 0
+    # batched exact swap deltas over the n=75 population
+    cols = torch.from_numpy(state.pq_to_columns(p, q)).to(dev)
+    rng = np.random.default_rng(5)
+    M = 1 << 16
+    moves = torch.from_numpy(np.stack([rng.integers(0, cols.shape[0], M), rng.integers(0, 150, M),
+                                       rng.integers(0, 150, M)], 1).astype(np.int32)).to(dev)
+    dE = torch.empty(M, dtype=torch.int32, device=dev)
+    L = _lib.lib()
+    sptr = _lib.stream_ptr()
+    for _ in range(3):
+        _lib.check(L.n3_swap_delta(cols.data_ptr(), cols.shape[0], N, moves.data_ptr(), M, dE.data_ptr(), None, sptr),
+                   "n3_swap_delta")
+    a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    a.record()
+    for _ in range(10):
+        _lib.check(L.n3_swap_delta(cols.data_ptr(), cols.shape[0], N, moves.data_ptr(), M, dE.data_ptr(), None, sptr),
+                   "n3_swap_delta")
+    b.record()
+    b.synchronize()
+    legal = int((dE != gpu_delta.SENTINEL).sum().item())
+    out["swap_delta_batch"] = {"moves": M, "legal": legal, "deltas_per_s": 10 * M / (a.elapsed_time(b) / 1e3),
+                               "kernel": "n3::swap_delta_kernel<false> (direction-class, no badness output)"}
+    launches += 13
+    # C3: 2048 chains at n=75, 32 ladders of 64 temperatures, exchange every 10 sweeps
+    pc, qc = state.seeded_population(N, 2048)
+    ch = tempering.TemperingChains(state.pq_to_columns(pc, qc), np.tile(tempering.geometric_ladder(0.05, 5.0, 64), 32),
+                                   seed=1, ladder_size=64)
+    ch.run(20, exchange_every=10, sweeps_per_launch=20)
+    res = ch.run(100, exchange_every=10, sweeps_per_launch=100)
+    ch.validate()
+    out["tempering_n75_2048_chains"] = {"sweeps": res.sweeps, "seconds": res.seconds,
+                                        "deltas_per_s": res.proposals / res.seconds,
+                                        "triple_tests_per_s_equivalent": res.proposals / res.seconds * 43808,
+                                        "best_E_after_120_sweeps": res.best}
+    launches += 2
+    # C4: mixed sizes in one launch, autotuned
+    groups = []
+    for k, (n, cnt) in enumerate([(40, 1024), (52, 768), (60, 512), (68, 384), (75, 256)]):
+        pp, qq = state.seeded_population(n, cnt)
+        groups.append((n, state.pq_to_columns(pp, qq)))
+    mixed = tempering.TemperingChains.mixed(groups, tempering.geometric_ladder(0.05, 5.0, 32), seed=2)
+    tune = autotune.autotune(mixed, probe_sweeps=20)
+    mixed.run(max(tune.ladder_sweeps), exchange_every=10, chains_per_block=tune.chains_per_block,
+              ladder_sweeps=tune.ladder_sweeps)
+    res = mixed.run(max(tune.ladder_sweeps), exchange_every=10, chains_per_block=tune.chains_per_block,
+                    ladder_sweeps=tune.ladder_sweeps)
+    mixed.validate()
+    per = {}
+    for n in sorted(tune.size_sweeps):
+        lad = int((mixed.ladder_n_host == n).sum())
+        per[str(n)] = tune.size_sweeps[n] * 2 * n * 32 * lad / res.seconds
+    out["mixed_sizes_one_launch"] = {"autotuned": {"threads_per_chain": tune.threads_per_chain,
+                                                   "chains_per_block": tune.chains_per_block,
+                                                   "sweeps_per_launch": {str(k): v for k, v in tune.size_sweeps.items()},
+                                                   "cpb_candidates_deltas_per_s": {str(k): v for k, v in
+                                                                                   tune.candidates.items()}},
+                                     "seconds": res.seconds, "deltas_per_s_per_size": per,
+                                     "deltas_per_s_total": res.proposals / res.seconds}
+    launches += 2
+    # C5: learned proposals, 2048 chains at n=75, 128 candidates per chain per step
+    lp = learned.LearnedProposal(ch, seed=1, batch=4096)
+    res = lp.run(300, exchange_every=300, train_every=10, block=50)
+    st = lp.read_stats()
+    tiles = ch.cols.shape[0]
+    d = lp._descriptor()
+    for _ in range(3):
+        _lib.check(L.n3_mlp_infer(__import__("ctypes").byref(d), tiles, sptr), "n3_mlp_infer")
+    a.record()
+    for _ in range(10):
+        _lib.check(L.n3_mlp_infer(__import__("ctypes").byref(d), tiles, sptr), "n3_mlp_infer")
+    b.record()
+    b.synchronize()
+    infer_s = a.elapsed_time(b) / 1e3 / 10
+    flop = 2.0 * tiles * 128 * (16 * 256 + 256 * 256)
+    peaks, kind = measured_peaks()
+    out["learned_n75_2048_chains"] = {"steps_per_s": 300 / res.seconds, "candidates_per_s": 300 * tiles * 128 /
+                                      res.seconds, "mae_dE": st.mae, "accept_rate": st.accepted / max(1, st.proposals),
+                                      "infer_kernel_us": infer_s * 1e6, "infer_tflops": flop / infer_s / 1e12,
+                                      "infer_frac_of_bf16_peak": flop / infer_s / 1e12 / peaks["bf16_tflops"],
+                                      "peak_kind": kind}
+    launches += 13
+    return out, launches
+
+
+def run_chain_mode(args):
+    """One step = one exchange round (10 sweeps) of uniform-proposal tempering
+    over 2048 n=75 chains in 64-temperature ladders (--mode tempering), or 50
+    learned-proposal steps over the same chains (--mode learned)."""
+    import torch
+
+    from no_three_in_line_b200 import _lib, learned, state, tempering
+
+    _lib.require_device()
+    pc, qc = state.seeded_population(N, 2048)
+    ch = tempering.TemperingChains(state.pq_to_columns(pc, qc), np.tile(tempering.geometric_ladder(0.05, 5.0, 64), 32),
+                                   seed=1, ladder_size=64)
+    if args.mode == "tempering":
+        step = lambda: ch.run(10, exchange_every=10, sweeps_per_launch=10)  # noqa: E731
+        per_step, unit, what = 2048 * 150 * 10, "deltas/s", "exact swap deltas (proposals)"
+    else:
+        lp = learned.LearnedProposal(ch, seed=1)
+        lp.run(50, exchange_every=50, train_every=10, block=50)
+        step = lambda: lp.run(50, exchange_every=50, train_every=10, block=50, warm=False)  # noqa: E731
+        per_step, unit, what = 2048 * 128 * 50, "candidates/s", "MLP-scored candidates"
+    for _ in range(max(3, args.warmup)):
+        step()
+    torch.cuda.synchronize()
+    secs = 0.0
+    for _ in range(args.steps):
+        secs += step().seconds
+    ch.validate()
+    line = {"metric": METRIC, "value": per_step * args.steps / secs, "unit": unit, "n_gpus": 1, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": 1e3 * secs / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "int32" if args.mode == "tempering" else "bf16",
+            "data": "synthetic: random_state(75, Random(91001+c)) chain starts",
+            "config": {"workload": f"n=75, 2048 chains, 32 ladders x 64 temperatures (0.05..5.0): {what}",
+                       "mode": args.mode}, "best_E": int(ch.best_energy.min().item())}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def run_time_to_target(args):
+    from no_three_in_line_b200 import compare
+
+    moves = tuple(int(x) for x in args.learned_moves.split(","))
+    res = compare.compare(list(range(1, args.seeds + 1)), args.target, args.budget, learned_moves=moves)
+    line = {"metric": "time-to-E<=target, learned vs plain proposal (n=75, 2048 chains, 64-temperature ladders)",
+            "unit": "s", "higher_is_better": False, "target": args.target, "budget_s": args.budget,
+            **{k: v for k, v in res.items() if k.startswith("plain") or k.startswith("learned")},
+            "common_level": res["common_level"],
+            "data": "synthetic: random_state(75, Random(91001+c)) chain starts",
+            "runs": [{k: r[k] for k in ("method", "seed", "reached", "seconds", "best")} for r in res["runs"]],
+            "trajectories": {f'{r["method"]}-{r["seed"]}': r["trajectory"][::max(1, len(r["trajectory"]) // 40)]
+                             for r in res["runs"]}}
+    print(json.dumps(line), flush=True)
+    return 0
 
 
 def run_reference(args):
@@ -282,6 +441,19 @@ def run_b200(args):
         dist.all_reduce(t_e2e, op=dist.ReduceOp.MAX)
     e2e_ms = float(t_e2e.item())
 
+    # the dominant kernel alone (the determinant count), for the roofline
+    det_ms = []
+    for k in range(12):
+        flush.fill_(k)
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record(stream)
+        _lib.check(L.n3_score_columns(cols.data_ptr(), B, N, scores.data_ptr(), None, sptr), "n3_score_columns")
+        b.record(stream)
+        det_ms.append((a, b))
+    torch.cuda.synchronize()
+    det_ms = [a.elapsed_time(b) for a, b in det_ms[2:]]
+    det_launch_s = statistics.mean(det_ms) / 1e3
+
     # integer-pipe ceiling of the same test expression
     scratch = torch.zeros(2, dtype=torch.int64, device=dev)
     sms = torch.cuda.get_device_properties(dev).multi_processor_count
@@ -299,7 +471,10 @@ def run_b200(args):
     if rank == 0:
         ms_per_step = total_ms / args.steps
         tests_per_s = value * TESTS_PER_STATE
-        achieved = tests_per_s / world * OPS_PER_TEST / 1e9
+        if args.mode == "slope":
+            achieved = tests_per_s / world * OPS_PER_TEST / 1e9
+        else:  # the determinant kernel's own launches: 4096 states x 551,300 tests x 4 ops
+            achieved = B * TESTS_PER_STATE * OPS_PER_TEST / det_launch_s / 1e9
         peak = ceiling_tests * OPS_PER_TEST / 1e9
         peaks, peak_kind = measured_peaks()
         line = {
@@ -315,21 +490,26 @@ def run_b200(args):
             "e2e": {"value": world * B / (e2e_ms / 1e3), "unit": UNIT,
                     "h2d_bytes_per_step": int(cols_host.nbytes),
                     "d2h_bytes_per_step": int(h_scores.numel() * 4 + h_flags.numel() * 4)},
-            "gpu_launches": args.steps,
+            "gpu_launches": args.steps * (2 if args.mode == "checked" else 1),
             "roofline": {"bound": "int32-alu",
-                         "kernel": {"checked": "n3::slope_kernel<1> (determinant + slope, checked)",
+                         "kernel": {"checked": "n3::det_kernel<ColSource,false> (the larger of the step's two "
+                                               "launches; the other is n3::slope_kernel<2>)",
                                     "det": "n3::det_kernel<ColSource,false>",
                                     "slope": "n3::slope_kernel<0>"}[args.mode],
+                         "kernel_launch_us": det_launch_s * 1e6 if args.mode != "slope" else None,
                          "achieved": achieved, "peak": peak, "unit": "Gop/s", "frac": achieved / peak,
                          "peak_source": "measured on this GPU: n3_calibrate_det_ceiling, the scorer's own "
                                         "test expression on registers (4 int32 ops per triple test)",
-                         "traffic": None,
+                         "traffic": DET_TRAFFIC_BYTES if args.mode != "slope" else None,
                          "hbm_context": {"bytes_per_step": int(cols_host.nbytes + B * 4 + B * 2 * N * 4),
                                          "hbm_gbs_peak": peaks.get("hbm_gbs"), "peak_kind": peak_kind}},
             "wall_s_timed": wall,
             "clocks": clocks.summary(),
         }
         line["cpu_baseline"] = cpu_baseline(p, q, threads=os.cpu_count() or 1)
+        if world == 1 and not args.no_secondary and args.mode == "checked":
+            line["secondary"], extra = secondary_measurements(dev, p, q)
+            line["secondary"]["note"] = ("measured after the timed region; not part of value, e2e or gpu_launches")
     if world > 1:
         dist.barrier()
         dist.destroy_process_group()
@@ -345,6 +525,10 @@ def main():
     load_package()
     if args.impl == "reference":
         return run_reference(args)
+    if args.mode == "time-to-target":
+        return run_time_to_target(args)
+    if args.mode in ("tempering", "learned"):
+        return run_chain_mode(args)
     return run_b200(args)
 
 

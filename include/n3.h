@@ -235,9 +235,12 @@ int n3_mlp_pack(const n3_mlp* mlp, void* stream);
 int n3_mlp_candidates(const n3_chains* chains, const n3_mlp* mlp, uint64_t seed, void* stream);
 /* pred[t][j] for `tiles` tiles of 128 candidates from a1_img and c1 (tcgen05). */
 int n3_mlp_infer(const n3_mlp* mlp, int tiles, void* stream);
-/* Samples, scores exactly, accepts and records one move per chain, then
+/* Samples, scores exactly, accepts and records `moves` moves per chain
+ * (drawn without replacement from this step's 128 candidates, each re-checked
+ * for legality on the current state; 1 is the plain learned step), then
  * advances the step counter.  temps: the ladder's L temperatures (device). */
-int n3_mlp_step(const n3_chains* chains, const n3_mlp* mlp, const float* temps, uint64_t seed, void* stream);
+int n3_mlp_step(const n3_chains* chains, const n3_mlp* mlp, const float* temps, uint64_t seed, int moves,
+                void* stream);
 /* One Adam step on a batch drawn from the ring slots recorded so far (all
  * counters live on the device, so the call is graph-capturable); scratch
  * holds n3_mlp_scratch_floats(batch) floats, grads/adam_m/adam_v

@@ -1,0 +1,108 @@
+"""Time to a target energy: uniform-proposal tempering against learned-proposal
+tempering on the same GPU, chains and seeds.
+
+Both start from the same seeded states (random_state(n, Random(91001 + c))),
+the same temperature ladders and the same exchange schedule (every 10 sweeps of
+2n proposals).  The clock is the device's: CUDA events around the launches,
+with the target checked at launch boundaries (plain: inside the kernel, at the
+first exchange round after some chain reaches the target; learned: after each
+block of steps).  A run that does not reach the target within its budget is
+reported as censored at the budget.
+"""
+from __future__ import annotations
+
+import json
+import statistics
+import time
+from dataclasses import asdict, dataclass
+
+import numpy as np
+
+from . import state, tempering
+
+
+@dataclass
+class TargetRun:
+    method: str
+    seed: int
+    target: int
+    reached: bool
+    seconds: float           # device time to the hit, or the time spent when censored
+    best: int
+    trajectory: list          # (device seconds, best E) after each launch or block
+
+
+def seeded_chains(n: int, chains: int, ladder: int, seed: int, tmin: float = 0.05, tmax: float = 5.0):
+    p, q = state.seeded_population(n, chains)
+    temps = np.tile(tempering.geometric_ladder(tmin, tmax, ladder), chains // ladder)
+    return tempering.TemperingChains(state.pq_to_columns(p, q), temps, seed, ladder_size=ladder)
+
+
+def run_plain(seed: int, target: int, budget: float, *, n=75, chains=2048, ladder=64, block_sweeps=100):
+    ch = seeded_chains(n, chains, ladder, seed)
+    traj, spent = [], 0.0
+    while spent < budget:
+        res = ch.run(block_sweeps, exchange_every=10, target=target, sweeps_per_launch=block_sweeps)
+        if res.hit is not None:
+            spent += res.hit[2]
+            traj.append((spent, res.best))
+            return TargetRun("plain", seed, target, True, spent, res.best, traj)
+        spent += res.seconds
+        traj.append((spent, res.best))
+    return TargetRun("plain", seed, target, False, spent, int(ch.best_energy.min().item()), traj)
+
+
+def run_learned(seed: int, target: int, budget: float, *, n=75, chains=2048, ladder=64, block=50,
+                train_every=10, moves=1):
+    """Learned-proposal tempering; `moves` > 1 draws that many moves per step
+    (without replacement) from each step's scored candidates."""
+    from .learned import LearnedProposal
+
+    ch = seeded_chains(n, chains, ladder, seed)
+    lp = LearnedProposal(ch, seed=seed, moves=moves)
+    name = "learned" if moves == 1 else f"learned-x{moves}"
+    traj, spent, first = [], 0.0, True
+    while spent < budget:
+        res = lp.run(1500, exchange_every=1500, train_every=train_every, block=block, target=target, warm=first)
+        first = False
+        if res.hit is not None:
+            spent += res.hit[2]
+            traj.append((spent, res.best))
+            return TargetRun(name, seed, target, True, spent, res.best, traj)
+        spent += res.seconds
+        traj.append((spent, res.best))
+    return TargetRun(name, seed, target, False, spent, int(ch.best_energy.min().item()), traj)
+
+
+def time_to_reach(traj, level: int):
+    """Device seconds until the best energy first reached <= level (None if never)."""
+    for t, e in traj:
+        if e <= level:
+            return t
+    return None
+
+
+def compare(seeds, target: int, budget: float, *, learned_moves=(1,), **kw) -> dict:
+    runs = []
+    for s in seeds:
+        runs.append(run_plain(s, target, budget, **kw))
+        for k in learned_moves:
+            runs.append(run_learned(s, target, budget, moves=k, **kw))
+    out = {"target": target, "budget_s": budget, "runs": [asdict(r) for r in runs]}
+    methods = ["plain"] + ["learned" if k == 1 else f"learned-x{k}" for k in learned_moves]
+    for method in methods:
+        rs = [r for r in runs if r.method == method]
+        out[method] = {"median_s": statistics.median(r.seconds for r in rs),
+                       "reached": sum(r.reached for r in rs), "seeds": len(rs),
+                       "median_best": statistics.median(r.best for r in rs)}
+    # the lowest level every run of both methods reached, and the time each took
+    common = max(r.best for r in runs)
+    out["common_level"] = common
+    for method in methods:
+        times = [time_to_reach(r.trajectory, common) for r in runs if r.method == method]
+        out[method]["median_s_to_common_level"] = statistics.median(times)
+    return out
+
+
+if __name__ == "__main__":  # pragma: no cover
+    print(json.dumps(compare([1, 2, 3], 12, 30.0)))

@@ -293,6 +293,7 @@ struct StepArgs {
   int16_t* rb_dE;         // [cap]
   int64_t rb_cap;
   float* stats;           // [4]: sum |pred - dE|, count, accepted, sum dE accepted
+  int moves;              // moves drawn per step (without replacement)
 };
 
 constexpr int kStepWarps = 16;
@@ -321,31 +322,32 @@ __global__ void __launch_bounds__(kStepWarps * 32, 1) learned_step_kernel(const 
   }
   const int temp = ch.temp_of[c];
   const float T = A.temps[temp];
-  // softmax(-pred / T) over the legal candidates, sampled by inverse CDF
-  float logit[kCand / 32];
+  // softmax(-pred / T) over the legal candidates, sampled by inverse CDF;
+  // with moves > 1 the step draws again without replacement after each move
+  // (candidates are re-checked for legality on the current state).
+  float w[kCand / 32];
   float mx = -INFINITY;
 #pragma unroll
   for (int q = 0; q < kCand / 32; ++q) {
     const int j = lane + 32 * q;
     const int cw = A.cand[(size_t)c * kCand + j];
-    logit[q] = cw < 0 ? -A.pred[(size_t)c * kCand + j] / T : -INFINITY;
-    mx = fmaxf(mx, logit[q]);
+    w[q] = cw < 0 ? -A.pred[(size_t)c * kCand + j] / T : -INFINITY;
+    mx = fmaxf(mx, w[q]);
   }
 #pragma unroll
   for (int o = 16; o; o >>= 1) mx = fmaxf(mx, __shfl_xor_sync(0xffffffffu, mx, o));
-  const uint64_t step = *A.step;
-  const U4 r = philox4x32_10(U4{(uint32_t)step, (uint32_t)(step >> 32), (uint32_t)c, kTagCandidate | 0xFFFFu},
-                             A.k0, A.k1);
-  int chosen = -1;
-  if (mx > -INFINITY) {
-    float w[kCand / 32], tot = 0.f;
 #pragma unroll
-    for (int q = 0; q < kCand / 32; ++q) {
-      w[q] = logit[q] > -INFINITY ? __expf(logit[q] - mx) : 0.f;
-      tot += w[q];
-    }
-    // inclusive prefix over lanes of the per-lane totals (candidate order j = lane + 32 q, by q then lane)
-    float laneq[kCand / 32];
+  for (int q = 0; q < kCand / 32; ++q) w[q] = w[q] > -INFINITY ? __expf(w[q] - mx) : 0.f;
+  const uint64_t step = *A.step;
+  const uint32_t* thr = ch.acc_thresh + (size_t)temp * ch.acc_width;
+  int E = ch.energy[c];
+  int bestE = ch.best_energy[c];
+  uint32_t err = 0;
+  for (int k = 0; k < A.moves; ++k) {
+    const U4 r = philox4x32_10(U4{(uint32_t)step, (uint32_t)(step >> 32), (uint32_t)c,
+                                  kTagCandidate | 0xFF00u | (uint32_t)k}, A.k0, A.k1);
+    // inclusive prefix sums of the weights, candidate order j = lane + 32 q (by q, then lane)
+    float laneq[kCand / 32], qtot[kCand / 32], acc_w = 0.f;
 #pragma unroll
     for (int q = 0; q < kCand / 32; ++q) {
       float x = w[q];
@@ -354,15 +356,12 @@ __global__ void __launch_bounds__(kStepWarps * 32, 1) learned_step_kernel(const 
         const float y = __shfl_up_sync(0xffffffffu, x, o);
         if (lane >= o) x += y;
       }
-      laneq[q] = x;  // prefix within block q
+      laneq[q] = x;
+      qtot[q] = __shfl_sync(0xffffffffu, x, 31);
+      acc_w += qtot[q];
     }
-    float qtot[kCand / 32], acc = 0.f;
-#pragma unroll
-    for (int q = 0; q < kCand / 32; ++q) {
-      qtot[q] = __shfl_sync(0xffffffffu, laneq[q], 31);
-      acc += qtot[q];
-    }
-    const float target = ((float)(r.x >> 8) + 0.5f) * (1.0f / 16777216.0f) * acc;
+    if (!(acc_w > 0.f)) break;  // no legal candidate left
+    const float target = ((float)(r.x >> 8) + 0.5f) * (1.0f / 16777216.0f) * acc_w;
     float before = 0.f;
     int pick = -1;
 #pragma unroll
@@ -373,24 +372,22 @@ __global__ void __launch_bounds__(kStepWarps * 32, 1) learned_step_kernel(const 
       }
       before += qtot[q];
     }
-    if (pick < 0) {  // rounding at the top end: take the last legal candidate
+    if (pick < 0) {  // rounding at the top end: the last candidate with weight
 #pragma unroll
       for (int q = 0; q < kCand / 32; ++q) {
         const unsigned hit = __ballot_sync(0xffffffffu, w[q] > 0.f);
         if (hit) pick = 32 * q + (31 - __clz(hit));
       }
     }
-    chosen = pick;
-  }
-  __syncwarp();
-  int E = ch.energy[c];
-  uint32_t err = 0;
-  if (chosen >= 0) {
-    const int cw = A.cand[(size_t)c * kCand + chosen];
+    if (lane == (pick & 31)) w[pick >> 5] = 0.f;  // without replacement
+    __syncwarp();
+    const int cw = A.cand[(size_t)c * kCand + pick];
     const int u = cw & 0xFF, v = (cw >> 8) & 0xFF;
-    const float p = A.pred[(size_t)c * kCand + chosen];
+    if (k > 0 && !legal_swap(cs, u, v)) continue;  // an earlier move of this step made it illegal
+    const float p = A.pred[(size_t)c * kCand + pick];
     // tuple: features of the state before the move
-    const int64_t slot = (int64_t)((step * (uint64_t)ch.n_chains + (uint64_t)c) % (uint64_t)A.rb_cap);
+    const uint64_t tuple = (step * (uint64_t)ch.n_chains + (uint64_t)c) * (uint64_t)A.moves + (uint64_t)k;
+    const int64_t slot = (int64_t)(tuple % (uint64_t)A.rb_cap);
     if (lane == 0) {
       float f[kCandFeat];
       const int sidx[4] = {u, v, u ^ 1, v ^ 1};
@@ -407,7 +404,6 @@ __global__ void __launch_bounds__(kStepWarps * 32, 1) learned_step_kernel(const 
     for (int s = lane; s < kChainFeat; s += 32)
       A.rb_bad[slot * kChainFeat + s] = (uint8_t)(s < m ? min(bs[s], 255) : 0);
     __syncwarp();
-    const uint32_t* thr = ch.acc_thresh + (size_t)temp * ch.acc_width;
     int dE = 0;
     const int acc = move_exact(cs, bs, m, lut, hist, lane, u, v, r.y, thr, ch.acc_width, E, err, &dE);
     if (lane == 0) {
@@ -420,8 +416,8 @@ __global__ void __launch_bounds__(kStepWarps * 32, 1) learned_step_kernel(const 
         ch.accepted[c] += 1;
       }
     }
-    if (acc && E < ch.best_energy[c]) {
-      if (lane == 0) ch.best_energy[c] = E;
+    if (acc && E < bestE) {
+      bestE = E;
       for (int s = lane; s < m; s += 32) ch.best_cols[(size_t)c * kMaxM + s] = (int16_t)cs[s];
     }
   }
@@ -431,6 +427,7 @@ __global__ void __launch_bounds__(kStepWarps * 32, 1) learned_step_kernel(const 
   }
   if (lane == 0) {
     ch.energy[c] = E;
+    ch.best_energy[c] = bestE;
     if (err && ch.error_word) atomicOr(ch.error_word, err);
     if (ch.global_best) atomicMin(ch.global_best, E);
   }
@@ -693,9 +690,10 @@ int n3_mlp_infer(const n3_mlp* M, int tiles, void* stream) {
   return n3host::check_launch("infer_kernel");
 }
 
-int n3_mlp_step(const n3_chains* ch, const n3_mlp* M, const float* temps, uint64_t seed, void* stream) {
+int n3_mlp_step(const n3_chains* ch, const n3_mlp* M, const float* temps, uint64_t seed, int moves, void* stream) {
   using namespace n3::mlp;
   if (!ch || !M || !temps) return n3host::set_error(N3_ERR_ARG, "null descriptor");
+  if (moves < 1 || moves > kCand) return n3host::set_error(N3_ERR_RANGE, "moves per step %d outside [1, 128]", moves);
   N3_TRY(n3host::ensure_device_tables());
   const size_t smem = n3host::step_smem();
   N3_TRY(n3host::allow_smem(reinterpret_cast<const void*>(learned_step_kernel), smem));
@@ -713,6 +711,7 @@ int n3_mlp_step(const n3_chains* ch, const n3_mlp* M, const float* temps, uint64
   A.rb_dE = M->rb_dE;
   A.rb_cap = M->rb_capacity;
   A.stats = M->stats;
+  A.moves = moves;
   const int grid = (ch->n_chains + kStepWarps - 1) / kStepWarps;
   learned_step_kernel<<<grid, kStepWarps * 32, smem, (cudaStream_t)stream>>>(A);
   N3_TRY(n3host::check_launch("learned_step_kernel"));

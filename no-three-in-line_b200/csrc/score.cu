@@ -97,7 +97,7 @@ struct ColSource {
   __device__ __forceinline__ int col(int b, int n, int s) const { return c[(size_t)b * 2 * n + s]; }
 };
 
-constexpr int kDetWarps = 8;
+constexpr int kDetWarps = 4;  // small CTAs: 4096 states spread evenly over 148 SMs
 
 template <class Src, bool BAD>
 __global__ void __launch_bounds__(kDetWarps * 32) det_kernel(Src src, int B, int n, int32_t* __restrict__ scores,
@@ -145,7 +145,9 @@ __device__ __forceinline__ uint32_t load_checked(const Src& src, int b, int n, i
   return err;
 }
 
-// MODE 0: slope only (scores, badness).  MODE 1: determinant + slope, checked.
+// MODE 0: slope only (scores, badness).  MODE 1: determinant + slope, checked,
+// in this kernel.  MODE 2: slope + check against determinant counts already in
+// `scores` (written by det_kernel on the same stream).
 template <int MODE>
 __global__ void __launch_bounds__(kSlopeWarps * 32) slope_kernel(ColSource src, int B, int n,
                                                                    int32_t* __restrict__ scores,
@@ -171,7 +173,7 @@ __global__ void __launch_bounds__(kSlopeWarps * 32) slope_kernel(ColSource src, 
       if (lane == 0) {
         scores[b] = -1;
         if (error_word) atomicOr(error_word, err);
-        if (MODE == 1) atomicAdd(mismatch, 1);
+        if (MODE != 0) atomicAdd(mismatch, 1);
       }
       if (badness)
         for (int s = lane; s < m; s += 32) badness[(size_t)b * m + s] = -1;
@@ -182,6 +184,11 @@ __global__ void __launch_bounds__(kSlopeWarps * 32) slope_kernel(ColSource src, 
     __syncwarp();
     if (MODE == 0) {
       if (lane == 0) scores[b] = total / 3;
+    } else if (MODE == 2) {  // scores[b] holds the determinant count of this state
+      if (lane == 0 && total != 3 * scores[b]) {
+        atomicAdd(mismatch, 1);
+        if (error_word) atomicOr(error_word, kErrMismatch);
+      }
     } else {
       const int e_det = warp_sum(det_state<false>(cs, n, lane, nullptr));
       if (lane == 0) {
@@ -229,6 +236,7 @@ static int check_common(int B, int n, const void* a, const void* out) {
 
 int prepare_score() {
   N3_TRY(allow_smem(reinterpret_cast<const void*>(n3::slope_kernel<0>), n3::kSlopeSmem));
+  N3_TRY(allow_smem(reinterpret_cast<const void*>(n3::slope_kernel<2>), n3::kSlopeSmem));
   return allow_smem(reinterpret_cast<const void*>(n3::slope_kernel<1>), n3::kSlopeSmem);
 }
 
@@ -281,7 +289,10 @@ int n3_score_checked(const int16_t* cols, int B, int n, int32_t* scores, int32_t
                      uint32_t* error_word, void* stream) {
   N3_TRY(n3host::check_common(B, n, cols, scores));
   if (B > 0 && mismatch == nullptr) return n3host::set_error(N3_ERR_ARG, "null mismatch counter");
-  return n3host::launch_slope<1>(cols, B, n, scores, badness, mismatch, error_word, (cudaStream_t)stream);
+  // Two launches on one stream: the determinant count at full occupancy, then
+  // the independent slope count, which validates each state and compares.
+  N3_TRY(n3host::launch_det(n3::ColSource{cols}, B, n, scores, nullptr, (cudaStream_t)stream));
+  return n3host::launch_slope<2>(cols, B, n, scores, badness, mismatch, error_word, (cudaStream_t)stream);
 }
 
 }  // extern "C"

@@ -44,7 +44,8 @@ _lib.register("n3_mlp_scratch_floats", [ctypes.c_int])
 _lib.register("n3_mlp_pack", [ctypes.POINTER(N3Mlp), _P])
 _lib.register("n3_mlp_candidates", [ctypes.POINTER(N3Chains), ctypes.POINTER(N3Mlp), ctypes.c_uint64, _P])
 _lib.register("n3_mlp_infer", [ctypes.POINTER(N3Mlp), ctypes.c_int, _P])
-_lib.register("n3_mlp_step", [ctypes.POINTER(N3Chains), ctypes.POINTER(N3Mlp), _P, ctypes.c_uint64, _P])
+_lib.register("n3_mlp_step", [ctypes.POINTER(N3Chains), ctypes.POINTER(N3Mlp), _P, ctypes.c_uint64, ctypes.c_int,
+                              _P])
 _lib.register("n3_mlp_train", [ctypes.POINTER(N3Mlp), ctypes.c_int, ctypes.c_int, ctypes.c_float, ctypes.c_uint64,
                                _P, _P, _P, _P, _P])
 
@@ -84,7 +85,7 @@ class LearnedProposal:
     """Learned proposals driving a TemperingChains object's chains."""
 
     def __init__(self, chains: TemperingChains, *, seed: int = 1, ring_capacity: int = 1 << 21,
-                 batch: int = 4096, lr: float = 1e-3, params: np.ndarray | None = None):
+                 batch: int = 4096, lr: float = 1e-3, params: np.ndarray | None = None, moves: int = 1):
         t = _lib.torch()
         self.ch = chains
         dev = chains.device
@@ -92,6 +93,7 @@ class LearnedProposal:
         self.seed = int(seed) & 0xFFFFFFFFFFFFFFFF
         self.batch = batch
         self.lr = lr
+        self.moves = int(moves)
         p = init_params(seed) if params is None else np.asarray(params, np.float32)
         count = int(_lib.lib().n3_mlp_param_count())
         if p.shape != (count,):
@@ -144,11 +146,12 @@ class LearnedProposal:
         self.propose_scores(stream)
         cd = self.ch._descriptor()
         _lib.check(_lib.lib().n3_mlp_step(ctypes.byref(cd), ctypes.byref(self._desc), self.temps.data_ptr(),
-                                          self.seed, _lib.stream_ptr(stream)), "n3_mlp_step")
+                                          self.seed, self.moves, _lib.stream_ptr(stream)), "n3_mlp_step")
 
     def train(self, stream=None):
         """One Adam step on a batch from the ring buffer."""
-        _lib.check(_lib.lib().n3_mlp_train(ctypes.byref(self._desc), self.ch.cols.shape[0], self.batch, self.lr,
+        _lib.check(_lib.lib().n3_mlp_train(ctypes.byref(self._desc), self.ch.cols.shape[0] * self.moves,
+                                           self.batch, self.lr,
                                            self.seed ^ 0x5A5A5A5A, self.scratch.data_ptr(), self.grads.data_ptr(),
                                            self.adam_m.data_ptr(), self.adam_v.data_ptr(), _lib.stream_ptr(stream)),
                    "n3_mlp_train")
@@ -236,7 +239,8 @@ class LearnedProposal:
         if hit is not None:
             hit = (hit[0], hit[1], seconds)
         C = self.ch.cols.shape[0]
-        return RunResult(done // 150, done // 150, done * C, seconds, int(self.ch.best_energy.min().item()), hit)
+        return RunResult(done // 150, done // 150, done * C * self.moves, seconds, int(self.ch.best_energy.min().item()),
+                         hit)
 
     def release_graphs(self):
         for h in self._graphs.values():

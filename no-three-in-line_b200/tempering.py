@@ -333,8 +333,12 @@ class TemperingChains:
             ns = (int(h[2]) & 0xFFFFFFFF) | ((int(h[3]) & 0xFFFFFFFF) << 32)
             hit = (int(h[0]), int(h[1]) & 0xFFFFFFFF, (ns - t0_ns) / 1e9)
         swept = done * exchange_every
-        m_tot = int(2 * np.repeat(self.ladder_n_host, self.L).sum())
-        return RunResult(done, swept, swept * m_tot, seconds, int(self.best_energy.min().item()), hit)
+        if ladder_sweeps is None:
+            proposals = swept * int(2 * np.repeat(self.ladder_n_host, self.L).sum())
+        else:  # each launch ran every ladder for its own number of sweeps
+            launched = done // rounds_per_launch
+            proposals = launched * int((np.asarray(ladder_sweeps) * 2 * self.ladder_n_host).sum()) * self.L
+        return RunResult(done, swept, proposals, seconds, int(self.best_energy.min().item()), hit)
 
     def _capture(self, cfg: N3TemperConfig):
         """CUDA graph of one launch with `cfg` (arguments frozen at capture)."""

@@ -130,3 +130,15 @@ def test_graph_and_eager_agree(cuda):
         lp.run(100, exchange_every=100, train_every=0, block=50, graph=graph, warm=False)
         runs.append((ch.cols.cpu().numpy(), ch.energy.cpu().numpy(), lp.params.cpu().numpy()))
     assert np.array_equal(runs[0][0], runs[1][0]) and np.array_equal(runs[0][1], runs[1][1])
+
+
+def test_several_moves_per_step_keep_energies_exact(cuda):
+    """moves=4: four draws without replacement per scoring pass, each re-checked
+    for legality on the current state and accepted by its exact delta."""
+    ch = make(chains=64, L=16, seed=8)
+    lp = learned.LearnedProposal(ch, seed=8, ring_capacity=1 << 16, batch=512, moves=4)
+    lp.run(200, exchange_every=200, train_every=10, block=50)
+    ch.validate()
+    assert int(ch.error_word.item()) == 0
+    st = lp.read_stats()
+    assert st.proposals > 64 * 201 * 3 and st.accepted > 0
