@@ -61,9 +61,11 @@ def run_learned(seed: int, target: int, budget: float, *, n=75, chains=2048, lad
     ch = seeded_chains(n, chains, ladder, seed)
     lp = LearnedProposal(ch, seed=seed, moves=moves)
     name = "learned" if moves == 1 else f"learned-x{moves}"
+    # exchange every 10 sweeps' worth of proposals (10 * 2n), as the uniform chains do
+    every = max(block, int(round(10 * 2 * n / moves / block)) * block)
     traj, spent, first = [], 0.0, True
     while spent < budget:
-        res = lp.run(1500, exchange_every=1500, train_every=train_every, block=block, target=target, warm=first)
+        res = lp.run(every, exchange_every=every, train_every=train_every, block=block, target=target, warm=first)
         first = False
         if res.hit is not None:
             spent += res.hit[2]
@@ -101,6 +103,17 @@ def compare(seeds, target: int, budget: float, *, learned_moves=(1,), **kw) -> d
     for method in methods:
         times = [time_to_reach(r.trajectory, common) for r in runs if r.method == method]
         out[method]["median_s_to_common_level"] = statistics.median(times)
+    # time to each level of a ladder of energies, censored at the budget
+    levels = list(range(common, min(r.best for r in runs) - 1, -1))
+    ladder = {}
+    for level in levels:
+        row = {}
+        for method in methods:
+            ts = [time_to_reach(r.trajectory, level) for r in runs if r.method == method]
+            row[method] = {"median_s": statistics.median(budget if t is None else t for t in ts),
+                           "reached": sum(t is not None for t in ts)}
+        ladder[str(level)] = row
+    out["time_to_level"] = ladder
     return out
 
 

@@ -46,16 +46,19 @@ constexpr int oW3 = oB2 + kH;
 constexpr int oB3 = oW3 + kH;
 constexpr int kParams = oB3 + 4;  // padded to a multiple of 4
 
-// Inference shared-memory map (offsets from a 1024-aligned base).
-constexpr uint32_t sW2 = 0;                       // SW128 image, 4 x [256 x 128 B]
-constexpr uint32_t sA2 = sW2 + 4 * kH * 128;      // SW128, 4 x [128 x 128 B]
-constexpr uint32_t sW1a = sA2 + 4 * kCand * 128;  // INTERLEAVE K=16, 256 rows
-constexpr uint32_t sA1 = sW1a + kH * 32;          // INTERLEAVE K=16, 128 rows
-constexpr uint32_t sC1 = sA1 + kCand * 32;        // fp32[256] chain part of layer 1
-constexpr uint32_t sB2 = sC1 + kH * 4;
+// Inference shared-memory map (offsets from a 1024-aligned base).  A1 and the
+// chain part are double-buffered so the next tile loads during this one.
+constexpr uint32_t sW2 = 0;                        // SW128 image, 4 x [256 x 128 B]
+constexpr uint32_t sA2 = sW2 + 4 * kH * 128;       // SW128, 4 x [128 x 128 B]
+constexpr uint32_t sW1a = sA2 + 4 * kCand * 128;   // INTERLEAVE K=16, 256 rows
+constexpr uint32_t sA1 = sW1a + kH * 32;           // 2 x INTERLEAVE K=16, 128 rows
+constexpr uint32_t sC1 = sA1 + 2 * kCand * 32;     // 2 x fp32[256] chain part of layer 1
+constexpr uint32_t sB2 = sC1 + 2 * kH * 4;
 constexpr uint32_t sW3 = sB2 + kH * 4;
-constexpr uint32_t sBar = sW3 + kH * 4;           // mbarrier (8 B) + TMEM address (4 B) + abort flag
-constexpr uint32_t kInferSmem = sBar + 64 + 1024; // + alignment slack
+constexpr uint32_t sPart = sW3 + kH * 4;           // fp32[2][128] half dot products
+constexpr uint32_t sBar = sPart + 2 * kCand * 4;   // 2 mbarriers, TMEM address, abort flag
+constexpr uint32_t kInferSmem = sBar + 64 + 1024;  // + alignment slack
+constexpr int kInferThreads = 256;                 // 8 warps: two per tensor-memory lane quarter
 constexpr uint32_t kWaitTries = 1u << 24;
 
 __device__ __forceinline__ uint16_t bf16_bits(float x) {
@@ -155,68 +158,92 @@ __device__ __forceinline__ void copy16(uint8_t* dst, const uint8_t* src, int byt
   for (int i = tid; i < bytes / 16; i += nthreads) d[i] = s[i];
 }
 
-__global__ void __launch_bounds__(128, 1) infer_kernel(const InferArgs A) {
+__device__ __forceinline__ void cp_async16(uint32_t saddr, const void* g) {
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(saddr), "l"(g) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_group 0;" ::: "memory"); }
+
+// Prefetch of tile t's candidate features (4 KB) and chain part (1 KB).
+__device__ __forceinline__ void load_tile_async(uint32_t base, int buf, const InferArgs& A, int t, int tid) {
+  const uint8_t* a1 = A.a1_img + (size_t)t * (kCand * 32);
+  const float* c1 = A.c1 + (size_t)t * kH;
+  const uint32_t sa = base + sA1 + (uint32_t)buf * (kCand * 32);
+  const uint32_t sc = base + sC1 + (uint32_t)buf * (kH * 4);
+  for (int i = tid; i < kCand * 32 / 16; i += kInferThreads) cp_async16(sa + 16 * i, a1 + 16 * i);
+  for (int i = tid; i < kH * 4 / 16; i += kInferThreads) cp_async16(sc + 16 * i, c1 + 4 * i);
+  cp_async_commit();
+}
+
+// Per CTA: tiles t0, t0 + G, ...  Pipeline per tile i (D1 = TMEM columns
+// 0..255, D2 = 256..511):
+//   wait MMA1(i) -> epilogue 1 (D1 + chain part -> A2) -> issue MMA2(i) ->
+//   issue MMA1(i+1) from the prefetched A1 -> wait MMA2(i) -> epilogue 2.
+// Eight warps: warp w reads TMEM lanes 32*(w%4).., columns 128*(w/4)...
+__global__ void __launch_bounds__(kInferThreads, 1) infer_kernel(const InferArgs A) {
   extern __shared__ uint8_t smem_raw[];
   const uint32_t raw = umma::smem_addr(smem_raw);
   uint8_t* sm = smem_raw + ((1024u - (raw & 1023u)) & 1023u);  // 1024-aligned base
   const uint32_t base = umma::smem_addr(sm);
-  const int tid = threadIdx.x, warp = tid >> 5;
-  float* c1s = reinterpret_cast<float*>(sm + sC1);
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  const int quarter = warp & 3, half = warp >> 2;
   float* b2s = reinterpret_cast<float*>(sm + sB2);
   float* w3s = reinterpret_cast<float*>(sm + sW3);
-  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(sm + sBar + 8);
-  int* abort_flag = reinterpret_cast<int*>(sm + sBar + 16);
-  const uint32_t mbar = base + sBar;
+  float* part = reinterpret_cast<float*>(sm + sPart);
+  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(sm + sBar + 16);
+  int* abort_flag = reinterpret_cast<int*>(sm + sBar + 24);
+  const uint32_t bar1 = base + sBar, bar2 = base + sBar + 8;
+  const int stride = gridDim.x;
 
-  copy16(sm + sW2, A.w2_img, 4 * kH * 128, tid, blockDim.x);
-  copy16(sm + sW1a, A.w1a_img, kH * 32, tid, blockDim.x);
-  for (int i = tid; i < kH; i += blockDim.x) {
+  if (blockIdx.x < A.tiles) load_tile_async(base, 0, A, blockIdx.x, tid);
+  copy16(sm + sW2, A.w2_img, 4 * kH * 128, tid, kInferThreads);
+  copy16(sm + sW1a, A.w1a_img, kH * 32, tid, kInferThreads);
+  for (int i = tid; i < kH; i += kInferThreads) {
     b2s[i] = A.P[oB2 + i];
     w3s[i] = A.P[oW3 + i];
   }
   const float b3 = A.P[oB3];
   if (warp == 0) {
-    umma::tmem_alloc(base + sBar + 8, 256);
+    umma::tmem_alloc(base + sBar + 16, 512);
     umma::tmem_relinquish();
   }
   if (tid == 0) {
-    umma::mbar_init(mbar, 1);
+    umma::mbar_init(bar1, 1);
+    umma::mbar_init(bar2, 1);
     umma::mbar_fence_init();
     *abort_flag = 0;
   }
+  cp_async_wait_all();
+  umma::fence_async_smem();
   umma::fence_before_sync();
   __syncthreads();
   umma::fence_after_sync();
   const uint32_t tmem = *tmem_slot;
-  const uint32_t lane_base = tmem + ((uint32_t)(32 * warp) << 16);
+  const uint32_t d1 = tmem, d2 = tmem + 256u;
+  const uint32_t lane_off = (uint32_t)(32 * quarter) << 16;
   const uint32_t idesc = umma::idesc_bf16_f32(128, 256);
-  uint32_t phase = 0;
-  const int row = tid;  // candidate row = TMEM lane
-
-  for (int t = blockIdx.x; t < A.tiles; t += gridDim.x) {
-    copy16(sm + sA1, A.a1_img + (size_t)t * (kCand * 32), kCand * 32, tid, blockDim.x);
-    for (int i = tid; i < kH; i += blockDim.x) c1s[i] = A.c1[(size_t)t * kH + i];
-    umma::fence_async_smem();
-    umma::fence_before_sync();
-    __syncthreads();
+  const int row = 32 * quarter + lane;
+  uint32_t ph1 = 0, ph2 = 0;
+  if (tid == 0 && blockIdx.x < A.tiles) {
+    umma::mma_bf16(d1, umma::desc_interleave(base + sA1, 128, 256), umma::desc_interleave(base + sW1a, 128, 256),
+                   idesc, 0u);
+    umma::commit(bar1);
+  }
+  int buf = 0;
+  for (int t = blockIdx.x; t < A.tiles; t += stride, buf ^= 1) {
+    const bool has_next = t + stride < A.tiles;
+    if (has_next) load_tile_async(base, buf ^ 1, A, t + stride, tid);
+    if (!umma::mbar_wait(bar1, ph1, kWaitTries)) atomicExch(abort_flag, 1);
+    ph1 ^= 1u;
     umma::fence_after_sync();
-    if (tid == 0) {
-      umma::mma_bf16(tmem, umma::desc_interleave(base + sA1, 128, 256), umma::desc_interleave(base + sW1a, 128, 256),
-                     idesc, 0u);
-      umma::commit(mbar);
-    }
-    if (!umma::mbar_wait(mbar, phase, kWaitTries)) atomicExch(abort_flag, 1);
-    phase ^= 1u;
-    umma::fence_after_sync();
-    __syncthreads();
-    if (*abort_flag) break;
-    // epilogue 1: h1 = relu(D1 + chain part) -> bf16 -> A2 (SW128)
+    // epilogue 1: h1 = relu(D1 + chain part) -> bf16 -> A2 (SW128), this warp's 128 columns
+    const float* c1s = reinterpret_cast<const float*>(sm + sC1 + (uint32_t)buf * (kH * 4));
 #pragma unroll 1
-    for (int j = 0; j < kH / 32; ++j) {
+    for (int j = 4 * half; j < 4 * half + 4; ++j) {
       float v[32];
-      umma::tmem_ld32(lane_base + 32 * j, v);
+      umma::tmem_ld32(d1 + lane_off + 32 * j, v);
 #pragma unroll
-      for (int q = 0; q < 4; ++q) {  // 8 values -> one 16-byte chunk
+      for (int q = 0; q < 4; ++q) {
         uint32_t w[4];
 #pragma unroll
         for (int e = 0; e < 4; ++e) {
@@ -229,47 +256,57 @@ __global__ void __launch_bounds__(128, 1) infer_kernel(const InferArgs A) {
             make_uint4(w[0], w[1], w[2], w[3]);
       }
     }
+    cp_async_wait_all();  // next tile's A1 / chain part have landed (this thread's copies)
     umma::fence_async_smem();
     umma::fence_before_sync();
     __syncthreads();
     umma::fence_after_sync();
+    if (*abort_flag) break;
     if (tid == 0) {
 #pragma unroll
       for (int s = 0; s < kH / 16; ++s) {
         const uint32_t koff = (uint32_t)(s & 3) * 32u;  // K = 16 step inside a 64-wide slice
         const uint64_t ad = umma::desc_sw128(base + sA2 + (uint32_t)(s >> 2) * (kCand * 128) + koff);
         const uint64_t bd = umma::desc_sw128(base + sW2 + (uint32_t)(s >> 2) * (kH * 128) + koff);
-        umma::mma_bf16(tmem, ad, bd, idesc, s > 0 ? 1u : 0u);
+        umma::mma_bf16(d2, ad, bd, idesc, s > 0 ? 1u : 0u);
       }
-      umma::commit(mbar);
+      umma::commit(bar2);
+      if (has_next) {  // D1 was fully read by epilogue 1 above
+        const uint32_t a1 = base + sA1 + (uint32_t)(buf ^ 1) * (kCand * 32);
+        umma::mma_bf16(d1, umma::desc_interleave(a1, 128, 256), umma::desc_interleave(base + sW1a, 128, 256),
+                       idesc, 0u);
+        umma::commit(bar1);
+      }
     }
-    if (!umma::mbar_wait(mbar, phase, kWaitTries)) atomicExch(abort_flag, 1);
-    phase ^= 1u;
+    if (!umma::mbar_wait(bar2, ph2, kWaitTries)) atomicExch(abort_flag, 1);
+    ph2 ^= 1u;
     umma::fence_after_sync();
-    __syncthreads();
-    if (*abort_flag) break;
-    // epilogue 2: relu(D2 + b2) . w3 + b3
-    float acc = b3;
+    // epilogue 2: relu(D2 + b2) . w3 over this warp's 128 columns
+    float acc = 0.f;
 #pragma unroll 1
-    for (int j = 0; j < kH / 32; ++j) {
+    for (int j = 4 * half; j < 4 * half + 4; ++j) {
       float v[32];
-      umma::tmem_ld32(lane_base + 32 * j, v);
+      umma::tmem_ld32(d2 + lane_off + 32 * j, v);
 #pragma unroll
       for (int e = 0; e < 32; ++e) acc = fmaf(fmaxf(v[e] + b2s[32 * j + e], 0.f), w3s[32 * j + e], acc);
     }
-    A.pred[(size_t)t * kCand + row] = acc * kTargetScale;
+    part[half * kCand + row] = acc;
     umma::fence_before_sync();
     __syncthreads();
+    if (half == 0) A.pred[(size_t)t * kCand + row] = (part[row] + part[kCand + row] + b3) * kTargetScale;
+    if (*abort_flag) break;
   }
   if (*abort_flag && tid == 0) {
     if (A.error_word) atomicOr(A.error_word, kErrTimeout);
-    umma::mbar_wait(mbar, phase ^ 1u, kWaitTries);  // bounded wait for the MMA still in flight
+    umma::mbar_wait(bar1, ph1, kWaitTries);  // bounded waits for MMAs still in flight
+    umma::mbar_wait(bar2, ph2, kWaitTries);
   }
+  cp_async_wait_all();
   umma::fence_before_sync();
   __syncthreads();
   if (warp == 0) {
     umma::fence_after_sync();
-    umma::tmem_dealloc(tmem, 256);
+    umma::tmem_dealloc(tmem, 512);
   }
 }
 
@@ -686,7 +723,7 @@ int n3_mlp_infer(const n3_mlp* M, int tiles, void* stream) {
   A.tiles = tiles;
   A.error_word = M->error_word;
   const int grid = tiles < n3host::sm_count() ? tiles : n3host::sm_count();
-  infer_kernel<<<grid, 128, kInferSmem, (cudaStream_t)stream>>>(A);
+  infer_kernel<<<grid, kInferThreads, kInferSmem, (cudaStream_t)stream>>>(A);
   return n3host::check_launch("infer_kernel");
 }
 

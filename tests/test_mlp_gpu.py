@@ -36,7 +36,9 @@ def features(cols, bad, n, u, v):
 
 
 def test_inference_matches_bf16_reference(cuda):
-    ch = make()
+    # 480 chain tiles: more than one tile per SM, so the kernel's prefetch /
+    # overlapped-MMA pipeline runs several iterations per CTA
+    ch = make(chains=480, L=16)
     lp = learned.LearnedProposal(ch, seed=9, ring_capacity=1 << 12, batch=256)
     lp.propose_scores()
     P = lp.params.cpu().numpy().astype(np.float64)
@@ -52,7 +54,7 @@ def test_inference_matches_bf16_reference(cuda):
     pred = lp.pred.cpu().numpy()
     img = lp.a1_img.cpu().numpy().reshape(-1, 4096)
     c1_dev = lp.c1.cpu().numpy()
-    for c in range(cols.shape[0]):
+    for c in list(range(0, cols.shape[0], 13)) + [cols.shape[0] - 1]:
         x_chain = bad[c] / 16.0
         c1 = b1 + W1[:, 12:162] @ x_chain
         assert np.allclose(c1_dev[c], c1, rtol=1e-5, atol=1e-5)
