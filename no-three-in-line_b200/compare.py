@@ -53,7 +53,7 @@ def run_plain(seed: int, target: int, budget: float, *, n=75, chains=2048, ladde
 
 
 def run_learned(seed: int, target: int, budget: float, *, n=75, chains=2048, ladder=64, block=50,
-                train_every=10, moves=1):
+                train_every=10, moves=1, exchange_steps=None):
     """Learned-proposal tempering; `moves` > 1 draws that many moves per step
     (without replacement) from each step's scored candidates."""
     from .learned import LearnedProposal
@@ -61,8 +61,9 @@ def run_learned(seed: int, target: int, budget: float, *, n=75, chains=2048, lad
     ch = seeded_chains(n, chains, ladder, seed)
     lp = LearnedProposal(ch, seed=seed, moves=moves)
     name = "learned" if moves == 1 else f"learned-x{moves}"
-    # exchange every 10 sweeps' worth of proposals (10 * 2n), as the uniform chains do
-    every = max(block, int(round(10 * 2 * n / moves / block)) * block)
+    # exchange every 10 sweeps, a sweep being 2n learned steps (scoring passes);
+    # with moves > 1 each step makes up to `moves` proposals
+    every = exchange_steps if exchange_steps else 10 * 2 * n
     traj, spent, first = [], 0.0, True
     while spent < budget:
         res = lp.run(every, exchange_every=every, train_every=train_every, block=block, target=target, warm=first)

@@ -528,11 +528,13 @@ __global__ void __launch_bounds__(256) gemm_kernel(int M, int N, int K, const fl
   const int kb = blockIdx.z * kchunk, ke = min(K, kb + kchunk);
   float acc[4][4] = {};
   for (int k0 = kb; k0 < ke; k0 += 16) {
+    // Tile loads: consecutive threads walk whichever index is contiguous in memory.
     for (int i = threadIdx.x; i < 16 * 64; i += 256) {
-      const int kk = i / 64, mm = i % 64;
-      const int gk = k0 + kk;
-      As[kk][mm] = (m0 + mm < M && gk < ke) ? A[(size_t)(m0 + mm) * sam + (size_t)gk * sak] : 0.f;
-      Bs[kk][mm] = (n0 + mm < N && gk < ke) ? Bm[(size_t)gk * sbk + (size_t)(n0 + mm) * sbn] : 0.f;
+      const int ka = sak == 1 ? (i & 15) : (i >> 6), ma = sak == 1 ? (i >> 4) : (i & 63);
+      const int kb = sbk == 1 ? (i & 15) : (i >> 6), nb = sbk == 1 ? (i >> 4) : (i & 63);
+      const int gka = k0 + ka, gkb = k0 + kb;
+      As[ka][ma] = (m0 + ma < M && gka < ke) ? A[(size_t)(m0 + ma) * sam + (size_t)gka * sak] : 0.f;
+      Bs[kb][nb] = (n0 + nb < N && gkb < ke) ? Bm[(size_t)gkb * sbk + (size_t)(n0 + nb) * sbn] : 0.f;
     }
     __syncthreads();
 #pragma unroll
@@ -599,14 +601,17 @@ __global__ void head_kernel(int B, const float* __restrict__ H2, const float* __
   for (int k = lane; k < kH; k += 32) dZ2[(size_t)b * kH + k] = Z2[(size_t)b * kH + k] > 0.f ? g * P[oW3 + k] : 0.f;
 }
 
-// column sums: out[n] = sum_b M[b][n] (+ for gw3: sum_b H2[b][n] d[b])
+// Column sums added into a zeroed `out`: out[n] += sum_b M[b][n] (* scale[b]).
+// Block (x, y) sums rows [y * kColRows, ...) of columns x * blockDim.x + t.
+constexpr int kColRows = 128;
 __global__ void colsum_kernel(int B, int N, const float* __restrict__ Mx, const float* __restrict__ scale,
                               float* __restrict__ out) {
   const int n = blockIdx.x * blockDim.x + threadIdx.x;
   if (n >= N) return;
+  const int b0 = blockIdx.y * kColRows, b1 = min(B, b0 + kColRows);
   float acc = 0.f;
-  for (int b = 0; b < B; ++b) acc = fmaf(Mx[(size_t)b * N + n], scale ? scale[b] : 1.f, acc);
-  out[n] = acc;
+  for (int b = b0; b < b1; ++b) acc = fmaf(Mx[(size_t)b * N + n], scale ? scale[b] : 1.f, acc);
+  atomicAdd(out + n, acc);
 }
 
 __global__ void sum_kernel(int B, const float* __restrict__ v, float* __restrict__ out) {
@@ -784,19 +789,19 @@ int n3_mlp_train(const n3_mlp* M, int n_chains, int batch, float lr, uint64_t se
   gemm_kernel<1><<<g_fwd, 256, 0, st>>>(B, kH, kH, H1, kH, 1, P + oW2, 1, kH, H2, kH, P + oB2, Z2);
   head_kernel<<<(B + 7) / 8, 256, 0, st>>>(B, H2, Z2, P, y, d, dZ2, loss);
   // gradients of the head and layer 2
-  colsum_kernel<<<(kH + 127) / 128, 128, 0, st>>>(B, kH, H2, d, grads + oW3);
+  colsum_kernel<<<dim3((kH + 127) / 128, (B + kColRows - 1) / kColRows), 128, 0, st>>>(B, kH, H2, d, grads + oW3);
   sum_kernel<<<1, 1024, 0, st>>>(B, d, grads + oB3);
   const int splits = B >= 2048 ? 16 : 4;
   // gW2[n][k] = sum_b dZ2[b][n] H1[b][k]
   gemm_kernel<0><<<dim3(kH / 64, kH / 64, splits), 256, 0, st>>>(kH, kH, B, dZ2, 1, kH, H1, kH, 1, grads + oW2, kH,
                                                                    nullptr, nullptr);
-  colsum_kernel<<<(kH + 127) / 128, 128, 0, st>>>(B, kH, dZ2, nullptr, grads + oB2);
+  colsum_kernel<<<dim3((kH + 127) / 128, (B + kColRows - 1) / kColRows), 128, 0, st>>>(B, kH, dZ2, nullptr, grads + oB2);
   // dZ1 = (dZ2 W2) * (Z1 > 0)            (B(k, n) = W2[k*256 + n])
   gemm_kernel<2><<<g_fwd, 256, 0, st>>>(B, kH, kH, dZ2, kH, 1, P + oW2, kH, 1, dZ1, kH, nullptr, Z1);
   // gW1[n][k] = sum_b dZ1[b][n] X[b][k]
   gemm_kernel<0><<<dim3(kIn / 64, kH / 64, splits), 256, 0, st>>>(kH, kIn, B, dZ1, 1, kH, X, kIn, 1, grads + oW1,
                                                                     kIn, nullptr, nullptr);
-  colsum_kernel<<<(kH + 127) / 128, 128, 0, st>>>(B, kH, dZ1, nullptr, grads + oB1);
+  colsum_kernel<<<dim3((kH + 127) / 128, (B + kColRows - 1) / kColRows), 128, 0, st>>>(B, kH, dZ1, nullptr, grads + oB1);
   adam_kernel<<<(kParams + 255) / 256, 256, 0, st>>>(kParams, P, grads, adam_m, adam_v, lr, 0.9f, 0.999f, 1e-8f,
                                                      M->counters);
   bump_kernel<<<1, 1, 0, st>>>(M->counters, 1);
@@ -886,16 +891,16 @@ extern "C" int n3_mlp_train_noalloc(const n3_mlp* M, int n_chains, int batch, fl
   gemm_kernel<1><<<g_fwd, 256, 0, st>>>(B, kH, kIn, X, kIn, 1, P + oW1, 1, kIn, H1, kH, P + oB1, Z1);
   gemm_kernel<1><<<g_fwd, 256, 0, st>>>(B, kH, kH, H1, kH, 1, P + oW2, 1, kH, H2, kH, P + oB2, Z2);
   head_kernel<<<(B + 7) / 8, 256, 0, st>>>(B, H2, Z2, P, y, d, dZ2, loss);
-  colsum_kernel<<<(kH + 127) / 128, 128, 0, st>>>(B, kH, H2, d, grads + oW3);
+  colsum_kernel<<<dim3((kH + 127) / 128, (B + kColRows - 1) / kColRows), 128, 0, st>>>(B, kH, H2, d, grads + oW3);
   sum_kernel<<<1, 1024, 0, st>>>(B, d, grads + oB3);
   const int splits = 4;
   gemm_kernel<0><<<dim3(kH / 64, kH / 64, splits), 256, 0, st>>>(kH, kH, B, dZ2, 1, kH, H1, kH, 1, grads + oW2, kH,
                                                                    nullptr, nullptr);
-  colsum_kernel<<<(kH + 127) / 128, 128, 0, st>>>(B, kH, dZ2, nullptr, grads + oB2);
+  colsum_kernel<<<dim3((kH + 127) / 128, (B + kColRows - 1) / kColRows), 128, 0, st>>>(B, kH, dZ2, nullptr, grads + oB2);
   gemm_kernel<2><<<g_fwd, 256, 0, st>>>(B, kH, kH, dZ2, kH, 1, P + oW2, kH, 1, dZ1, kH, nullptr, Z1);
   gemm_kernel<0><<<dim3(kIn / 64, kH / 64, splits), 256, 0, st>>>(kH, kIn, B, dZ1, 1, kH, X, kIn, 1, grads + oW1,
                                                                     kIn, nullptr, nullptr);
-  colsum_kernel<<<(kH + 127) / 128, 128, 0, st>>>(B, kH, dZ1, nullptr, grads + oB1);
+  colsum_kernel<<<dim3((kH + 127) / 128, (B + kColRows - 1) / kColRows), 128, 0, st>>>(B, kH, dZ1, nullptr, grads + oB1);
   adam_kernel<<<(kParams + 255) / 256, 256, 0, st>>>(kParams, P, grads, adam_m, adam_v, lr, 0.9f, 0.999f, 1e-8f,
                                                      M->counters);
   bump_kernel<<<1, 1, 0, st>>>(M->counters, 1);
