@@ -64,7 +64,8 @@ def parse():
     ap.add_argument("--budget", type=float, default=30.0, help="time-to-target: device seconds per run")
     ap.add_argument("--target", type=int, default=12, help="time-to-target: energy target")
     ap.add_argument("--learned-moves", type=str, default="1",
-                    help="time-to-target: comma-separated moves per learned step to compare (1 = one move per step)")
+                    help="time-to-target: comma-separated moves per learned step to compare (1 = one move per "
+                         "step); learned: the first value is the moves per step")
     return ap.parse_args()
 
 
@@ -270,7 +271,8 @@ def run_chain_mode(args):
         step = lambda: ch.run(10, exchange_every=10, sweeps_per_launch=10)  # noqa: E731
         per_step, unit, what = 2048 * 150 * 10, "deltas/s", "exact swap deltas (proposals)"
     else:
-        lp = learned.LearnedProposal(ch, seed=1)
+        moves = int(args.learned_moves.split(",")[0])
+        lp = learned.LearnedProposal(ch, seed=1, moves=moves)
         lp.run(50, exchange_every=50, train_every=10, block=50)
         step = lambda: lp.run(50, exchange_every=50, train_every=10, block=50, warm=False)  # noqa: E731
         per_step, unit, what = 2048 * 128 * 50, "candidates/s", "MLP-scored candidates"
@@ -286,7 +288,8 @@ def run_chain_mode(args):
             "scaling": "weak", "vs_baseline": None, "dtype": "int32" if args.mode == "tempering" else "bf16",
             "data": "synthetic: random_state(75, Random(91001+c)) chain starts",
             "config": {"workload": f"n=75, 2048 chains, 32 ladders x 64 temperatures (0.05..5.0): {what}",
-                       "mode": args.mode}, "best_E": int(ch.best_energy.min().item())}
+                       "mode": args.mode, **({"moves_per_step": moves} if args.mode == "learned" else {})},
+            "best_E": int(ch.best_energy.min().item())}
     print(json.dumps(line), flush=True)
     return 0
 

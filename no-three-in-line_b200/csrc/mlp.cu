@@ -380,6 +380,7 @@ __global__ void __launch_bounds__(kStepWarps * 32, 1) learned_step_kernel(const 
   int E = ch.energy[c];
   int bestE = ch.best_energy[c];
   uint32_t err = 0;
+  float st_abs = 0.f, st_n = 0.f, st_acc = 0.f, st_dE = 0.f;  // this chain's statistics (lane-uniform)
   for (int k = 0; k < A.moves; ++k) {
     const U4 r = philox4x32_10(U4{(uint32_t)step, (uint32_t)(step >> 32), (uint32_t)c,
                                   kTagCandidate | 0xFF00u | (uint32_t)k}, A.k0, A.k1);
@@ -445,13 +446,13 @@ __global__ void __launch_bounds__(kStepWarps * 32, 1) learned_step_kernel(const 
     const int acc = move_exact(cs, bs, m, lut, hist, lane, u, v, r.y, thr, ch.acc_width, E, err, &dE);
     if (lane == 0) {
       A.rb_dE[slot] = (int16_t)max(-32768, min(32767, dE));
-      atomicAdd(A.stats + 0, fabsf(p - (float)dE));
-      atomicAdd(A.stats + 1, 1.0f);
-      if (acc) {
-        atomicAdd(A.stats + 2, 1.0f);
-        atomicAdd(A.stats + 3, (float)dE);
-        ch.accepted[c] += 1;
-      }
+      if (acc) ch.accepted[c] += 1;
+    }
+    st_abs += fabsf(p - (float)dE);
+    st_n += 1.0f;
+    if (acc) {
+      st_acc += 1.0f;
+      st_dE += (float)dE;
     }
     if (acc && E < bestE) {
       bestE = E;
@@ -467,6 +468,11 @@ __global__ void __launch_bounds__(kStepWarps * 32, 1) learned_step_kernel(const 
     ch.best_energy[c] = bestE;
     if (err && ch.error_word) atomicOr(ch.error_word, err);
     if (ch.global_best) atomicMin(ch.global_best, E);
+    // one set of statistics atomics per chain and step, not per move
+    atomicAdd(A.stats + 0, st_abs);
+    atomicAdd(A.stats + 1, st_n);
+    atomicAdd(A.stats + 2, st_acc);
+    atomicAdd(A.stats + 3, st_dE);
   }
 }
 
@@ -527,16 +533,39 @@ __global__ void __launch_bounds__(256) gemm_kernel(int M, int N, int K, const fl
   const int kchunk = (K + gridDim.z - 1) / gridDim.z;
   const int kb = blockIdx.z * kchunk, ke = min(K, kb + kchunk);
   float acc[4][4] = {};
-  for (int k0 = kb; k0 < ke; k0 += 16) {
-    // Tile loads: consecutive threads walk whichever index is contiguous in memory.
-    for (int i = threadIdx.x; i < 16 * 64; i += 256) {
+  // Each thread moves 4 A and 4 B elements per 16-deep tile; consecutive threads
+  // walk whichever index is contiguous in memory.  The next tile is fetched into
+  // registers while the current one is multiplied.
+  float ra[4], rb[4];
+  auto fetch = [&](int k0) {
+#pragma unroll
+    for (int r = 0; r < 4; ++r) {
+      const int i = threadIdx.x + 256 * r;
       const int ka = sak == 1 ? (i & 15) : (i >> 6), ma = sak == 1 ? (i >> 4) : (i & 63);
-      const int kb = sbk == 1 ? (i & 15) : (i >> 6), nb = sbk == 1 ? (i >> 4) : (i & 63);
-      const int gka = k0 + ka, gkb = k0 + kb;
-      As[ka][ma] = (m0 + ma < M && gka < ke) ? A[(size_t)(m0 + ma) * sam + (size_t)gka * sak] : 0.f;
-      Bs[kb][nb] = (n0 + nb < N && gkb < ke) ? Bm[(size_t)gkb * sbk + (size_t)(n0 + nb) * sbn] : 0.f;
+      const int kq = sbk == 1 ? (i & 15) : (i >> 6), nq = sbk == 1 ? (i >> 4) : (i & 63);
+      const int gka = k0 + ka, gkb = k0 + kq;
+      ra[r] = (m0 + ma < M && gka < ke) ? A[(size_t)(m0 + ma) * sam + (size_t)gka * sak] : 0.f;
+      rb[r] = (n0 + nq < N && gkb < ke) ? Bm[(size_t)gkb * sbk + (size_t)(n0 + nq) * sbn] : 0.f;
     }
-    __syncthreads();
+  };
+  auto stash = [&]() {
+#pragma unroll
+    for (int r = 0; r < 4; ++r) {
+      const int i = threadIdx.x + 256 * r;
+      const int ka = sak == 1 ? (i & 15) : (i >> 6), ma = sak == 1 ? (i >> 4) : (i & 63);
+      const int kq = sbk == 1 ? (i & 15) : (i >> 6), nq = sbk == 1 ? (i >> 4) : (i & 63);
+      As[ka][ma] = ra[r];
+      Bs[kq][nq] = rb[r];
+    }
+  };
+  if (kb < ke) {
+    fetch(kb);
+    stash();
+  }
+  __syncthreads();
+  for (int k0 = kb; k0 < ke; k0 += 16) {
+    const bool more = k0 + 16 < ke;
+    if (more) fetch(k0 + 16);
 #pragma unroll
     for (int kk = 0; kk < 16; ++kk) {
       float a[4], b[4];
@@ -551,6 +580,10 @@ __global__ void __launch_bounds__(256) gemm_kernel(int M, int N, int K, const fl
         for (int j = 0; j < 4; ++j) acc[i][j] = fmaf(a[i], b[j], acc[i][j]);
     }
     __syncthreads();
+    if (more) {
+      stash();
+      __syncthreads();
+    }
   }
 #pragma unroll
   for (int i = 0; i < 4; ++i) {

@@ -123,7 +123,7 @@ __global__ void __launch_bounds__(kDetWarps * 32) det_kernel(Src src, int B, int
   }
 }
 
-constexpr int kSlopeWarps = 4;
+constexpr int kSlopeWarps = 8;  // 8 chains share one copy of the direction table per CTA
 constexpr size_t kSlopeSmem = sizeof(uint16_t) * kLutSize + sizeof(uint32_t) * kDirWords * kSlopeWarps +
                               sizeof(int) * kMaxM * kSlopeWarps * 2 + 64;
 
@@ -258,7 +258,7 @@ static int launch_slope(const int16_t* cols, int B, int n, int32_t* scores, int3
   N3_TRY(ensure_device_tables());
   N3_TRY(allow_smem(reinterpret_cast<const void*>(n3::slope_kernel<MODE>), n3::kSlopeSmem));
   const int blocks_needed = (B + n3::kSlopeWarps - 1) / n3::kSlopeWarps;
-  const int grid = blocks_needed < sm_count() * 3 ? blocks_needed : sm_count() * 3;
+  const int grid = blocks_needed < sm_count() * 2 ? blocks_needed : sm_count() * 2;  // 2 CTAs fit per SM
   n3::slope_kernel<MODE><<<grid, n3::kSlopeWarps * 32, n3::kSlopeSmem, st>>>(n3::ColSource{cols}, B, n, scores,
                                                                              badness, mismatch, error_word);
   return check_launch("slope_kernel");
