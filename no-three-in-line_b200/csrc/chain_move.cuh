@@ -9,20 +9,21 @@
 namespace n3 {
 
 // Exact dE of the move (u, v) of the chain held by this warp (state in shared
-// memory: columns cs, badness bs, m slots), Metropolis test against the
+// memory: columns cs, badness bs, m slots; lutf the full direction table in
+// shared memory), Metropolis test against the
 // threshold row `thr` (width W) with the 32-bit uniform z, and on acceptance
 // the exact update of every slot's badness, the columns and E.  The caller
 // has checked legality.  Returns 1 if accepted; *dE_out receives dE.
 __device__ __forceinline__ int move_exact(int* __restrict__ cs, int* __restrict__ bs, int m,
-                                          const uint16_t* __restrict__ lut, uint32_t* __restrict__ hist, int lane,
+                                          const uint16_t* __restrict__ lutf, uint32_t* __restrict__ hist, int lane,
                                           int u, int v, uint32_t z, const uint32_t* __restrict__ thr, int W, int& E,
                                           uint32_t& err, int* dE_out) {
   const int ru = u >> 1, rv = v >> 1, cu = cs[u], cv = cs[v];
   int ids[kSlotsPerLane], cnt_new[kSlotsPerLane];
   // centre u' = (r_u, c_v)
-  const int part_a = hist_build(cs, m, ru, cv, u, v, lut, hist, lane, ids);
+  const int part_a = hist_build_full(cs, m, ru, cv, u, v, lutf, hist, lane, ids);
   __syncwarp();
-  const int line_new = dir_id(lut, rv - ru, cu - cv);
+  const int line_new = dir_id_full(lutf, rv - ru, cu - cv);
   const int j_new = hist_get(hist, line_new);
 #pragma unroll
   for (int t = 0; t < kSlotsPerLane; ++t)
@@ -31,7 +32,7 @@ __device__ __forceinline__ int move_exact(int* __restrict__ cs, int* __restrict_
   hist_release(hist, ids);
   __syncwarp();
   // centre v' = (r_v, c_u)
-  const int part_b = hist_build(cs, m, rv, cu, u, v, lut, hist, lane, ids);
+  const int part_b = hist_build_full(cs, m, rv, cu, u, v, lutf, hist, lane, ids);
   __syncwarp();
 #pragma unroll
   for (int t = 0; t < kSlotsPerLane; ++t) cnt_new[t] += ids[t] >= 0 ? hist_get(hist, ids[t]) - 1 : 0;
@@ -57,9 +58,9 @@ __device__ __forceinline__ int move_exact(int* __restrict__ cs, int* __restrict_
   // Old-side histograms: exact badness change of every other point.
   __syncwarp();
   int dB[kSlotsPerLane];
-  const int part_c = hist_build(cs, m, ru, cu, u, v, lut, hist, lane, ids);
+  const int part_c = hist_build_full(cs, m, ru, cu, u, v, lutf, hist, lane, ids);
   __syncwarp();
-  const int line_old = dir_id(lut, rv - ru, cv - cu);
+  const int line_old = dir_id_full(lutf, rv - ru, cv - cu);
   const int j_old = hist_get(hist, line_old);
 #pragma unroll
   for (int t = 0; t < kSlotsPerLane; ++t)
@@ -67,7 +68,7 @@ __device__ __forceinline__ int move_exact(int* __restrict__ cs, int* __restrict_
   __syncwarp();
   hist_release(hist, ids);
   __syncwarp();
-  const int part_d = hist_build(cs, m, rv, cv, u, v, lut, hist, lane, ids);
+  const int part_d = hist_build_full(cs, m, rv, cv, u, v, lutf, hist, lane, ids);
   __syncwarp();
 #pragma unroll
   for (int t = 0; t < kSlotsPerLane; ++t) dB[t] -= ids[t] >= 0 ? hist_get(hist, ids[t]) - 1 : 0;
@@ -96,13 +97,13 @@ __device__ __forceinline__ int move_exact(int* __restrict__ cs, int* __restrict_
 // One uniform proposal (tempering.py:50-58 draws u, v uniformly; here from a
 // Philox block).  Returns 1 if accepted.
 __device__ __forceinline__ int propose(int* __restrict__ cs, int* __restrict__ bs, int m,
-                                       const uint16_t* __restrict__ lut, uint32_t* __restrict__ hist, int lane,
+                                       const uint16_t* __restrict__ lutf, uint32_t* __restrict__ hist, int lane,
                                        U4 rnd, const uint32_t* __restrict__ thr, int W, int& E, uint32_t& err) {
   const int u = (int)__umulhi(rnd.x, (unsigned)m);
   const int v = (int)__umulhi(rnd.y, (unsigned)m);
   if (!legal_swap(cs, u, v)) return 0;
   int dE;
-  return move_exact(cs, bs, m, lut, hist, lane, u, v, rnd.z, thr, W, E, err, &dE);
+  return move_exact(cs, bs, m, lutf, hist, lane, u, v, rnd.z, thr, W, E, err, &dE);
 }
 
 }  // namespace n3

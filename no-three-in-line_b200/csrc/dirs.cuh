@@ -68,6 +68,46 @@ __device__ __forceinline__ int hist_build(const int* __restrict__ cs, int m, int
   return pairs;
 }
 
+// Full direction table (signed dx, no normalisation at lookup), kept in shared
+// memory by the kernels that evaluate moves: entry (dx + kMaxN - 1) * kLutW +
+// dy + kMaxN - 1 holds the id of (dx, dy); (0, 0) holds 0 and is never read.
+// With key(r, c) = r * kLutW + c the entry of the difference a - b sits at
+// key(a) - key(b) + kFullLutCentre, one add per lookup.
+constexpr int kFullLutSize = kLutW * kLutW;  // 22,201 entries
+constexpr size_t kFullLutBytes = ((sizeof(uint16_t) * kFullLutSize + 15) / 16) * 16;
+constexpr int kFullLutCentre = (kMaxN - 1) * kLutW + (kMaxN - 1);
+
+// Fills the full table from the compact (dx >= 0) one; all threads of the block call it.
+__device__ __forceinline__ void full_lut_fill(uint16_t* __restrict__ dst, const uint16_t* __restrict__ half) {
+  for (int e = threadIdx.x; e < kFullLutSize; e += blockDim.x) {
+    const int dx = e / kLutW - (kMaxN - 1), dy = e % kLutW - (kMaxN - 1);
+    dst[e] = (dx == 0 && dy == 0) ? (uint16_t)0 : (uint16_t)dir_id(half, dx, dy);
+  }
+}
+
+__device__ __forceinline__ int dir_id_full(const uint16_t* __restrict__ lutf, int dx, int dy) {
+  return lutf[dx * kLutW + dy + kFullLutCentre];
+}
+
+// hist_build over the full table: same insertions, same result.
+__device__ __forceinline__ int hist_build_full(const int* __restrict__ cs, int m, int rx, int cx, int skip0,
+                                               int skip1, const uint16_t* __restrict__ lutf,
+                                               uint32_t* __restrict__ hist, int lane, int (&ids)[kSlotsPerLane]) {
+  const uint16_t* base = lutf + kFullLutCentre - (rx * kLutW + cx);
+  int pairs = 0;
+#pragma unroll
+  for (int t = 0; t < kSlotsPerLane; ++t) {
+    const int k = lane + 32 * t;
+    ids[t] = -1;
+    if (k < m && k != skip0 && k != skip1 && (k >> 1) != rx) {
+      const int id = base[(k >> 1) * kLutW + cs[k]];
+      ids[t] = id;
+      pairs += hist_add(hist, id);
+    }
+  }
+  return pairs;
+}
+
 __device__ __forceinline__ void hist_release(uint32_t* hist, const int (&ids)[kSlotsPerLane]) {
 #pragma unroll
   for (int t = 0; t < kSlotsPerLane; ++t)

@@ -339,10 +339,10 @@ __global__ void __launch_bounds__(kStepWarps * 32, 1) learned_step_kernel(const 
   extern __shared__ __align__(16) unsigned char smem[];
   const n3_chains& ch = A.ch;
   uint16_t* lut = reinterpret_cast<uint16_t*>(smem);
-  uint32_t* hist_all = reinterpret_cast<uint32_t*>(smem + ((sizeof(uint16_t) * kLutSize + 15) / 16) * 16);
+  uint32_t* hist_all = reinterpret_cast<uint32_t*>(smem + kFullLutBytes);
   int* cs_all = reinterpret_cast<int*>(hist_all + kStepWarps * kDirWords);
   int* bs_all = cs_all + kStepWarps * kMaxM;
-  for (int i = threadIdx.x; i < kLutSize; i += blockDim.x) lut[i] = A.lut[i];
+  full_lut_fill(lut, A.lut);
   for (int i = threadIdx.x; i < kStepWarps * kDirWords; i += blockDim.x) hist_all[i] = 0u;
   __syncthreads();
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -695,7 +695,7 @@ static int launch_pack(const n3_mlp* M, cudaStream_t st) {
 }
 
 static size_t step_smem() {
-  return ((sizeof(uint16_t) * n3::kLutSize + 15) / 16) * 16 +
+  return n3::kFullLutBytes +
          kStepWarps * (sizeof(uint32_t) * n3::kDirWords + 2 * sizeof(int) * n3::kMaxM);
 }
 

@@ -124,7 +124,7 @@ __global__ void __launch_bounds__(kDetWarps * 32) det_kernel(Src src, int B, int
 }
 
 constexpr int kSlopeWarps = 8;  // 8 chains share one copy of the direction table per CTA
-constexpr size_t kSlopeSmem = sizeof(uint16_t) * kLutSize + sizeof(uint32_t) * kDirWords * kSlopeWarps +
+constexpr size_t kSlopeSmem = kFullLutBytes + sizeof(uint32_t) * kDirWords * kSlopeWarps +
                               sizeof(int) * kMaxM * kSlopeWarps * 2 + 64;
 
 // Loads one state, validating columns (range, row duplicates).  Returns the
@@ -156,10 +156,10 @@ __global__ void __launch_bounds__(kSlopeWarps * 32) slope_kernel(ColSource src, 
                                                                    uint32_t* __restrict__ error_word) {
   extern __shared__ __align__(16) unsigned char smem[];
   uint16_t* lut = reinterpret_cast<uint16_t*>(smem);
-  uint32_t* hist_all = reinterpret_cast<uint32_t*>(smem + ((sizeof(uint16_t) * kLutSize + 15) & ~size_t(15)));
+  uint32_t* hist_all = reinterpret_cast<uint32_t*>(smem + kFullLutBytes);
   int* cs_all = reinterpret_cast<int*>(hist_all + kDirWords * kSlopeWarps);
   int* bad_all = cs_all + kMaxM * kSlopeWarps;
-  for (int i = threadIdx.x; i < kLutSize; i += blockDim.x) lut[i] = g_dir_lut[i];
+  full_lut_fill(lut, g_dir_lut);
   for (int i = threadIdx.x; i < kDirWords * kSlopeWarps; i += blockDim.x) hist_all[i] = 0u;
   __syncthreads();
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;

@@ -91,29 +91,39 @@ __device__ __forceinline__ int det_state(const int* __restrict__ cs, int n, int 
 }
 
 // Slope line count of one state.  Returns sum over anchors of badness (3E).
-// hist: this warp's zeroed direction histogram (kDirWords words); it is left
-// zeroed on return.  bad_out (per slot) may be null.
-__device__ __forceinline__ int slope_state(const int* __restrict__ cs, int n, const uint16_t* __restrict__ lut,
-                           uint32_t* __restrict__ hist, int lane, int* __restrict__ bad_out) {
+// lutf: the full direction table in shared memory (dirs.cuh).  hist: this
+// warp's zeroed direction histogram (kDirWords words); it is left zeroed on
+// return.  bad_out (per slot) may be null.
+__device__ __forceinline__ int slope_state(const int* __restrict__ cs, int n, const uint16_t* __restrict__ lutf,
+                                           uint32_t* __restrict__ hist, int lane, int* __restrict__ bad_out) {
+  constexpr int kT = (kMaxM + 31) / 32;
   const int m = 2 * n;
+  // this lane's slots b = lane + 32 t: their keys (row * kLutW + column) and rows
+  int key[kT], row[kT];
+#pragma unroll
+  for (int t = 0; t < kT; ++t) {
+    const int b = lane + 32 * t;
+    row[t] = b < m ? b >> 1 : -1;
+    key[t] = b < m ? (b >> 1) * kLutW + cs[b] : 0;
+  }
   int total = 0;
   for (int a = 0; a < m; ++a) {
-    const int ra = a >> 1, ca = cs[a];
+    const int ra = a >> 1;
+    const uint16_t* base = lutf + kFullLutCentre - (ra * kLutW + cs[a]);
     int pairs = 0;
-    int ids[(kMaxM + 31) / 32];
+    int ids[kT];
 #pragma unroll
-    for (int t = 0; t < (kMaxM + 31) / 32; ++t) {
-      const int b = lane + 32 * t;
+    for (int t = 0; t < kT; ++t) {
       ids[t] = -1;
-      if (b < m && (b >> 1) != ra) {  // the row partner has the lone direction (0,1)
-        const int id = dir_id(lut, (b >> 1) - ra, cs[b] - ca);
+      if (row[t] >= 0 && row[t] != ra) {  // the row partner has the lone direction (0,1)
+        const int id = base[key[t]];
         ids[t] = id;
         pairs += hist_add(hist, id);  // earlier points on this direction
       }
     }
     __syncwarp();
 #pragma unroll
-    for (int t = 0; t < (kMaxM + 31) / 32; ++t)
+    for (int t = 0; t < kT; ++t)
       if (ids[t] >= 0) hist_clear(hist, ids[t]);
     __syncwarp();
     pairs = warp_sum(pairs);

@@ -48,9 +48,10 @@ __device__ __forceinline__ uint64_t global_ns() {
   return t;
 }
 
-// Shared-memory layout of the tempering kernel (dynamic).
+// Shared-memory layout of the tempering kernel (dynamic): the full direction
+// table, then per chain a histogram, columns and badness, then the leader arrays.
 struct TemperSmem {
-  static constexpr size_t lut_bytes = ((sizeof(uint16_t) * kLutSize + 15) / 16) * 16;
+  static constexpr size_t lut_bytes = kFullLutBytes;
   static __host__ __device__ size_t bytes(int cpb) {
     return lut_bytes + (size_t)cpb * (sizeof(uint32_t) * kDirWords + 2 * sizeof(int) * kMaxM) +
            3 * sizeof(int) * 64 + 16;
@@ -120,7 +121,7 @@ __global__ void __launch_bounds__(512, 1) temper_kernel(const TemperArgs A) {
   int* bs = bs_all + warp * kMaxM;
   uint32_t* hist = hist_all + (size_t)warp * kDirWords;
 
-  for (int i = threadIdx.x; i < kLutSize; i += blockDim.x) lut[i] = A.lut[i];
+  full_lut_fill(lut, A.lut);
   for (int i = threadIdx.x; i < cpb * kDirWords; i += blockDim.x) hist_all[i] = 0u;
   for (int s = lane; s < m; s += 32) {
     cs[s] = ch.cols[(size_t)c * kMaxM + s];
@@ -225,15 +226,16 @@ __global__ void __launch_bounds__(512, 1) temper_kernel(const TemperArgs A) {
 // Full recompute of every chain's energy (determinant count) and badness
 // (slope count) compared with the maintained values.  One warp per chain.
 constexpr int kAuditWarps = 4;
+constexpr size_t kAuditSmem = kFullLutBytes + kAuditWarps * (sizeof(uint32_t) * kDirWords + 2 * sizeof(int) * kMaxM);
 
 __global__ void __launch_bounds__(kAuditWarps * 32) audit_kernel(const n3_chains ch, const uint16_t* __restrict__ g_lut,
                                                                    int32_t* mismatch) {
   extern __shared__ __align__(16) unsigned char smem[];
   uint16_t* lut = reinterpret_cast<uint16_t*>(smem);
-  uint32_t* hist_all = reinterpret_cast<uint32_t*>(smem + TemperSmem::lut_bytes);
+  uint32_t* hist_all = reinterpret_cast<uint32_t*>(smem + kFullLutBytes);
   int* cs_all = reinterpret_cast<int*>(hist_all + kAuditWarps * kDirWords);
   int* bs_all = cs_all + kAuditWarps * kMaxM;
-  for (int i = threadIdx.x; i < kLutSize; i += blockDim.x) lut[i] = g_lut[i];
+  full_lut_fill(lut, g_lut);
   for (int i = threadIdx.x; i < kAuditWarps * kDirWords; i += blockDim.x) hist_all[i] = 0u;
   __syncthreads();
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -324,9 +326,7 @@ int temper_launch(const n3_chains* ch, const n3_temper_config* cfg, cudaStream_t
 namespace n3host {
 int prepare_tempering() {
   N3_TRY(allow_smem(reinterpret_cast<const void*>(n3::temper_kernel), n3::TemperSmem::bytes(16)));
-  const size_t audit = n3::TemperSmem::lut_bytes +
-                       n3::kAuditWarps * (sizeof(uint32_t) * n3::kDirWords + 2 * sizeof(int) * n3::kMaxM);
-  return allow_smem(reinterpret_cast<const void*>(n3::audit_kernel), audit);
+  return allow_smem(reinterpret_cast<const void*>(n3::audit_kernel), n3::kAuditSmem);
 }
 }  // namespace n3host
 
@@ -341,8 +341,7 @@ int n3_temper_audit(const n3_chains* chains, int32_t* mismatch, void* stream) {
   if (mismatch == nullptr) return n3host::set_error(N3_ERR_ARG, "null mismatch counter");
   N3_TRY(n3host::ensure_device_tables());
   const n3_chains ch = *chains;
-  const size_t smem = n3::TemperSmem::lut_bytes +
-                      n3::kAuditWarps * (sizeof(uint32_t) * n3::kDirWords + 2 * sizeof(int) * n3::kMaxM);
+  const size_t smem = n3::kAuditSmem;
   N3_TRY(n3host::allow_smem(reinterpret_cast<const void*>(n3::audit_kernel), smem));
   const int want = (ch.n_chains + n3::kAuditWarps - 1) / n3::kAuditWarps;
   const int grid = want < n3host::sm_count() * 4 ? want : n3host::sm_count() * 4;
