@@ -10,11 +10,14 @@
 //   [12..161] the chain's per-slot badness (150 slots, zero beyond 2n), / 16
 //   [162..191] zero
 // Layer 1 is split accordingly: W1 = [W1a | W1b].  The 150 chain features are
-// shared by all 128 candidates of a chain, so W1b x + b1 is computed once per
-// chain (candidates_kernel) and added in the epilogue of the per-candidate
-// K = 16 tensor-core product.  Inference per chain is one M = 128 tile:
-//   D1 = A1 (128 x 16) W1a^T  -> + chain part, ReLU, bf16 -> A2 (shared memory)
-//   D2 = A2 (128 x 256) W2^T  -> + b2, ReLU, . w3 + b3 -> predicted dE
+// shared by all 128 candidates of a chain, so the chain part c1 = W1b x + b1 is
+// computed once per chain (a GEMM after candidates_kernel) and enters the
+// per-candidate K = 16 tensor-core product through two constant-1 columns of
+// A1 (k = 12, 13) against c1 split into bf16 high and low parts (B columns
+// 12, 13; c1 = hi + lo to about 2^-17 relative).  Inference per chain is one
+// M = 128 tile:
+//   D1 = A1 (128 x 16) [W1a | hi | lo]^T  -> ReLU, bf16 -> A2 (shared memory)
+//   D2 = A2 (128 x 256) W2^T              -> + b2, ReLU, . w3 + b3 -> predicted dE
 // both on tcgen05 with fp32 accumulators in tensor memory.
 // Training (SIMT fp32, hand-written GEMMs) uses MSE on dE / kTargetScale with
 // Adam; the packed bf16 images are rebuilt after each update.
@@ -33,7 +36,7 @@ namespace mlp {
 
 constexpr int kCand = 128;    // candidates per chain per step (one M tile)
 constexpr int kIn = 192;      // input width
-constexpr int kCandFeat = 12; // per-candidate features
+constexpr int kCandFeat = 12; // per-candidate features (A1 columns 12 and 13 hold 1.0)
 constexpr int kChainFeat = 150;
 constexpr int kH = 256;
 constexpr float kTargetScale = 16.0f;
@@ -47,23 +50,39 @@ constexpr int oB3 = oW3 + kH;
 constexpr int kParams = oB3 + 4;  // padded to a multiple of 4
 
 // Inference shared-memory map (offsets from a 1024-aligned base).  A1 and the
-// chain part are double-buffered so the next tile loads during this one.
+// chain part have three buffers: tile i + 2 loads while tile i is processed.
 constexpr uint32_t sW2 = 0;                        // SW128 image, 4 x [256 x 128 B]
 constexpr uint32_t sA2 = sW2 + 4 * kH * 128;       // SW128, 4 x [128 x 128 B]
-constexpr uint32_t sW1a = sA2 + 4 * kCand * 128;   // INTERLEAVE K=16, 256 rows
-constexpr uint32_t sA1 = sW1a + kH * 32;           // 2 x INTERLEAVE K=16, 128 rows
-constexpr uint32_t sC1 = sA1 + 2 * kCand * 32;     // 2 x fp32[256] chain part of layer 1
-constexpr uint32_t sB2 = sC1 + 2 * kH * 4;
+constexpr uint32_t sW1a = sA2 + 4 * kCand * 128;   // INTERLEAVE K=16, 256 rows: W1a | c1 hi | c1 lo | 0
+constexpr int kStages = 3;
+constexpr uint32_t sA1 = sW1a + kH * 32;           // 3 x INTERLEAVE K=16, 128 rows
+constexpr uint32_t sC1 = sA1 + kStages * kCand * 32;  // 3 x fp32[256] chain part of layer 1
+constexpr uint32_t sB2 = sC1 + kStages * kH * 4;
 constexpr uint32_t sW3 = sB2 + kH * 4;
-constexpr uint32_t sPart = sW3 + kH * 4;           // fp32[2][128] half dot products
-constexpr uint32_t sBar = sPart + 2 * kCand * 4;   // 2 mbarriers, TMEM address, abort flag
-constexpr uint32_t kInferSmem = sBar + 64 + 1024;  // + alignment slack
-constexpr int kInferThreads = 256;                 // 8 warps: two per tensor-memory lane quarter
+constexpr uint32_t sPart = sW3 + kH * 4;           // fp32[2][2][128] half dot products
+constexpr uint32_t sBar = sPart + 4 * kCand * 4;   // 9 mbarriers, TMEM address, abort flag
+constexpr uint32_t kInferSmem = sBar + 128 + 1024; // + alignment slack
+constexpr int kGroupThreads = 256;                 // a warp group: 2 warps per tensor-memory lane quarter
+constexpr int kInferThreads = 2 * kGroupThreads;
 constexpr uint32_t kWaitTries = 1u << 24;
 
 __device__ __forceinline__ uint16_t bf16_bits(float x) {
   const __nv_bfloat16 h = __float2bfloat16_rn(x);
   return *reinterpret_cast<const uint16_t*>(&h);
+}
+
+// ReLU of two floats rounded to bf16 (round-to-nearest-even) and packed, a in
+// bits 0-15, b in 16-31: one paired conversion, then a paired bf16 max with 0
+// (rounding keeps the sign, so ReLU after rounding equals rounding after ReLU).
+__device__ __forceinline__ uint32_t relu_bf16x2_bits(float a, float b) {
+  const __nv_bfloat162 h = __hmax2(__floats2bfloat162_rn(a, b), __float2bfloat162_rn(0.f));
+  return *reinterpret_cast<const uint32_t*>(&h);
+}
+
+// Two floats rounded to bf16 in one conversion: lo in bits 0-15, hi in 16-31.
+__device__ __forceinline__ uint32_t bf16x2_bits(float lo, float hi) {
+  const __nv_bfloat162 h = __floats2bfloat162_rn(lo, hi);
+  return *reinterpret_cast<const uint32_t*>(&h);
 }
 
 // ---------------------------------------------------------------------------
@@ -100,7 +119,8 @@ struct CandArgs {
   uint32_t k0, k1;
 };
 
-__device__ __forceinline__ void candidate_features(const int16_t* cols, const int32_t* bad, int n, int u, int v,
+template <class ColT, class BadT>
+__device__ __forceinline__ void candidate_features(const ColT* cols, const BadT* bad, int n, int u, int v,
                                                    float (&f)[kCandFeat]) {
   const float inv_n = 1.0f / (float)n;
   const int s[4] = {u, v, u ^ 1, v ^ 1};
@@ -113,28 +133,99 @@ __device__ __forceinline__ void candidate_features(const int16_t* cols, const in
 }
 
 __global__ void __launch_bounds__(kCand) candidates_kernel(const CandArgs A) {
+  __shared__ int s_cols[kChainFeat], s_bad[kChainFeat];
   const int c = blockIdx.x;
   const int n = A.ladder_n[c / A.ladder_size], m = 2 * n;
-  const int16_t* cols = A.cols + (size_t)c * kChainFeat;
-  const int32_t* bad = A.badness + (size_t)c * kChainFeat;
-  for (int s = threadIdx.x; s < kChainFeat; s += blockDim.x)
-    A.badn[(size_t)c * kChainFeat + s] = s < m ? (float)bad[s] * (1.0f / 16.0f) : 0.f;
-  {
-    const int j = threadIdx.x;
-    const uint64_t step = *A.step;
-    const U4 r = philox4x32_10(U4{(uint32_t)step, (uint32_t)(step >> 32), (uint32_t)c, kTagCandidate | (uint32_t)j},
-                               A.k0, A.k1);
-    const int u = (int)__umulhi(r.x, (unsigned)m), v = (int)__umulhi(r.y, (unsigned)m);
-    const int cu = cols[u], cv = cols[v];
-    const bool legal = (u >> 1) != (v >> 1) && cu != cv && cols[u ^ 1] != cv && cols[v ^ 1] != cu;
-    float f[kCandFeat];
-    candidate_features(cols, bad, n, u, v, f);
-    uint8_t* img = A.a1_img + (size_t)c * (kCand * 32);
-#pragma unroll
-    for (int k = 0; k < 16; ++k)
-      *reinterpret_cast<uint16_t*>(img + umma::inter16_offset(j, k)) = bf16_bits(k < kCandFeat ? f[k] : 0.0f);
-    A.cand[(size_t)c * kCand + j] = u | (v << 8) | (legal ? (1 << 31) : 0);
+  for (int s = threadIdx.x; s < kChainFeat; s += blockDim.x) {
+    const int b = A.badness[(size_t)c * kChainFeat + s];
+    s_cols[s] = A.cols[(size_t)c * kChainFeat + s];
+    s_bad[s] = b;
+    A.badn[(size_t)c * kChainFeat + s] = s < m ? (float)b * (1.0f / 16.0f) : 0.f;
   }
+  __syncthreads();
+  const int j = threadIdx.x;
+  const uint64_t step = *A.step;
+  const U4 r = philox4x32_10(U4{(uint32_t)step, (uint32_t)(step >> 32), (uint32_t)c, kTagCandidate | (uint32_t)j},
+                             A.k0, A.k1);
+  const int u = (int)__umulhi(r.x, (unsigned)m), v = (int)__umulhi(r.y, (unsigned)m);
+  const int cu = s_cols[u], cv = s_cols[v];
+  const bool legal = (u >> 1) != (v >> 1) && cu != cv && s_cols[u ^ 1] != cv && s_cols[v ^ 1] != cu;
+  float f[kCandFeat];
+  candidate_features(s_cols, s_bad, n, u, v, f);
+  // row j of the INTERLEAVE image: K 0-7 and K 8-15 are two 16-byte core-matrix rows
+  uint8_t* img = A.a1_img + (size_t)c * (kCand * 32);
+  const uint4 lo = make_uint4(bf16x2_bits(f[0], f[1]), bf16x2_bits(f[2], f[3]), bf16x2_bits(f[4], f[5]),
+                              bf16x2_bits(f[6], f[7]));
+  const uint4 hi = make_uint4(bf16x2_bits(f[8], f[9]), bf16x2_bits(f[10], f[11]), bf16x2_bits(1.0f, 1.0f), 0u);
+  *reinterpret_cast<uint4*>(img + umma::inter16_offset(j, 0)) = lo;
+  *reinterpret_cast<uint4*>(img + umma::inter16_offset(j, 8)) = hi;
+  A.cand[(size_t)c * kCand + j] = u | (v << 8) | (legal ? (1 << 31) : 0);
+}
+
+// Chain part of layer 1 for every chain: c1[c][n] = b1[n] + sum_k W1[n][12 + k] badn[c][k]
+// (k < 150).  One thread per output column n, kChainTile chains per CTA (their
+// badness rows staged in shared memory, zero-padded to 160; 2048 chains make 293
+// CTAs, two per SM).  W1's chain columns pass through shared memory in chunks of
+// 32, read row-contiguously (coalesced, the next chunk in flight while this one
+// is used) and stored transposed with a 257-float stride (no bank conflicts
+// either way).  Columns up to 171 stay inside the 192-wide rows.  Deterministic:
+// one thread sums each output in a fixed order.
+constexpr int kChainTile = 7;
+constexpr int kChainPad = 160;
+constexpr int kWStride = kH + 1;
+__global__ void __launch_bounds__(kH) chain_part_kernel(int C, const float* __restrict__ badn,
+                                                        const float* __restrict__ P, float* __restrict__ c1) {
+  __shared__ __align__(16) float xs[kChainTile][kChainPad];
+  __shared__ float ws[32][kWStride];
+  const int c0 = blockIdx.x * kChainTile;
+  for (int i = threadIdx.x; i < kChainTile * kChainPad; i += blockDim.x) {
+    const int cc = i / kChainPad, k = i % kChainPad;
+    xs[cc][k] = (c0 + cc < C && k < kChainFeat) ? badn[(size_t)(c0 + cc) * kChainFeat + k] : 0.f;
+  }
+  const int nn = threadIdx.x;
+  float acc[kChainTile];
+#pragma unroll
+  for (int cc = 0; cc < kChainTile; ++cc) acc[cc] = 0.f;
+  // element i = thread + 256 r of a chunk: row i / 8, columns k0 + 4 (i % 8) ..
+  auto fetch = [&](int k0, float4 (&v)[8]) {
+#pragma unroll
+    for (int r = 0; r < 8; ++r) {
+      const int i = threadIdx.x + kH * r;
+      v[r] = *reinterpret_cast<const float4*>(P + oW1 + (size_t)(i >> 3) * kIn + kCandFeat + k0 + 4 * (i & 7));
+    }
+  };
+  float4 v[8];
+  fetch(0, v);
+#pragma unroll 1
+  for (int k0 = 0; k0 < kChainPad; k0 += 32) {
+    __syncthreads();  // the previous chunk has been consumed (and, first time, xs is in place)
+#pragma unroll
+    for (int r = 0; r < 8; ++r) {
+      const int i = threadIdx.x + kH * r, row = i >> 3, kq = 4 * (i & 7);
+      ws[kq][row] = v[r].x;
+      ws[kq + 1][row] = v[r].y;
+      ws[kq + 2][row] = v[r].z;
+      ws[kq + 3][row] = v[r].w;
+    }
+    __syncthreads();
+    if (k0 + 32 < kChainPad) fetch(k0 + 32, v);
+#pragma unroll
+    for (int k = 0; k < 32; k += 4) {
+      const float w0 = ws[k][nn], w1 = ws[k + 1][nn], w2 = ws[k + 2][nn], w3 = ws[k + 3][nn];
+#pragma unroll
+      for (int cc = 0; cc < kChainTile; ++cc) {
+        const float4 x = *reinterpret_cast<const float4*>(&xs[cc][k0 + k]);
+        acc[cc] = fmaf(w0, x.x, acc[cc]);
+        acc[cc] = fmaf(w1, x.y, acc[cc]);
+        acc[cc] = fmaf(w2, x.z, acc[cc]);
+        acc[cc] = fmaf(w3, x.w, acc[cc]);
+      }
+    }
+  }
+  const float bias = P[oB1 + nn];
+#pragma unroll
+  for (int cc = 0; cc < kChainTile; ++cc)
+    if (c0 + cc < C) c1[(size_t)(c0 + cc) * kH + nn] = acc[cc] + bias;
 }
 
 // ---------------------------------------------------------------------------
@@ -161,41 +252,108 @@ __device__ __forceinline__ void copy16(uint8_t* dst, const uint8_t* src, int byt
 __device__ __forceinline__ void cp_async16(uint32_t saddr, const void* g) {
   asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(saddr), "l"(g) : "memory");
 }
+__device__ __forceinline__ void cp_async4(uint32_t saddr, const void* g) {
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 4;" ::"r"(saddr), "l"(g) : "memory");
+}
 __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
 __device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_group 0;" ::: "memory"); }
+// All but the most recent group have landed.
+__device__ __forceinline__ void cp_async_wait_prev() { asm volatile("cp.async.wait_group 1;" ::: "memory"); }
 
-// Prefetch of tile t's candidate features (4 KB) and chain part (1 KB).
-__device__ __forceinline__ void load_tile_async(uint32_t base, int buf, const InferArgs& A, int t, int tid) {
-  const uint8_t* a1 = A.a1_img + (size_t)t * (kCand * 32);
-  const float* c1 = A.c1 + (size_t)t * kH;
-  const uint32_t sa = base + sA1 + (uint32_t)buf * (kCand * 32);
-  const uint32_t sc = base + sC1 + (uint32_t)buf * (kH * 4);
-  for (int i = tid; i < kCand * 32 / 16; i += kInferThreads) cp_async16(sa + 16 * i, a1 + 16 * i);
-  for (int i = tid; i < kH * 4 / 16; i += kInferThreads) cp_async16(sc + 16 * i, c1 + 4 * i);
+// Prefetch of tile t's candidate features (4 KB) and chain part (1 KB) by
+// `nthreads` >= 256 threads, as one cp.async group (committed, empty when t is
+// past the last tile, so that every thread's group count stays in step).
+// Thread j < 256 copies chain-part float j itself.
+__device__ __forceinline__ void load_tile_async(uint32_t base, int buf, const InferArgs& A, int t, int tid,
+                                                int nthreads) {
+  if (t < A.tiles) {
+    const uint8_t* a1 = A.a1_img + (size_t)t * (kCand * 32);
+    const uint32_t sa = base + sA1 + (uint32_t)buf * (kCand * 32);
+    for (int i = tid; i < kCand * 32 / 16; i += nthreads) cp_async16(sa + 16 * i, a1 + 16 * i);
+    if (tid < kH) cp_async4(base + sC1 + (uint32_t)buf * (kH * 4) + 4 * tid, A.c1 + (size_t)t * kH + tid);
+  }
   cp_async_commit();
 }
 
-// Per CTA: tiles t0, t0 + G, ...  Pipeline per tile i (D1 = TMEM columns
-// 0..255, D2 = 256..511):
-//   wait MMA1(i) -> epilogue 1 (D1 + chain part -> A2) -> issue MMA2(i) ->
-//   issue MMA1(i+1) from the prefetched A1 -> wait MMA2(i) -> epilogue 2.
-// Eight warps: warp w reads TMEM lanes 32*(w%4).., columns 128*(w/4)...
+// Writes chain part value c of B row n into columns 12 (bf16 high part) and 13
+// (bf16 low part) of the layer-1 B operand.
+__device__ __forceinline__ void put_chain_part(uint8_t* sm, int n, float c) {
+  const float hi = __bfloat162float(__float2bfloat16_rn(c));
+  *reinterpret_cast<uint32_t*>(sm + sW1a + umma::inter16_offset(n, kCandFeat)) = bf16x2_bits(hi, c - hi);
+}
+
+// Barrier of one warp group (named barrier ID, kGroupThreads threads) that
+// also ORs a flag over the group, so that the group leaves its loop together.
+template <int ID>
+__device__ __forceinline__ bool group_sync_or(bool v) {
+  uint32_t out;
+  asm volatile(
+      "{\n\t.reg .pred p, q;\n\t"
+      "setp.ne.u32 q, %1, 0;\n\t"
+      "barrier.cta.red.or.pred p, %2, %3, q;\n\t"
+      "selp.u32 %0, 1, 0, p;\n\t}\n"
+      : "=r"(out)
+      : "r"((uint32_t)v), "n"(ID), "n"(kGroupThreads)
+      : "memory");
+  return out != 0;
+}
+
+__device__ __forceinline__ void mbar_arrive(uint32_t saddr) {
+  asm volatile("{\n\t.reg .b64 st;\n\tmbarrier.arrive.shared::cta.b64 st, [%0];\n\t}\n" ::"r"(saddr) : "memory");
+}
+
+// Layer-2 product of one tile: D (+)= A2 (128 x 256) W2^T, sixteen K = 16 steps.
+__device__ __forceinline__ void issue_layer2(uint32_t base, uint32_t d, uint32_t idesc) {
+#pragma unroll
+  for (int s = 0; s < kH / 16; ++s) {
+    const uint32_t koff = (uint32_t)(s & 3) * 32u;  // K = 16 step inside a 64-wide slice
+    const uint64_t ad = umma::desc_sw128(base + sA2 + (uint32_t)(s >> 2) * (kCand * 128) + koff);
+    const uint64_t bd = umma::desc_sw128(base + sW2 + (uint32_t)(s >> 2) * (kH * 128) + koff);
+    umma::mma_bf16(d, ad, bd, idesc, s > 0 ? 1u : 0u);
+  }
+}
+
+__device__ __forceinline__ void issue_layer1(uint32_t base, int a1buf, uint32_t d, uint32_t idesc) {
+  const uint32_t a1 = base + sA1 + (uint32_t)a1buf * (kCand * 32);
+  umma::mma_bf16(d, umma::desc_interleave(a1, 128, 256), umma::desc_interleave(base + sW1a, 128, 256), idesc, 0u);
+}
+
+// Per CTA: tiles t_i = blockIdx.x + i * gridDim.x.  Tensor memory holds two
+// 256-column accumulators; tile i uses buffer i & 1 first for its layer-1
+// product D1 and then, once D1 has been read, for its layer-2 product D2.
+// Warp group 1 (warps 0-7) runs epilogue 1 (D1 + chain part, ReLU, bf16 into
+// the A2 operand); its thread 0 issues the layer-2 MMAs and thread 32 the
+// layer-1 MMAs (each tracks its own MMAs with tcgen05.commit).  Warp group 2
+// (warps 8-15) runs epilogue 2 (ReLU(D2 + b2) . w3).  Per tile:
+//   MMA1(i) done, MMA2(i-1) done (A2 free)  -> group 1: epilogue 1(i) -> MMA2(i)
+//   MMA2(i) done                            -> group 2: epilogue 2(i) -> frees buffer i & 1
+//   epilogue 2(i-1) done                    -> MMA1(i+1) into buffer (i+1) & 1
+//   epilogue 1(i+1) done                    -> group 2 starts epilogue 2(i)
+// so epilogue 2 of tile i runs beside the layer-2 MMAs of tile i+1, and
+// epilogue 1, which the tensor core waits for, has the SM's issue slots alone.
+// In each group, warp w reads tensor-memory lanes 32 (w % 4) .. (its quarter of
+// the 128 rows), columns 128 ((w / 4) % 2) ..: each thread owns one row and
+// half of the 256 columns.
 __global__ void __launch_bounds__(kInferThreads, 1) infer_kernel(const InferArgs A) {
   extern __shared__ uint8_t smem_raw[];
   const uint32_t raw = umma::smem_addr(smem_raw);
   uint8_t* sm = smem_raw + ((1024u - (raw & 1023u)) & 1023u);  // 1024-aligned base
   const uint32_t base = umma::smem_addr(sm);
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-  const int quarter = warp & 3, half = warp >> 2;
+  const int group = warp >> 3, quarter = warp & 3, colhalf = (warp >> 2) & 1;
+  const int gtid = tid & (kGroupThreads - 1);
   float* b2s = reinterpret_cast<float*>(sm + sB2);
   float* w3s = reinterpret_cast<float*>(sm + sW3);
   float* part = reinterpret_cast<float*>(sm + sPart);
-  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(sm + sBar + 16);
-  int* abort_flag = reinterpret_cast<int*>(sm + sBar + 24);
-  const uint32_t bar1 = base + sBar, bar2 = base + sBar + 8;
-  const int stride = gridDim.x;
+  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(sm + sBar + 80);
+  volatile int* abort_flag = reinterpret_cast<volatile int*>(sm + sBar + 88);
+  // mbarriers: MMA1 done [2], MMA2 done [2], epilogue 2 done [2], final drain, epilogue 1 done [2]
+  const uint32_t barM1 = base + sBar, barM2 = base + sBar + 16, barE2 = base + sBar + 32, barFin = base + sBar + 48;
+  const uint32_t barE1 = base + sBar + 56;
+  const int G = gridDim.x;
 
-  if (blockIdx.x < A.tiles) load_tile_async(base, 0, A, blockIdx.x, tid);
+  load_tile_async(base, 0, A, blockIdx.x, tid, kInferThreads);
+  load_tile_async(base, 1, A, blockIdx.x + gridDim.x, tid, kInferThreads);
   copy16(sm + sW2, A.w2_img, 4 * kH * 128, tid, kInferThreads);
   copy16(sm + sW1a, A.w1a_img, kH * 32, tid, kInferThreads);
   for (int i = tid; i < kH; i += kInferThreads) {
@@ -203,13 +361,22 @@ __global__ void __launch_bounds__(kInferThreads, 1) infer_kernel(const InferArgs
     w3s[i] = A.P[oW3 + i];
   }
   const float b3 = A.P[oB3];
+  cp_async_wait_all();
+  __syncthreads();  // the W1a image is in place before its chain-part columns are written
+  if (tid < kH && blockIdx.x < A.tiles)  // this thread's own copy of tile 0's chain part
+    put_chain_part(sm, tid, reinterpret_cast<const float*>(sm + sC1)[tid]);
   if (warp == 0) {
-    umma::tmem_alloc(base + sBar + 16, 512);
+    umma::tmem_alloc(base + sBar + 80, 512);
     umma::tmem_relinquish();
   }
   if (tid == 0) {
-    umma::mbar_init(bar1, 1);
-    umma::mbar_init(bar2, 1);
+    for (int k = 0; k < 2; ++k) {
+      umma::mbar_init(barM1 + 8 * k, 1);
+      umma::mbar_init(barM2 + 8 * k, 1);
+      umma::mbar_init(barE2 + 8 * k, kGroupThreads);
+      umma::mbar_init(barE1 + 8 * k, 1);
+    }
+    umma::mbar_init(barFin, 2);  // threads 0 and 32 each commit their MMAs
     umma::mbar_fence_init();
     *abort_flag = 0;
   }
@@ -219,91 +386,117 @@ __global__ void __launch_bounds__(kInferThreads, 1) infer_kernel(const InferArgs
   __syncthreads();
   umma::fence_after_sync();
   const uint32_t tmem = *tmem_slot;
-  const uint32_t d1 = tmem, d2 = tmem + 256u;
   const uint32_t lane_off = (uint32_t)(32 * quarter) << 16;
   const uint32_t idesc = umma::idesc_bf16_f32(128, 256);
   const int row = 32 * quarter + lane;
-  uint32_t ph1 = 0, ph2 = 0;
+  const int sl0 = 2 * colhalf;  // this thread's two K = 64 slices / column blocks
   if (tid == 0 && blockIdx.x < A.tiles) {
-    umma::mma_bf16(d1, umma::desc_interleave(base + sA1, 128, 256), umma::desc_interleave(base + sW1a, 128, 256),
-                   idesc, 0u);
-    umma::commit(bar1);
+    issue_layer1(base, 0, tmem, idesc);
+    umma::commit(barM1);
   }
-  int buf = 0;
-  for (int t = blockIdx.x; t < A.tiles; t += stride, buf ^= 1) {
-    const bool has_next = t + stride < A.tiles;
-    if (has_next) load_tile_async(base, buf ^ 1, A, t + stride, tid);
-    if (!umma::mbar_wait(bar1, ph1, kWaitTries)) atomicExch(abort_flag, 1);
-    ph1 ^= 1u;
-    umma::fence_after_sync();
-    // epilogue 1: h1 = relu(D1 + chain part) -> bf16 -> A2 (SW128), this warp's 128 columns
-    const float* c1s = reinterpret_cast<const float*>(sm + sC1 + (uint32_t)buf * (kH * 4));
+
+  if (group == 0) {
+    // ---- warp group 1: epilogue 1 and the MMA issue ----
+    for (int i = 0, t = blockIdx.x; t < A.tiles; ++i, t += G) {
+      const int b = i & 1;
+      const uint32_t d = tmem + 256u * (uint32_t)b;
+      const bool has_next = t + G < A.tiles;
+      const int next_stage = (i + 1) % kStages;
+      // tile i + 2 into the stage that tile i - 1 used (its MMA1 is done)
+      load_tile_async(base, (i + 2) % kStages, A, t + 2 * G, gtid, kGroupThreads);
+      bool ok = umma::mbar_wait(barM1 + 8 * b, (uint32_t)(i >> 1) & 1u, kWaitTries);
+      if (i > 0) ok = ok && umma::mbar_wait(barM2 + 8 * (b ^ 1), (uint32_t)((i - 1) >> 1) & 1u, kWaitTries);
+      ok = __all_sync(0xffffffffu, ok && !*abort_flag);  // warp-uniform: tcgen05.ld is .sync.aligned
+      umma::fence_after_sync();
+      if (ok) {
 #pragma unroll 1
-    for (int j = 4 * half; j < 4 * half + 4; ++j) {
-      float v[32];
-      umma::tmem_ld32(d1 + lane_off + 32 * j, v);
+        for (int h = 2 * sl0; h < 2 * sl0 + 4; ++h) {  // columns 32 h .. 32 h + 31 (K slice h / 2 of A2)
+          float r[32];
+          umma::tmem_ld32(d + lane_off + 32u * (uint32_t)h, r);
 #pragma unroll
-      for (int q = 0; q < 4; ++q) {
-        uint32_t w[4];
+          for (int q = 0; q < 4; ++q) {
+            uint32_t w[4];
 #pragma unroll
-        for (int e = 0; e < 4; ++e) {
-          const int k0 = 32 * j + 8 * q + 2 * e;
-          const float h0 = fmaxf(v[8 * q + 2 * e] + c1s[k0], 0.f);
-          const float h1 = fmaxf(v[8 * q + 2 * e + 1] + c1s[k0 + 1], 0.f);
-          w[e] = (uint32_t)bf16_bits(h0) | ((uint32_t)bf16_bits(h1) << 16);
+            for (int e = 0; e < 4; ++e)
+              w[e] = relu_bf16x2_bits(r[8 * q + 2 * e], r[8 * q + 2 * e + 1]);
+            *reinterpret_cast<uint4*>(sm + sA2 + umma::sw128_offset(row, 32 * h + 8 * q, kCand)) =
+                make_uint4(w[0], w[1], w[2], w[3]);
+          }
         }
-        *reinterpret_cast<uint4*>(sm + sA2 + umma::sw128_offset(row, 32 * j + 8 * q, kCand)) =
-            make_uint4(w[0], w[1], w[2], w[3]);
+      }
+      cp_async_wait_prev();  // tile i + 1's A1 / chain part have landed (this thread's copies)
+      if (ok && has_next)  // MMA1(i) has completed: columns 12, 13 are free; one value per thread
+        put_chain_part(sm, gtid, reinterpret_cast<const float*>(sm + sC1 + (uint32_t)next_stage * (kH * 4))[gtid]);
+      umma::fence_async_smem();
+      umma::fence_before_sync();
+      if (group_sync_or<1>(!ok)) {
+        if (tid == 0) *abort_flag = 1;
+        break;
+      }
+      if (tid == 0) {
+        umma::fence_after_sync();
+        issue_layer2(base, d, idesc);
+        umma::commit(barM2 + 8 * b);
+      } else if (tid == 32) {
+        mbar_arrive(barE1 + 8 * b);  // epilogue 1(i) is done: group 2 may run epilogue 2(i - 1)
+        if (has_next) {  // buffer b ^ 1 is free once epilogue 2 of tile i - 1 has read it
+          if (i == 0 || umma::mbar_wait(barE2 + 8 * (b ^ 1), (uint32_t)((i - 1) >> 1) & 1u, kWaitTries)) {
+            umma::fence_after_sync();
+            issue_layer1(base, next_stage, tmem + 256u * (uint32_t)(b ^ 1), idesc);
+            umma::commit(barM1 + 8 * (b ^ 1));
+          } else {
+            *abort_flag = 1;
+          }
+        }
       }
     }
-    cp_async_wait_all();  // next tile's A1 / chain part have landed (this thread's copies)
-    umma::fence_async_smem();
-    umma::fence_before_sync();
-    __syncthreads();
-    umma::fence_after_sync();
-    if (*abort_flag) break;
-    if (tid == 0) {
-#pragma unroll
-      for (int s = 0; s < kH / 16; ++s) {
-        const uint32_t koff = (uint32_t)(s & 3) * 32u;  // K = 16 step inside a 64-wide slice
-        const uint64_t ad = umma::desc_sw128(base + sA2 + (uint32_t)(s >> 2) * (kCand * 128) + koff);
-        const uint64_t bd = umma::desc_sw128(base + sW2 + (uint32_t)(s >> 2) * (kH * 128) + koff);
-        umma::mma_bf16(d2, ad, bd, idesc, s > 0 ? 1u : 0u);
-      }
-      umma::commit(bar2);
-      if (has_next) {  // D1 was fully read by epilogue 1 above
-        const uint32_t a1 = base + sA1 + (uint32_t)(buf ^ 1) * (kCand * 32);
-        umma::mma_bf16(d1, umma::desc_interleave(a1, 128, 256), umma::desc_interleave(base + sW1a, 128, 256),
-                       idesc, 0u);
-        umma::commit(bar1);
-      }
-    }
-    if (!umma::mbar_wait(bar2, ph2, kWaitTries)) atomicExch(abort_flag, 1);
-    ph2 ^= 1u;
-    umma::fence_after_sync();
-    // epilogue 2: relu(D2 + b2) . w3 over this warp's 128 columns
-    float acc = 0.f;
+  } else {
+    // ---- warp group 2: epilogue 2 ----
+    const float4* b2v = reinterpret_cast<const float4*>(b2s);
+    const float4* w3v = reinterpret_cast<const float4*>(w3s);
+    for (int i = 0, t = blockIdx.x; t < A.tiles; ++i, t += G) {
+      const int b = i & 1;
+      const uint32_t d = tmem + 256u * (uint32_t)b;
+      bool ok = umma::mbar_wait(barM2 + 8 * b, (uint32_t)(i >> 1) & 1u, kWaitTries);
+      // leave the issue slots to epilogue 1 of the next tile, which the tensor core waits for
+      if (t + G < A.tiles) ok = ok && umma::mbar_wait(barE1 + 8 * (b ^ 1), (uint32_t)((i + 1) >> 1) & 1u, kWaitTries);
+      ok = __all_sync(0xffffffffu, ok && !*abort_flag);
+      umma::fence_after_sync();
+      float* pb = part + b * (2 * kCand);
+      if (ok) {
+        float acc[4] = {0.f, 0.f, 0.f, 0.f};
 #pragma unroll 1
-    for (int j = 4 * half; j < 4 * half + 4; ++j) {
-      float v[32];
-      umma::tmem_ld32(d2 + lane_off + 32 * j, v);
+        for (int sl = sl0; sl < sl0 + 2; ++sl) {
+          uint32_t r[64];
+          umma::tmem_ld64(d + lane_off + 64u * (uint32_t)sl, r);
 #pragma unroll
-      for (int e = 0; e < 32; ++e) acc = fmaf(fmaxf(v[e] + b2s[32 * j + e], 0.f), w3s[32 * j + e], acc);
+          for (int q = 0; q < 16; ++q) {
+            const float4 bb = b2v[16 * sl + q], ww = w3v[16 * sl + q];
+            acc[0] = fmaf(fmaxf(__uint_as_float(r[4 * q + 0]) + bb.x, 0.f), ww.x, acc[0]);
+            acc[1] = fmaf(fmaxf(__uint_as_float(r[4 * q + 1]) + bb.y, 0.f), ww.y, acc[1]);
+            acc[2] = fmaf(fmaxf(__uint_as_float(r[4 * q + 2]) + bb.z, 0.f), ww.z, acc[2]);
+            acc[3] = fmaf(fmaxf(__uint_as_float(r[4 * q + 3]) + bb.w, 0.f), ww.w, acc[3]);
+          }
+        }
+        umma::fence_before_sync();
+        mbar_arrive(barE2 + 8 * b);
+        pb[colhalf * kCand + row] = (acc[0] + acc[1]) + (acc[2] + acc[3]);
+      }
+      if (group_sync_or<2>(!ok)) {
+        *abort_flag = 1;
+        break;
+      }
+      if (colhalf == 0) A.pred[(size_t)t * kCand + row] = (pb[row] + pb[kCand + row] + b3) * kTargetScale;
     }
-    part[half * kCand + row] = acc;
-    umma::fence_before_sync();
-    __syncthreads();
-    if (half == 0) A.pred[(size_t)t * kCand + row] = (part[row] + part[kCand + row] + b3) * kTargetScale;
-    if (*abort_flag) break;
   }
-  if (*abort_flag && tid == 0) {
-    if (A.error_word) atomicOr(A.error_word, kErrTimeout);
-    umma::mbar_wait(bar1, ph1, kWaitTries);  // bounded waits for MMAs still in flight
-    umma::mbar_wait(bar2, ph2, kWaitTries);
+  if (tid == 0 || tid == 32) {  // drain: every MMA issued by threads 0 and 32 has completed
+    umma::commit(barFin);
+    if (!umma::mbar_wait(barFin, 0u, kWaitTries)) *abort_flag = 1;
   }
   cp_async_wait_all();
   umma::fence_before_sync();
   __syncthreads();
+  if (tid == 0 && *abort_flag && A.error_word) atomicOr(A.error_word, kErrTimeout);
   if (warp == 0) {
     umma::fence_after_sync();
     umma::tmem_dealloc(tmem, 512);
@@ -333,7 +526,7 @@ struct StepArgs {
   int moves;              // moves drawn per step (without replacement)
 };
 
-constexpr int kStepWarps = 16;
+constexpr int kStepWarps = 14;  // 2048 chains -> 147 CTAs, one per SM
 
 __global__ void __launch_bounds__(kStepWarps * 32, 1) learned_step_kernel(const StepArgs A) {
   extern __shared__ __align__(16) unsigned char smem[];
@@ -520,7 +713,6 @@ __global__ void gather_kernel(const uint16_t* __restrict__ rb_feat, const uint8_
 // EPI 0: C = acc (+ atomically when split over gridDim.z)
 // EPI 1: Z = acc + bias[n]; C = relu(Z); aux = Z
 // EPI 2: C = acc * (aux[m, n] > 0)
-// EPI 3: C = acc + bias[n]
 template <int EPI>
 __global__ void __launch_bounds__(256) gemm_kernel(int M, int N, int K, const float* __restrict__ A, int sam, int sak,
                                                    const float* __restrict__ Bm, int sbk, int sbn,
@@ -604,10 +796,8 @@ __global__ void __launch_bounds__(256) gemm_kernel(int M, int N, int K, const fl
         v += bias[nn];
         aux[o] = v;
         C[o] = fmaxf(v, 0.f);
-      } else if (EPI == 2) {
-        C[o] = aux[o] > 0.f ? v : 0.f;
       } else {
-        C[o] = v + bias[nn];
+        C[o] = aux[o] > 0.f ? v : 0.f;
       }
     }
   }
@@ -738,12 +928,10 @@ int n3_mlp_candidates(const n3_chains* ch, const n3_mlp* M, uint64_t seed, void*
   cudaStream_t st = (cudaStream_t)stream;
   candidates_kernel<<<ch->n_chains, kCand, 0, st>>>(A);
   N3_TRY(n3host::check_launch("candidates_kernel"));
-  // chain part of layer 1 for every chain: c1 = badn W1b^T + b1   (B(k, n) = W1[n*192 + 12 + k])
+  // chain part of layer 1 for every chain: c1 = badn W1b^T + b1
   const int C = ch->n_chains;
-  gemm_kernel<3><<<dim3(kH / 64, (C + 63) / 64, 1), 256, 0, st>>>(C, kH, kChainFeat, M->badn, kChainFeat, 1,
-                                                                  M->params + oW1 + kCandFeat, 1, kIn, M->c1, kH,
-                                                                  M->params + oB1, nullptr);
-  return n3host::check_launch("chain layer-1 gemm");
+  chain_part_kernel<<<(C + kChainTile - 1) / kChainTile, kH, 0, st>>>(C, M->badn, M->params, M->c1);
+  return n3host::check_launch("chain_part_kernel");
 }
 
 int n3_mlp_infer(const n3_mlp* M, int tiles, void* stream) {

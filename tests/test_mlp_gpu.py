@@ -59,6 +59,7 @@ def test_inference_matches_bf16_reference(cuda):
         c1 = b1 + W1[:, 12:162] @ x_chain
         assert np.allclose(c1_dev[c], c1, rtol=1e-5, atol=1e-5)
         F = np.zeros((128, 16))
+        F[:, 12:14] = 1.0  # constant columns that carry the chain part (hi, lo) into layer 1
         for j in range(128):
             u, v = cand[c, j] & 0xFF, (cand[c, j] >> 8) & 0xFF
             F[j, :12] = features(cols[c], bad[c], 75, u, v)
