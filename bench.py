@@ -55,10 +55,13 @@ def parse():
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", choices=["b200", "reference"], default="b200")
     ap.add_argument("--states", type=int, default=STATES)
-    ap.add_argument("--mode", choices=["checked", "det", "slope", "tempering", "learned", "time-to-target"],
+    ap.add_argument("--mode", choices=["checked", "det", "slope", "tempering", "learned", "time-to-target", "beam",
+                                       "scan"],
                     default="checked",
                     help="kernel a step runs: fused checked scoring (default), determinant only, slope only; "
-                         "or the learned-vs-plain time-to-target comparison")
+                         "tempering / learned chain rounds; one device beam-search generation (beam); one "
+                         "four-cycle + double-switch neighbourhood scan (scan); or the learned-vs-plain "
+                         "time-to-target comparison")
     ap.add_argument("--no-secondary", action="store_true", help="skip the delta/tempering/MLP measurements")
     ap.add_argument("--seeds", type=int, default=3, help="time-to-target: seeds per method")
     ap.add_argument("--budget", type=float, default=30.0, help="time-to-target: device seconds per run")
@@ -290,6 +293,67 @@ def run_chain_mode(args):
             "config": {"workload": f"n=75, 2048 chains, 32 ladders x 64 temperatures (0.05..5.0): {what}",
                        "mode": args.mode, **({"moves_per_step": moves} if args.mode == "learned" else {})},
             "best_E": int(ch.best_energy.min().item())}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def run_search_mode(args):
+    """--mode beam: one step = one generation of the device beam search at the
+    reference CLI's defaults (gpu-search --engine device: population 32768,
+    elite 64, max strength 12, energy window 12, bad bias 85; cli.py:1515-1527),
+    n = 75, from random_state(75, Random(91001)).  --mode scan: one step = one
+    n3_neighborhood_scan (every four-cycle and double switch, 4.67 M candidates)
+    through the worst slot of that state."""
+    from random import Random
+
+    import torch
+
+    from no_three_in_line_b200 import _lib, gpu_device_search, gpu_neighborhood, state
+
+    _lib.require_device()
+    init = state.random_state(N, Random(91001))
+    stream = torch.cuda.current_stream()
+    if args.mode == "beam":
+        pop, elite = 32768, 64
+        gens = args.warmup + args.steps
+        beam = gpu_device_search.DeviceBeam(N, seed=1, population=pop, elite_size=elite, max_strength=12,
+                                            energy_window=12, bad_bias=85, history_len=gens)
+        beam.init(np.column_stack((init.P, init.Q)).astype(np.int32)[None])
+        counter = iter(range(1, gens + 1))
+        step = lambda: beam.generation(next(counter))  # noqa: E731
+        per_step, unit, what = pop, "children/s", "device beam search generations (mutate, score, select, rank)"
+        launches = 6
+    else:
+        anchor = gpu_neighborhood.bad_anchor_indices(init, 1)[0]
+        dp = torch.tensor(init.P, dtype=torch.int32, device="cuda")
+        dq = torch.tensor(init.Q, dtype=torch.int32, device="cuda")
+        base = int(gpu_neighborhood.score_and_badness(np.asarray(init.P), np.asarray(init.Q))[0])
+        out = torch.empty(4, dtype=torch.int64, device="cuda")
+        L = _lib.lib()
+        step = lambda: _lib.check(L.n3_neighborhood_scan(dp.data_ptr(), dq.data_ptr(), N, anchor, base,  # noqa: E731
+                                                         out.data_ptr(), out.data_ptr() + 16,
+                                                         int(stream.cuda_stream)), "n3_neighborhood_scan")
+        per_step, unit, what = 64824 * 8 * 9, "candidates/s", "four-cycle + double-switch candidates scored exactly"
+        launches = 1
+    for _ in range(max(3, args.warmup) if args.mode == "scan" else args.warmup):
+        step()
+    torch.cuda.synchronize()
+    start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with ClockSampler(torch.cuda.current_device()) as clocks:
+        start.record(stream)
+        for _ in range(args.steps):
+            step()
+        end.record(stream)
+        end.synchronize()
+    secs = start.elapsed_time(end) / 1e3
+    line = {"metric": METRIC, "value": per_step * args.steps / secs, "unit": unit, "n_gpus": 1, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": 1e3 * secs / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "int32",
+            "data": "synthetic: random_state(75, Random(91001))",
+            "config": {"workload": f"n=75: {what}", "mode": args.mode}, "gpu_launches": launches * args.steps,
+            "clocks": clocks.summary()}
+    if args.mode == "beam":
+        line["best_E"] = int(beam.read_status()[1])
     print(json.dumps(line), flush=True)
     return 0
 
@@ -532,6 +596,8 @@ def main():
         return run_time_to_target(args)
     if args.mode in ("tempering", "learned"):
         return run_chain_mode(args)
+    if args.mode in ("beam", "scan"):
+        return run_search_mode(args)
     return run_b200(args)
 
 

@@ -263,6 +263,99 @@ int n3_mlp_train(const n3_mlp* mlp, int n_chains, int batch, float lr, uint64_t 
 int n3_mlp_train_noalloc(const n3_mlp* mlp, int n_chains, int batch, float lr, uint64_t seed, float* adam_m,
                          float* adam_v, void* stream);
 
+/* ---------------------------------------------------------------------------
+ * Multi-point moves.
+ * ------------------------------------------------------------------------- */
+
+/* Scores after three-cycles (src/no_three_75/accelerated.py:196-276,
+ * evaluate_three_cycles): candidate (u, v, w, o) moves u <- v <- w <- u (o = 0)
+ * or u <- w <- v <- u (o = 1) column-wise; scores[k] = current + exact dE.
+ * Candidates must be the kind search.py:38-65 generates (three rows, three
+ * distinct columns, no repeated column in a row afterwards); any other gets
+ * 1 << 60.  p, q int32 [n]; candidates int32 [count][4]; scores int64 [count]. */
+int n3_three_cycle_scores(const int32_t* p, const int32_t* q, int n, const int32_t* candidates, int count,
+                          int64_t current, int64_t* scores, void* stream);
+
+/* Every four-cycle and double switch through slot `anchor`
+ * (src/no_three_75/gpu_neighborhood.py:70-211, best_four_cycle and
+ * best_double_switch), scored exactly.  best[0] / best[1] receive
+ * (score << 32 | index) of the lowest-scoring legal four-cycle / double switch,
+ * the index counting candidates in the reference's enumeration order (row
+ * triple, layers, ordering or pairing), the first one on ties; legal[0] /
+ * legal[1] the number of legal candidates.  current: E of the state.
+ * best, legal: device uint64 [2] each. */
+int n3_neighborhood_scan(const int32_t* p, const int32_t* q, int n, int anchor, int64_t current,
+                         unsigned long long* best, unsigned long long* legal, void* stream);
+
+/* ---------------------------------------------------------------------------
+ * Device-resident beam search: the generation loop of
+ * src/no_three_75/gpu_device_search.py:254-432 (gpu_device_beam_search) with
+ * mutation, scoring, selection (including its random.Random shuffle) and
+ * elite ranking all on the device, so a generation needs no host round trip.
+ * ------------------------------------------------------------------------- */
+
+/* The mutation kernel mutate_population (gpu_device_search.py:27-114, its
+ * test-facing wrapper mutate_population_device :206-251): child c copies
+ * parent c when c < parent_count, otherwise a parent drawn from the first
+ * quality_count (160/256) or all parents, then applies 1..active_strength
+ * (1 in 32: 1..max_strength) same-slot-layer column swaps, the first slot drawn
+ * by parent badness with probability bad_bias/100; xorshift64* per child
+ * seeded from (seed, child, generation).  Bit-identical to the reference.
+ *   parent_p, parent_q int32 [parent_count][n], parent_badness int32 [parent_count][2n]
+ *   child_p, child_q   int32 [population][n] */
+int n3_beam_mutate(const int32_t* parent_p, const int32_t* parent_q, const int32_t* parent_badness,
+                   int parent_count, int quality_count, int n, int population, int active_strength,
+                   int max_strength, int bad_bias, uint64_t seed, int generation, int32_t* child_p,
+                   int32_t* child_q, void* stream);
+
+/* Python's random.Random(seed) (MT19937 seeded by init_by_array over the 32-bit
+ * words of |seed|), used by the reference for its diversity shuffle
+ * (gpu_device_search.py:280, 343).  state: device uint32[625] (624 words and
+ * the position). */
+int n3_py_random_seed(uint32_t* state, uint64_t seed, void* stream);
+/* random.Random.shuffle(values[0..count)) with that state (count <= 65536),
+ * advancing it exactly as CPython does (_randbelow by getrandbits). */
+int n3_py_random_shuffle(uint32_t* state, int32_t* values, int count, void* stream);
+
+#define N3_BEAM_STATUS 8 /* int64 status words, see n3_beam */
+
+typedef struct n3_beam {
+  int n, population, elite_size, energy_window, max_strength, bad_bias;
+  uint64_t seed;
+  int32_t* elite_p;         /* [elite_size][n] elites, ranked (rank_elites order) */
+  int32_t* elite_q;         /* [elite_size][n] */
+  int32_t* elite_badness;   /* [elite_size][2n] */
+  int32_t* elite_scores;    /* [elite_size] */
+  int32_t* child_p;         /* [population][n] this generation's children */
+  int32_t* child_q;         /* [population][n] */
+  int32_t* child_scores;    /* [population] */
+  int32_t* pick_p;          /* [elite_size][n] selected children before ranking */
+  int32_t* pick_q;          /* [elite_size][n] */
+  int32_t* pick_badness;    /* [elite_size][2n] */
+  int32_t* pick_scores;     /* [elite_size] */
+  int32_t* selected;        /* [elite_size] child indices */
+  uint32_t* rng;            /* [625] random.Random(seed) state */
+  int64_t* status;          /* [N3_BEAM_STATUS]: elite count, best E, best max badness, best sum of
+                               squared badness, last improvement, generations completed,
+                               this generation's best E, improved (0/1) */
+  int32_t* best_p;          /* [n] best state so far (raw P/Q rows) */
+  int32_t* best_q;          /* [n] */
+  int32_t* history;         /* [history_len][2] per generation: its best E, best E so far (or NULL) */
+  int history_len;
+} n3_beam;
+
+/* Set-up: elite rows [0, base_count) hold the initial state and any supplied
+ * elites (base_count <= elite_size); scores and ranks them, records the best
+ * and seeds the shuffle RNG with the search seed (gpu_device_search.py:279-313). */
+int n3_beam_init(const n3_beam* beam, int base_count, void* stream);
+/* One generation (gpu_device_search.py:315-411): mutate the elites into
+ * population children, score them, keep the best quarter plus a shuffled pick
+ * of the children within energy_window of the best, fill from the score order,
+ * rank by (E, max badness, sum of squared badness) and update the best.  Does
+ * nothing once a generation has reached E = 0.  population <= 65536,
+ * elite_size <= 2048. */
+int n3_beam_generation(const n3_beam* beam, int generation, void* stream);
+
 /* Device clock (%globaltimer, ns) written to *out (device int64) in stream
  * order; used to time a run to its first target hit on the device. */
 int n3_device_clock_ns(int64_t* out, void* stream);

@@ -1,0 +1,643 @@
+// Device-resident beam search: the generation loop of
+// src/no_three_75/gpu_device_search.py:254-432 (gpu_device_beam_search) on the
+// GPU.  Per generation, five launches on one stream and no host round trip:
+//   mutate_kernel      children from the ranked elites (gpu_device_search.py:27-114)
+//   det scorer         E of every child (n3_score_population)
+//   select_kernel      stable score order prefix, the children within the energy
+//                      window in index order, their random.Random shuffle, the
+//                      pick of elite_size children (gpu_device_search.py:343-373)
+//   gather_kernel      + det scorer with badness on the picked children
+//   rank_kernel        rank_elites order (gpu_device_search.py:185-197) and the
+//                      best-so-far update by elite_key (:200-203, :388-396)
+// The reference does the selection and ranking on the host with a copy of
+// every child's score each generation.  Here the selection is one CTA: a radix
+// select of the elite_size-th smallest score, a bitonic sort of the scores
+// below it, ordered compactions by block scans, and the shuffle by one thread
+// on a copy of the window list in shared memory (the shuffle is a sequential
+// RNG walk and must consume exactly CPython's draws).
+#include <stdint.h>
+
+#include "n3_common.cuh"
+
+namespace n3 {
+namespace beam {
+
+// --------------------------------------------------------------------------
+// xorshift64* (Vigna), the reference's per-child RNG (gpu_device_search.py:18-25).
+// --------------------------------------------------------------------------
+__device__ __forceinline__ uint64_t xs64(uint64_t& s) {
+  uint64_t x = s;
+  x ^= x >> 12;
+  x ^= x << 25;
+  x ^= x >> 27;
+  s = x;
+  return x * 2685821657736338717ULL;
+}
+
+struct MutArgs {
+  const int32_t* pp;
+  const int32_t* pq;
+  const int32_t* pbad;
+  int parent_count, quality_count, active_strength;  // used when status == nullptr
+  const int64_t* status;                              // beam status: counts and strength derive from it
+  int elite_size, n, population, max_strength, bad_bias, generation;
+  uint64_t seed;
+  int32_t* cp;
+  int32_t* cq;
+};
+
+// One thread per child, as the reference's kernel; same draws in the same order.
+// The parent's total badness is summed once per child instead of once per attempt
+// (it does not change), which leaves every draw and result unchanged.
+__global__ void __launch_bounds__(128) mutate_kernel(const MutArgs A) {
+  const int child = blockIdx.x * blockDim.x + threadIdx.x;
+  if (child >= A.population) return;
+  int parent_count = A.parent_count, quality_count = A.quality_count, active = A.active_strength;
+  if (A.status != nullptr) {
+    if (A.status[1] == 0) return;  // the search has reached E = 0
+    parent_count = (int)A.status[0];
+    quality_count = max(1, min(parent_count, A.elite_size / 4));
+    active = min(A.max_strength, 2 + (A.generation - (int)A.status[4]) / 10);
+  }
+  const int n = A.n, m = 2 * n;
+  uint64_t rng = A.seed ^ (0x9e3779b97f4a7c15ULL * (uint64_t)(child + 1)) ^
+                 (0xbf58476d1ce4e5b9ULL * (uint64_t)(A.generation + 1));
+  int parent = child;
+  if (child >= parent_count) {
+    const uint64_t pick = xs64(rng);
+    const int pool = (pick & 255ULL) < 160ULL ? quality_count : parent_count;
+    parent = (int)(xs64(rng) % (uint64_t)pool);
+  }
+  int32_t* P = A.cp + (size_t)child * n;
+  int32_t* Q = A.cq + (size_t)child * n;
+  const int32_t* src_p = A.pp + (size_t)parent * n;
+  const int32_t* src_q = A.pq + (size_t)parent * n;
+  for (int r = 0; r < n; ++r) {
+    P[r] = src_p[r];
+    Q[r] = src_q[r];
+  }
+  if (child < parent_count) return;
+  const int32_t* bad = A.pbad + (size_t)parent * m;
+  int total = 0;
+  for (int e = 0; e < m; ++e) total += bad[e];
+  int strength;
+  if ((xs64(rng) & 31ULL) == 0ULL)
+    strength = 1 + (int)(xs64(rng) % (uint64_t)A.max_strength);
+  else
+    strength = 1 + (int)(xs64(rng) % (uint64_t)active);
+  for (int step = 0; step < strength; ++step) {
+    for (int attempt = 0; attempt < 32; ++attempt) {
+      int u;
+      if ((int)(xs64(rng) % 100ULL) < A.bad_bias) {
+        if (total) {
+          int t = (int)(xs64(rng) % (uint64_t)total);
+          for (u = 0; u < m - 1; ++u) {
+            t -= bad[u];
+            if (t < 0) break;
+          }
+        } else {
+          u = (int)(xs64(rng) % (uint64_t)m);
+        }
+      } else {
+        u = (int)(xs64(rng) % (uint64_t)m);
+      }
+      const int v = (int)(xs64(rng) % (uint64_t)m);
+      const int ru = u >> 1, rv = v >> 1;
+      if (ru == rv) continue;
+      int32_t* su = (u & 1) ? &Q[ru] : &P[ru];
+      int32_t* sv = (v & 1) ? &Q[rv] : &P[rv];
+      const int cu = *su, cv = *sv;
+      if (cu == cv) continue;
+      const int ou = (u & 1) ? P[ru] : Q[ru];
+      const int ov = (v & 1) ? P[rv] : Q[rv];
+      if (cv == ou || cu == ov) continue;
+      *su = cv;
+      *sv = cu;
+      break;
+    }
+  }
+}
+
+// --------------------------------------------------------------------------
+// MT19937 as CPython's random.Random uses it (Matsumoto & Nishimura, 1998;
+// seeding by init_by_array, 2002), and CPython's shuffle: for i = len-1 .. 1,
+// j = _randbelow(i + 1) with getrandbits(bit_length(i + 1)) and rejection.
+// --------------------------------------------------------------------------
+constexpr int kMT = 624;
+
+__device__ void mt_twist(uint32_t* mt) {
+  for (int k = 0; k < kMT; ++k) {
+    const uint32_t y = (mt[k] & 0x80000000u) | (mt[(k + 1) % kMT] & 0x7fffffffu);
+    mt[k] = mt[(k + 397) % kMT] ^ (y >> 1) ^ ((y & 1u) ? 0x9908b0dfu : 0u);
+  }
+}
+
+__device__ __forceinline__ uint32_t mt_next(uint32_t* mt, int& idx) {
+  if (idx >= kMT) {
+    mt_twist(mt);
+    idx = 0;
+  }
+  uint32_t y = mt[idx++];
+  y ^= y >> 11;
+  y ^= (y << 7) & 0x9d2c5680u;
+  y ^= (y << 15) & 0xefc60000u;
+  y ^= y >> 18;
+  return y;
+}
+
+// random.Random.shuffle on values[0..count) (any address space).
+template <class T>
+__device__ void py_shuffle(uint32_t* mt, int& idx, T* values, int count) {
+  for (int i = count - 1; i >= 1; --i) {
+    const uint32_t range = (uint32_t)i + 1u;
+    const int k = 32 - __clz(range);  // bit_length(i + 1)
+    uint32_t r;
+    do {
+      r = mt_next(mt, idx) >> (32 - k);
+    } while (r >= range);
+    const T t = values[i];
+    values[i] = values[r];
+    values[r] = t;
+  }
+}
+
+__global__ void py_seed_kernel(uint32_t* state, uint64_t seed) {
+  uint32_t* mt = state;
+  const uint32_t key[2] = {(uint32_t)seed, (uint32_t)(seed >> 32)};
+  const int len = (seed >> 32) ? 2 : 1;
+  mt[0] = 19650218u;
+  for (int i = 1; i < kMT; ++i) mt[i] = 1812433253u * (mt[i - 1] ^ (mt[i - 1] >> 30)) + (uint32_t)i;
+  int i = 1, j = 0;
+  for (int k = kMT > len ? kMT : len; k; --k) {
+    mt[i] = (mt[i] ^ ((mt[i - 1] ^ (mt[i - 1] >> 30)) * 1664525u)) + key[j] + (uint32_t)j;
+    ++i;
+    ++j;
+    if (i >= kMT) {
+      mt[0] = mt[kMT - 1];
+      i = 1;
+    }
+    if (j >= len) j = 0;
+  }
+  for (int k = kMT - 1; k; --k) {
+    mt[i] = (mt[i] ^ ((mt[i - 1] ^ (mt[i - 1] >> 30)) * 1566083941u)) - (uint32_t)i;
+    ++i;
+    if (i >= kMT) {
+      mt[0] = mt[kMT - 1];
+      i = 1;
+    }
+  }
+  mt[0] = 0x80000000u;
+  state[kMT] = kMT;  // position: the first draw twists
+}
+
+__global__ void py_shuffle_kernel(uint32_t* state, int32_t* values, int count) {
+  __shared__ uint32_t mt[kMT];
+  for (int i = threadIdx.x; i < kMT; i += blockDim.x) mt[i] = state[i];
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    int idx = (int)state[kMT];
+    py_shuffle(mt, idx, values, count);
+    state[kMT] = (uint32_t)idx;
+  }
+  __syncthreads();
+  for (int i = threadIdx.x; i < kMT; i += blockDim.x) state[i] = mt[i];
+}
+
+// --------------------------------------------------------------------------
+// Selection (one CTA of kSelThreads threads).
+// --------------------------------------------------------------------------
+constexpr int kSelThreads = 1024;
+constexpr int kMaxPopulation = 65536;
+constexpr int kMaxElite = 2048;
+
+// Exclusive block scan of one value per thread; returns this thread's offset and
+// writes the total to *total (all threads).  `warp_tot`: shared int[32].
+__device__ __forceinline__ int block_exclusive_scan(int v, int* warp_tot, int* total) {
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  int x = v;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    const int y = __shfl_up_sync(0xffffffffu, x, o);
+    if (lane >= o) x += y;
+  }
+  if (lane == 31) warp_tot[warp] = x;
+  __syncthreads();
+  if (warp == 0) {
+    int w = lane < (int)(blockDim.x >> 5) ? warp_tot[lane] : 0;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const int y = __shfl_up_sync(0xffffffffu, w, o);
+      if (lane >= o) w += y;
+    }
+    warp_tot[lane] = w;  // inclusive prefix of the warp totals
+  }
+  __syncthreads();
+  const int before = (warp > 0 ? warp_tot[warp - 1] : 0) + x - v;
+  *total = warp_tot[(blockDim.x >> 5) - 1];
+  __syncthreads();
+  return before;
+}
+
+struct SelArgs {
+  const int32_t* scores;  // [population]
+  int population, elite_size, energy_window;
+  int64_t* status;
+  uint32_t* rng;          // [625]
+  int32_t* selected;      // [elite_size]
+};
+
+__global__ void __launch_bounds__(kSelThreads, 1) select_kernel(const SelArgs A) {
+  extern __shared__ __align__(16) unsigned char smem[];
+  const int P = A.population, E = A.elite_size, tid = threadIdx.x;
+  uint64_t* keys = reinterpret_cast<uint64_t*>(smem);                 // [kMaxElite]
+  uint32_t* mt = reinterpret_cast<uint32_t*>(keys + kMaxElite);       // [624]
+  int32_t* order = reinterpret_cast<int32_t*>(mt + kMT);              // [kMaxElite] score-order prefix
+  uint32_t* mark = reinterpret_cast<uint32_t*>(order + kMaxElite);    // [kMaxPopulation / 32]
+  uint16_t* window = reinterpret_cast<uint16_t*>(mark + kMaxPopulation / 32);  // [population]
+  __shared__ uint32_t hist[256];
+  __shared__ int warp_tot[32];
+  __shared__ int s_misc[4];
+  if (A.status[1] == 0) return;  // uniform: the search has reached E = 0
+  const int64_t limit = A.status[1] + (int64_t)A.energy_window;
+  for (int i = tid; i < kMaxPopulation / 32; i += kSelThreads) mark[i] = 0u;
+  for (int i = tid; i < kMT; i += kSelThreads) mt[i] = A.rng[i];
+  const int chunk = (P + kSelThreads - 1) / kSelThreads;
+  const int lo = min(P, tid * chunk), hi = min(P, lo + chunk);
+
+  // 1. T = the E-th smallest score (radix select over 32-bit scores, 8 bits a pass)
+  uint32_t prefix = 0u, mask = 0u;
+  int remaining = E;  // 1-based rank of the E-th element among those matching prefix
+  for (int shift = 24; shift >= 0; shift -= 8) {
+    for (int i = tid; i < 256; i += kSelThreads) hist[i] = 0u;
+    __syncthreads();
+    for (int i = lo; i < hi; ++i) {
+      const uint32_t x = (uint32_t)A.scores[i];
+      if ((x & mask) == prefix) atomicAdd(&hist[(x >> shift) & 255u], 1u);
+    }
+    __syncthreads();
+    if (tid == 0) {
+      int before = 0, d = 0;
+      for (; d < 255; ++d) {
+        if (before + (int)hist[d] >= remaining) break;
+        before += (int)hist[d];
+      }
+      s_misc[0] = d;
+      s_misc[1] = remaining - before;
+    }
+    __syncthreads();
+    prefix |= (uint32_t)s_misc[0] << shift;
+    mask |= 255u << shift;
+    remaining = s_misc[1];
+    __syncthreads();
+  }
+  const uint32_t T = prefix;
+  const int n_less = E - remaining;  // scores below T; then `remaining` ties at T by index
+
+  // 2. scores below T, sorted by (score, index): a bitonic sort of at most E - 1 keys
+  if (tid == 0) s_misc[2] = 0;
+  __syncthreads();
+  for (int i = lo; i < hi; ++i) {
+    const uint32_t x = (uint32_t)A.scores[i];
+    if (x < T) keys[atomicAdd(&s_misc[2], 1)] = ((uint64_t)x << 32) | (uint32_t)i;
+  }
+  __syncthreads();
+  int width = 1;
+  while (width < n_less) width <<= 1;
+  for (int i = n_less + tid; i < width; i += kSelThreads) keys[i] = ~0ull;
+  __syncthreads();
+  for (int size = 2; size <= width; size <<= 1) {
+    for (int stride = size >> 1; stride > 0; stride >>= 1) {
+      for (int i = tid; i < width; i += kSelThreads) {
+        const int j = i ^ stride;
+        if (j > i) {
+          const bool up = (i & size) == 0;
+          const uint64_t a = keys[i], b = keys[j];
+          if ((a > b) == up) {
+            keys[i] = b;
+            keys[j] = a;
+          }
+        }
+      }
+      __syncthreads();
+    }
+  }
+  for (int i = tid; i < n_less; i += kSelThreads) order[i] = (int32_t)(uint32_t)keys[i];
+
+  // 3. the first `remaining` ties at T in index order, then the window list in
+  //    index order (both by ordered compaction over the threads' chunks)
+  int c_tie = 0, c_win = 0;
+  for (int i = lo; i < hi; ++i) {
+    const int x = A.scores[i];
+    c_tie += (uint32_t)x == T;
+    c_win += (int64_t)x <= limit;
+  }
+  int total;
+  int o_tie = block_exclusive_scan(c_tie, warp_tot, &total);
+  int o_win = block_exclusive_scan(c_win, warp_tot, &total);
+  const int n_window = total;
+  for (int i = lo; i < hi; ++i) {
+    const int x = A.scores[i];
+    if ((uint32_t)x == T) {
+      if (o_tie < remaining) order[n_less + o_tie] = i;
+      ++o_tie;
+    }
+    if ((int64_t)x <= limit) window[o_win++] = (uint16_t)i;
+  }
+  __syncthreads();
+
+  // 4. one thread: the shuffle and the pick (gpu_device_search.py:340-373)
+  if (tid == 0) {
+    int idx = (int)A.rng[kMT];
+    py_shuffle(mt, idx, window, n_window);
+    A.rng[kMT] = (uint32_t)idx;
+    int sel = 0;
+    const int quality_keep = max(1, E / 4);
+    for (int r = 0; r < quality_keep; ++r) {
+      const int c = order[r];
+      mark[c >> 5] |= 1u << (c & 31);
+      A.selected[sel++] = c;
+    }
+    for (int k = 0; k < n_window && sel < E; ++k) {
+      const int c = window[k];
+      if (!(mark[c >> 5] & (1u << (c & 31)))) {
+        mark[c >> 5] |= 1u << (c & 31);
+        A.selected[sel++] = c;
+      }
+    }
+    for (int r = 0; r < E && sel < E; ++r) {
+      const int c = order[r];
+      if (!(mark[c >> 5] & (1u << (c & 31)))) {
+        mark[c >> 5] |= 1u << (c & 31);
+        A.selected[sel++] = c;
+      }
+    }
+  }
+  __syncthreads();
+  for (int i = tid; i < kMT; i += kSelThreads) A.rng[i] = mt[i];
+}
+
+constexpr size_t kSelSmem = sizeof(uint64_t) * kMaxElite + sizeof(uint32_t) * kMT + sizeof(int32_t) * kMaxElite +
+                            sizeof(uint32_t) * (kMaxPopulation / 32) + sizeof(uint16_t) * kMaxPopulation;
+
+// pick rows r = child rows selected[r]
+__global__ void gather_kernel(const int32_t* __restrict__ cp, const int32_t* __restrict__ cq,
+                              const int32_t* __restrict__ cs, const int32_t* __restrict__ selected, int n,
+                              const int64_t* status, int32_t* pp, int32_t* pq, int32_t* ps) {
+  if (status[1] == 0) return;
+  const int r = blockIdx.x, c = selected[r];
+  for (int i = threadIdx.x; i < n; i += blockDim.x) {
+    pp[(size_t)r * n + i] = cp[(size_t)c * n + i];
+    pq[(size_t)r * n + i] = cq[(size_t)c * n + i];
+  }
+  if (threadIdx.x == 0) ps[r] = cs[c];
+}
+
+// --------------------------------------------------------------------------
+// Ranking (one CTA): rank_elites (gpu_device_search.py:185-197) is a stable
+// sort by elite_key = (E, max badness, sum of squared badness); each element's
+// rank is the number of keys before it.  Then the best-so-far update
+// (gpu_device_search.py:388-396; set-up: :305-310).
+// --------------------------------------------------------------------------
+constexpr int kRankThreads = 1024;
+
+struct RankArgs {
+  const int32_t* pp;
+  const int32_t* pq;
+  const int32_t* pbad;
+  const int32_t* ps;
+  int count;       // picks to rank (set-up: the base count; a generation: elite_size)
+  int n, generation;
+  int32_t* ep;
+  int32_t* eq;
+  int32_t* ebad;
+  int32_t* es;
+  int64_t* status;
+  int32_t* best_p;
+  int32_t* best_q;
+  int32_t* history;
+  int history_len;
+};
+
+__global__ void __launch_bounds__(kRankThreads, 1) rank_kernel(const RankArgs A) {
+  __shared__ int32_t s_score[kMaxElite], s_max[kMaxElite], s_rank[kMaxElite];
+  __shared__ int64_t s_ss[kMaxElite];
+  __shared__ int s_first, s_improved;
+  if (A.generation > 0 && A.status[1] == 0) return;  // uniform
+  const int C = A.count, m = 2 * A.n, tid = threadIdx.x;
+  for (int i = tid; i < C; i += kRankThreads) {
+    int mx = INT32_MIN;
+    int64_t ss = 0;
+    for (int s = 0; s < m; ++s) {
+      const int b = A.pbad[(size_t)i * m + s];
+      mx = max(mx, b);
+      ss += (int64_t)b * b;
+    }
+    s_score[i] = A.ps[i];
+    s_max[i] = mx;
+    s_ss[i] = ss;
+  }
+  __syncthreads();
+  for (int i = tid; i < C; i += kRankThreads) {
+    const int a0 = s_score[i], a1 = s_max[i];
+    const int64_t a2 = s_ss[i];
+    int r = 0;
+    for (int j = 0; j < C; ++j) {
+      const int b0 = s_score[j], b1 = s_max[j];
+      const int64_t b2 = s_ss[j];
+      const bool less = b0 < a0 || (b0 == a0 && (b1 < a1 || (b1 == a1 && (b2 < a2 || (b2 == a2 && j < i)))));
+      r += less;
+    }
+    s_rank[i] = r;
+    if (r == 0) s_first = i;
+  }
+  __syncthreads();
+  for (int e = tid; e < C * A.n; e += kRankThreads) {
+    const int i = e / A.n, k = e % A.n;
+    A.ep[(size_t)s_rank[i] * A.n + k] = A.pp[e];
+    A.eq[(size_t)s_rank[i] * A.n + k] = A.pq[e];
+  }
+  for (int e = tid; e < C * m; e += kRankThreads) {
+    const int i = e / m, k = e % m;
+    A.ebad[(size_t)s_rank[i] * m + k] = A.pbad[e];
+  }
+  for (int i = tid; i < C; i += kRankThreads) A.es[s_rank[i]] = s_score[i];
+  if (tid == 0) {
+    const int f = s_first;
+    const int64_t k0 = s_score[f], k1 = s_max[f], k2 = s_ss[f];
+    int64_t* st = A.status;
+    const bool improved = A.generation == 0 || k0 < st[1] || (k0 == st[1] && (k1 < st[2] || (k1 == st[2] && k2 < st[3])));
+    if (improved) {
+      st[1] = k0;
+      st[2] = k1;
+      st[3] = k2;
+      if (A.generation > 0) st[4] = A.generation;
+    }
+    st[0] = C;
+    if (A.generation == 0) st[4] = 0;
+    st[5] = A.generation;
+    st[6] = k0;
+    st[7] = improved && A.generation > 0;
+    if (A.history != nullptr && A.generation >= 1 && A.generation <= A.history_len) {
+      A.history[2 * (A.generation - 1)] = (int32_t)k0;
+      A.history[2 * (A.generation - 1) + 1] = (int32_t)st[1];
+    }
+    s_improved = improved;
+  }
+  __syncthreads();
+  if (s_improved) {
+    const int f = s_first;
+    for (int k = tid; k < A.n; k += kRankThreads) {
+      A.best_p[k] = A.pp[(size_t)f * A.n + k];
+      A.best_q[k] = A.pq[(size_t)f * A.n + k];
+    }
+  }
+}
+
+}  // namespace beam
+}  // namespace n3
+
+namespace n3host {
+
+static int check_beam(const n3_beam* b) {
+  if (b == nullptr) return set_error(N3_ERR_ARG, "null beam descriptor");
+  if (b->n < 3 || b->n > N3_MAX_N) return set_error(N3_ERR_RANGE, "beam: n must lie in [3, %d]", N3_MAX_N);
+  if (b->elite_size < 2 || b->elite_size > n3::beam::kMaxElite)
+    return set_error(N3_ERR_RANGE, "beam: elite_size must lie in [2, %d]", n3::beam::kMaxElite);
+  if (b->population < b->elite_size || b->population > n3::beam::kMaxPopulation)
+    return set_error(N3_ERR_RANGE, "beam: population must lie in [elite_size, %d]", n3::beam::kMaxPopulation);
+  if (b->max_strength < 1) return set_error(N3_ERR_RANGE, "beam: max_strength must be positive");
+  if (b->bad_bias < 0 || b->bad_bias > 100) return set_error(N3_ERR_RANGE, "beam: bad_bias must lie in [0, 100]");
+  if (b->energy_window < 0) return set_error(N3_ERR_RANGE, "beam: energy_window must be non-negative");
+  const void* ptrs[] = {b->elite_p, b->elite_q, b->elite_badness, b->elite_scores, b->child_p, b->child_q,
+                        b->child_scores, b->pick_p, b->pick_q, b->pick_badness, b->pick_scores, b->selected,
+                        b->rng, b->status, b->best_p, b->best_q};
+  for (const void* p : ptrs)
+    if (p == nullptr) return set_error(N3_ERR_ARG, "beam: null buffer");
+  return N3_OK;
+}
+
+static n3::beam::RankArgs rank_args(const n3_beam* b, int count, int generation) {
+  n3::beam::RankArgs R;
+  R.pp = b->pick_p;
+  R.pq = b->pick_q;
+  R.pbad = b->pick_badness;
+  R.ps = b->pick_scores;
+  R.count = count;
+  R.n = b->n;
+  R.generation = generation;
+  R.ep = b->elite_p;
+  R.eq = b->elite_q;
+  R.ebad = b->elite_badness;
+  R.es = b->elite_scores;
+  R.status = b->status;
+  R.best_p = b->best_p;
+  R.best_q = b->best_q;
+  R.history = b->history;
+  R.history_len = b->history_len;
+  return R;
+}
+
+}  // namespace n3host
+
+extern "C" {
+
+int n3_beam_mutate(const int32_t* parent_p, const int32_t* parent_q, const int32_t* parent_badness,
+                   int parent_count, int quality_count, int n, int population, int active_strength,
+                   int max_strength, int bad_bias, uint64_t seed, int generation, int32_t* child_p,
+                   int32_t* child_q, void* stream) {
+  if (!parent_p || !parent_q || !parent_badness || !child_p || !child_q)
+    return n3host::set_error(N3_ERR_ARG, "beam mutate: null buffer");
+  if (n < 2 || n > N3_MAX_N || parent_count < 1 || population < 0 || quality_count < 1 ||
+      quality_count > parent_count || active_strength < 1 || max_strength < 1 || bad_bias < 0 || bad_bias > 100)
+    return n3host::set_error(N3_ERR_RANGE, "beam mutate: argument out of range");
+  if (population == 0) return N3_OK;
+  n3::beam::MutArgs A;
+  A.pp = parent_p;
+  A.pq = parent_q;
+  A.pbad = parent_badness;
+  A.parent_count = parent_count;
+  A.quality_count = quality_count;
+  A.active_strength = active_strength;
+  A.status = nullptr;
+  A.elite_size = parent_count;
+  A.n = n;
+  A.population = population;
+  A.max_strength = max_strength;
+  A.bad_bias = bad_bias;
+  A.generation = generation;
+  A.seed = seed;
+  A.cp = child_p;
+  A.cq = child_q;
+  n3::beam::mutate_kernel<<<(population + 127) / 128, 128, 0, (cudaStream_t)stream>>>(A);
+  return n3host::check_launch("beam mutate_kernel");
+}
+
+int n3_py_random_seed(uint32_t* state, uint64_t seed, void* stream) {
+  if (!state) return n3host::set_error(N3_ERR_ARG, "null RNG state");
+  n3::beam::py_seed_kernel<<<1, 1, 0, (cudaStream_t)stream>>>(state, seed);
+  return n3host::check_launch("py_seed_kernel");
+}
+
+int n3_py_random_shuffle(uint32_t* state, int32_t* values, int count, void* stream) {
+  if (!state || (!values && count > 0)) return n3host::set_error(N3_ERR_ARG, "null shuffle buffer");
+  if (count < 0 || count > n3::beam::kMaxPopulation) return n3host::set_error(N3_ERR_RANGE, "shuffle: bad count");
+  n3::beam::py_shuffle_kernel<<<1, 256, 0, (cudaStream_t)stream>>>(state, values, count);
+  return n3host::check_launch("py_shuffle_kernel");
+}
+
+int n3_beam_init(const n3_beam* b, int base_count, void* stream) {
+  N3_TRY(n3host::check_beam(b));
+  if (base_count < 1 || base_count > b->elite_size) return n3host::set_error(N3_ERR_RANGE, "beam: bad base count");
+  cudaStream_t st = (cudaStream_t)stream;
+  const size_t rows = sizeof(int32_t) * (size_t)base_count * b->n;
+  if (cudaMemcpyAsync(b->pick_p, b->elite_p, rows, cudaMemcpyDeviceToDevice, st) != cudaSuccess ||
+      cudaMemcpyAsync(b->pick_q, b->elite_q, rows, cudaMemcpyDeviceToDevice, st) != cudaSuccess)
+    return n3host::set_error(N3_ERR_CUDA, "beam init: copy failed");
+  N3_TRY(n3_score_population(b->pick_p, b->pick_q, base_count, b->n, b->pick_scores, b->pick_badness, stream));
+  n3::beam::rank_kernel<<<1, n3::beam::kRankThreads, 0, st>>>(n3host::rank_args(b, base_count, 0));
+  N3_TRY(n3host::check_launch("beam rank_kernel"));
+  return n3_py_random_seed(b->rng, b->seed, stream);
+}
+
+int n3_beam_generation(const n3_beam* b, int generation, void* stream) {
+  N3_TRY(n3host::check_beam(b));
+  if (generation < 1) return n3host::set_error(N3_ERR_RANGE, "beam: generations count from 1");
+  cudaStream_t st = (cudaStream_t)stream;
+  n3::beam::MutArgs M;
+  M.pp = b->elite_p;
+  M.pq = b->elite_q;
+  M.pbad = b->elite_badness;
+  M.parent_count = M.quality_count = M.active_strength = 0;
+  M.status = b->status;
+  M.elite_size = b->elite_size;
+  M.n = b->n;
+  M.population = b->population;
+  M.max_strength = b->max_strength;
+  M.bad_bias = b->bad_bias;
+  M.generation = generation;
+  M.seed = b->seed;
+  M.cp = b->child_p;
+  M.cq = b->child_q;
+  n3::beam::mutate_kernel<<<(b->population + 127) / 128, 128, 0, st>>>(M);
+  N3_TRY(n3host::check_launch("beam mutate_kernel"));
+  N3_TRY(n3_score_population(b->child_p, b->child_q, b->population, b->n, b->child_scores, nullptr, stream));
+  N3_TRY(n3host::allow_smem(reinterpret_cast<const void*>(n3::beam::select_kernel), n3::beam::kSelSmem));
+  n3::beam::SelArgs S;
+  S.scores = b->child_scores;
+  S.population = b->population;
+  S.elite_size = b->elite_size;
+  S.energy_window = b->energy_window;
+  S.status = b->status;
+  S.rng = b->rng;
+  S.selected = b->selected;
+  n3::beam::select_kernel<<<1, n3::beam::kSelThreads, n3::beam::kSelSmem, st>>>(S);
+  N3_TRY(n3host::check_launch("beam select_kernel"));
+  n3::beam::gather_kernel<<<b->elite_size, 128, 0, st>>>(b->child_p, b->child_q, b->child_scores, b->selected, b->n,
+                                                          b->status, b->pick_p, b->pick_q, b->pick_scores);
+  N3_TRY(n3host::check_launch("beam gather_kernel"));
+  N3_TRY(n3_score_population(b->pick_p, b->pick_q, b->elite_size, b->n, b->pick_scores, b->pick_badness, stream));
+  n3::beam::rank_kernel<<<1, n3::beam::kRankThreads, 0, st>>>(n3host::rank_args(b, b->elite_size, generation));
+  return n3host::check_launch("beam rank_kernel");
+}
+
+}  // extern "C"

@@ -519,3 +519,139 @@ void n3o_temper_run(int C, int L, int stride, int32_t* cols, int32_t* bad, int32
                 if (!ladder_rounds || r < ladder_rounds[lad]) n3o_temper_exchange(&T, lad);
     }
 }
+
+/* ------------------------------------------------------------------------
+ * Device beam search mutation (gpu_device_search.py:17-114, the CUDA kernel
+ * `mutate_population`), one child at a time.  The RNG is xorshift64* (Vigna)
+ * seeded per child and generation (gpu_device_search.py:18-25, 44-46): the
+ * multiplier and the two seed-mixing constants are the kernel's.
+ * ---------------------------------------------------------------------- */
+static uint64_t n3o_xs64(uint64_t* s) {
+  uint64_t x = *s;
+  x ^= x >> 12;
+  x ^= x << 25;
+  x ^= x >> 27;
+  *s = x;
+  return x * 2685821657736338717ULL;
+}
+
+void n3o_beam_mutate(const int32_t* pp, const int32_t* pq, const int32_t* pbad, int elite_count, int quality_count,
+                     int n, int population, int active_strength, int max_strength, int bad_bias, uint64_t seed,
+                     int generation, int32_t* cp, int32_t* cq) {
+  const int m = 2 * n;
+  for (int child = 0; child < population; ++child) {
+    uint64_t rng = seed ^ (0x9e3779b97f4a7c15ULL * (uint64_t)(child + 1)) ^
+                   (0xbf58476d1ce4e5b9ULL * (uint64_t)(generation + 1));
+    int parent = child;
+    if (child >= elite_count) {
+      const uint64_t pick = n3o_xs64(&rng);
+      const int pool = (pick & 255ULL) < 160ULL ? quality_count : elite_count;
+      parent = (int)(n3o_xs64(&rng) % (uint64_t)pool);
+    }
+    int32_t* P = cp + (size_t)child * n;
+    int32_t* Q = cq + (size_t)child * n;
+    for (int r = 0; r < n; ++r) {
+      P[r] = pp[(size_t)parent * n + r];
+      Q[r] = pq[(size_t)parent * n + r];
+    }
+    if (child < elite_count) continue;
+    const int32_t* bad = pbad + (size_t)parent * m;
+    int strength;
+    if ((n3o_xs64(&rng) & 31ULL) == 0ULL)
+      strength = 1 + (int)(n3o_xs64(&rng) % (uint64_t)max_strength);
+    else
+      strength = 1 + (int)(n3o_xs64(&rng) % (uint64_t)active_strength);
+    for (int step = 0; step < strength; ++step) {
+      for (int attempt = 0; attempt < 32; ++attempt) {
+        int u;
+        if ((int)(n3o_xs64(&rng) % 100ULL) < bad_bias) {
+          int total = 0;
+          for (int e = 0; e < m; ++e) total += bad[e];
+          if (total) {
+            int t = (int)(n3o_xs64(&rng) % (uint64_t)total);
+            for (u = 0; u < m - 1; ++u) {
+              t -= bad[u];
+              if (t < 0) break;
+            }
+          } else {
+            u = (int)(n3o_xs64(&rng) % (uint64_t)m);
+          }
+        } else {
+          u = (int)(n3o_xs64(&rng) % (uint64_t)m);
+        }
+        const int v = (int)(n3o_xs64(&rng) % (uint64_t)m);
+        const int ru = u >> 1, rv = v >> 1;
+        if (ru == rv) continue;
+        int32_t* su = (u & 1) ? &Q[ru] : &P[ru];
+        int32_t* sv = (v & 1) ? &Q[rv] : &P[rv];
+        const int cu = *su, cv = *sv;
+        if (cu == cv) continue;
+        const int ou = (u & 1) ? P[ru] : Q[ru];
+        const int ov = (v & 1) ? P[rv] : Q[rv];
+        if (cv == ou || cu == ov) continue;
+        *su = cv;
+        *sv = cu;
+        break;
+      }
+    }
+  }
+}
+
+/* ------------------------------------------------------------------------
+ * Three-cycle scores (accelerated.py:196-276): for each candidate
+ * (u, v, w, orientation) the triples through the three slots before the move
+ * (badness sum minus pair lines plus the triple itself) and after it, counted
+ * literally over all pairs as the reference does.
+ * ---------------------------------------------------------------------- */
+static int col3(const int32_t* rows, const int32_t* cols, int a, int b, int c) {
+  return (rows[b] - rows[a]) * (cols[c] - cols[a]) == (cols[b] - cols[a]) * (rows[c] - rows[a]);
+}
+
+void n3o_three_cycles(const int32_t* p, const int32_t* q, int n, const int32_t* cand, int count, int64_t current,
+                      const int64_t* badness, int64_t* out) {
+  const int m = 2 * n;
+  int32_t rows[150], cols[150], nc[150];
+  for (int r = 0; r < n; ++r) {
+    rows[2 * r] = rows[2 * r + 1] = r;
+    cols[2 * r] = p[r];
+    cols[2 * r + 1] = q[r];
+  }
+  for (int k = 0; k < count; ++k) {
+    const int u = cand[4 * k], v = cand[4 * k + 1], w = cand[4 * k + 2], o = cand[4 * k + 3];
+    int64_t juv = 0, juw = 0, jvw = 0;
+    for (int x = 0; x < m; ++x) {
+      if (x != u && x != v) juv += col3(rows, cols, u, v, x);
+      if (x != u && x != w) juw += col3(rows, cols, u, w, x);
+      if (x != v && x != w) jvw += col3(rows, cols, v, w, x);
+    }
+    const int64_t tri = col3(rows, cols, u, v, w);
+    const int64_t old_affected = badness[u] + badness[v] + badness[w] - juv - juw - jvw + tri;
+    for (int x = 0; x < m; ++x) nc[x] = cols[x];
+    if (o == 0) {
+      nc[u] = cols[v];
+      nc[v] = cols[w];
+      nc[w] = cols[u];
+    } else {
+      nc[u] = cols[w];
+      nc[w] = cols[v];
+      nc[v] = cols[u];
+    }
+    int64_t na = 0;
+    const int moved[3] = {u, v, w};
+    for (int t = 0; t < 3; ++t) {
+      const int c = moved[t];
+      for (int i = 0; i < m - 1; ++i) {
+        int skip = 0;
+        for (int s = 0; s <= t; ++s) skip |= i == moved[s];
+        if (skip) continue;
+        for (int j = i + 1; j < m; ++j) {
+          int sk = 0;
+          for (int s = 0; s <= t; ++s) sk |= j == moved[s];
+          if (sk) continue;
+          na += (rows[i] - rows[c]) * (nc[j] - nc[c]) == (nc[i] - nc[c]) * (rows[j] - rows[c]);
+        }
+      }
+    }
+    out[k] = current - old_affected + na;
+  }
+}

@@ -55,6 +55,11 @@ def lib():
         L.n3o_score_columns.restype = ctypes.c_int32
         L.n3o_score_columns.argtypes = [_i32p, ctypes.c_int, ctypes.c_void_p]
         L.n3o_max_threads.restype = ctypes.c_int
+        L.n3o_three_cycles.restype = None
+        L.n3o_three_cycles.argtypes = [_i32p, _i32p, ctypes.c_int, _i32p, ctypes.c_int, ctypes.c_int64, _i64p, _i64p]
+        L.n3o_beam_mutate.restype = None
+        L.n3o_beam_mutate.argtypes = [_i32p, _i32p, _i32p] + [ctypes.c_int] * 7 + [ctypes.c_uint64, ctypes.c_int,
+                                                                                    _i32p, _i32p]
         _lib = L
     return _lib
 
@@ -182,3 +187,179 @@ def temper_run(state: dict, *, ladder_size: int, acc, exch, seed: int, rounds: i
       acc.ctypes.data, acc.shape[1], exch.ctypes.data, exch.shape[1], seed & 0xFFFFFFFFFFFFFFFF, rounds,
       round_sweeps, round_proposals, int(exchange), lr.ctypes.data if lr is not None else None, threads)
     return s
+
+
+# --------------------------------------------------------------------------
+# Device beam search (gpu_device_search.py:185-432), restated on the CPU.
+# --------------------------------------------------------------------------
+def beam_mutate(parent_p, parent_q, parent_badness, *, quality_count: int, population: int, active_strength: int,
+                max_strength: int, bad_bias: int, seed: int, generation: int):
+    """The CUDA kernel ``mutate_population`` (gpu_device_search.py:17-114)."""
+    pp, pq, pb = _c32(parent_p), _c32(parent_q), _c32(parent_badness)
+    n = pp.shape[1]
+    cp_ = np.empty((population, n), np.int32)
+    cq_ = np.empty((population, n), np.int32)
+    lib().n3o_beam_mutate(pp, pq, pb, pp.shape[0], quality_count, n, population, active_strength, max_strength,
+                          bad_bias, seed & ((1 << 64) - 1), generation, cp_, cq_)
+    return cp_, cq_
+
+
+def elite_key(score: int, badness) -> tuple[int, int, int]:
+    """gpu_device_search.py:200-203."""
+    v = np.asarray(badness, dtype=np.int64)
+    return int(score), int(v.max()), int(np.dot(v, v))
+
+
+def rank_elites(scores, badness) -> np.ndarray:
+    """gpu_device_search.py:185-197: stable sort by (score, max badness, sum of squares)."""
+    return np.asarray(sorted(range(len(scores)), key=lambda i: elite_key(scores[i], badness[i])), dtype=np.int32)
+
+
+def beam_search(initial_p, initial_q, extra=None, *, seed: int, generations: int, population: int, elite_size: int,
+                max_strength: int, energy_window: int, bad_bias: int = 85, threads: int = 0) -> dict:
+    """The generation loop of gpu_device_beam_search (gpu_device_search.py:254-432):
+    mutate, score, keep the best quarter plus a seeded random.Random shuffle of the
+    children within ``energy_window`` of the best, rank by elite_key."""
+    from random import Random
+
+    rng = Random(seed)
+    base = np.column_stack((initial_p, initial_q)).astype(np.int32)[None]
+    if extra is not None:
+        base = np.concatenate((base, np.asarray(extra, np.int32)), axis=0)
+    base = base[:elite_size]
+    ep, eq = base[:, :, 0].copy(), base[:, :, 1].copy()
+    es, eb = score_population(ep, eq, badness=True, threads=threads)
+    order = rank_elites(es, eb)
+    ep, eq, eb, es = ep[order], eq[order], eb[order], es[order]
+    best_score = int(es[0])
+    best_key = elite_key(best_score, eb[0])
+    best_p, best_q = ep[0].copy(), eq[0].copy()
+    last_improvement, completed = 0, 0
+    out = {"generation_best": [], "best_history": [], "elite_scores": [], "elite_p": [], "elite_q": []}
+    for generation in range(1, generations + 1):
+        completed = generation
+        active = min(max_strength, 2 + (generation - last_improvement) // 10)
+        qc = max(1, min(len(es), elite_size // 4))
+        cp_, cq_ = beam_mutate(ep, eq, eb, quality_count=qc, population=population, active_strength=active,
+                               max_strength=max_strength, bad_bias=bad_bias, seed=seed, generation=generation)
+        scores = score_population(cp_, cq_, threads=threads)
+        order = np.argsort(scores, kind="stable")
+        selected = list(map(int, order[:max(1, elite_size // 4)]))
+        chosen = set(selected)
+        diverse = list(map(int, np.flatnonzero(scores <= best_score + energy_window)))
+        rng.shuffle(diverse)
+        for index in diverse:
+            if index not in chosen:
+                selected.append(index)
+                chosen.add(index)
+                if len(selected) == elite_size:
+                    break
+        if len(selected) < elite_size:
+            for index in map(int, order):
+                if index not in chosen:
+                    selected.append(index)
+                    chosen.add(index)
+                    if len(selected) == elite_size:
+                        break
+        sel = np.asarray(selected, np.int64)
+        ep, eq, es = cp_[sel], cq_[sel], scores[sel]
+        _, eb = score_population(ep, eq, badness=True, threads=threads)
+        rank = rank_elites(es, eb)
+        ep, eq, eb, es = ep[rank], eq[rank], eb[rank], es[rank]
+        key = elite_key(int(es[0]), eb[0])
+        if key < best_key:
+            best_score, best_key = int(es[0]), key
+            best_p, best_q = ep[0].copy(), eq[0].copy()
+            last_improvement = generation
+        out["generation_best"].append(int(es[0]))
+        out["best_history"].append(best_score)
+        out["elite_scores"].append(es.copy())
+        out["elite_p"].append(ep.copy())
+        out["elite_q"].append(eq.copy())
+        if best_score == 0:
+            break
+    out.update(completed=completed, best_score=best_score, best_p_raw=best_p, best_q_raw=best_q,
+               evaluations=len(base) + completed * population)
+    return out
+
+
+# --------------------------------------------------------------------------
+# Multi-point moves.
+# --------------------------------------------------------------------------
+def three_cycles(p, q, candidates, score: int, badness) -> np.ndarray:
+    """accelerated.py:196-276 (candidates int32 [M, 4]: u, v, w, orientation)."""
+    p, q = _c32(p), _c32(q)
+    cand = _c32(np.asarray(candidates).reshape(-1, 4))
+    out = np.zeros(cand.shape[0], np.int64)
+    lib().n3o_three_cycles(p, q, len(p), cand, cand.shape[0], int(score),
+                           np.ascontiguousarray(badness, dtype=np.int64), out)
+    return out
+
+
+def legal_three_cycle_candidates(p, q, selected: int) -> np.ndarray:
+    """search.py:38-65: (selected, v, w, orientation) for v < w in other, distinct
+    rows with three distinct columns and no row left with a repeated column."""
+    n = len(p)
+    cols = np.empty(2 * n, np.int64)
+    cols[0::2], cols[1::2] = p, q
+    srow = selected // 2
+    out = []
+    for v in range(2 * n - 1):
+        if v // 2 == srow:
+            continue
+        for w in range(v + 1, 2 * n):
+            if w // 2 in (srow, v // 2):
+                continue
+            if len({int(cols[selected]), int(cols[v]), int(cols[w])}) != 3:
+                continue
+            ou, ov, ow = selected ^ 1, v ^ 1, w ^ 1
+            if cols[v] != cols[ou] and cols[w] != cols[ov] and cols[selected] != cols[ow]:
+                out.append((selected, v, w, 0))
+            if cols[w] != cols[ou] and cols[v] != cols[ow] and cols[selected] != cols[ov]:
+                out.append((selected, v, w, 1))
+    return np.asarray(out, np.int32).reshape(-1, 4)
+
+
+def neighborhood_scan(p, q, anchor: int, *, kind: str, threads: int = 0):
+    """gpu_neighborhood.py:70-211 restated: every four-cycle (kind "four") or
+    double switch (kind "double") through ``anchor``, enumerated in the
+    reference's order (row triples, layer choices, orderings), each scored in
+    full; returns (best score, evaluated, legal, best P, best Q) with the first
+    strictly improving minimum, the base state when nothing improves."""
+    from itertools import combinations, permutations, product
+
+    p, q = _c32(p), _c32(q)
+    n = len(p)
+    base = np.column_stack((p, q)).astype(np.int32)
+    flat = base.reshape(-1)
+    best = int(score_and_badness(p, q)[0])
+    best_values = base.copy()
+    targets, sources = [], []
+    others = [r for r in range(n) if r != anchor // 2]
+    for rows in combinations(others, 3):
+        for layers in product((0, 1), repeat=3):
+            slots = tuple(2 * r + l for r, l in zip(rows, layers))
+            if kind == "four":
+                for order in permutations(slots):
+                    t = (anchor,) + order
+                    targets.append(t)
+                    sources.append(t[1:] + t[:1])
+            else:
+                a, b, c = slots
+                for src in ((a, anchor, c, b), (b, c, anchor, a), (c, b, a, anchor)):
+                    targets.append((anchor, a, b, c))
+                    sources.append(src)
+    targets = np.asarray(targets, np.int64)
+    sources = np.asarray(sources, np.int64)
+    new_cols = flat[sources]
+    legal = np.all(new_cols != flat[targets ^ 1], axis=1)
+    lt, lc = targets[legal], new_cols[legal]
+    cand = np.broadcast_to(flat, (len(lt), flat.size)).copy()
+    cand[np.arange(len(lt))[:, None], lt] = lc
+    scores = score_population(np.ascontiguousarray(cand[:, 0::2]), np.ascontiguousarray(cand[:, 1::2]),
+                              threads=threads) if len(lt) else np.empty(0, np.int32)
+    if len(scores) and int(scores.min()) < best:
+        i = int(np.argmin(scores))
+        best = int(scores[i])
+        best_values = cand[i].reshape(n, 2)
+    return best, int(len(targets)), int(legal.sum()), best_values[:, 0].copy(), best_values[:, 1].copy()
