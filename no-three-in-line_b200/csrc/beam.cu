@@ -12,9 +12,10 @@
 // The reference does the selection and ranking on the host with a copy of
 // every child's score each generation.  Here the selection is one CTA: a radix
 // select of the elite_size-th smallest score, a bitonic sort of the scores
-// below it, ordered compactions by block scans, and the shuffle by one thread
-// on a copy of the window list in shared memory (the shuffle is a sequential
-// RNG walk and must consume exactly CPython's draws).
+// below it, ordered compactions by block scans, and the shuffle by one warp on
+// a copy of the window list in shared memory (the shuffle must consume exactly
+// CPython's draws: the warp tries 32 steps per round and keeps those before the
+// first rejected draw).
 #include <stdint.h>
 
 #include "n3_common.cuh"
@@ -125,19 +126,25 @@ __global__ void __launch_bounds__(128) mutate_kernel(const MutArgs A) {
 // --------------------------------------------------------------------------
 constexpr int kMT = 624;
 
-__device__ void mt_twist(uint32_t* mt) {
-  for (int k = 0; k < kMT; ++k) {
-    const uint32_t y = (mt[k] & 0x80000000u) | (mt[(k + 1) % kMT] & 0x7fffffffu);
-    mt[k] = mt[(k + 397) % kMT] ^ (y >> 1) ^ ((y & 1u) ? 0x9908b0dfu : 0u);
+// The state twist by one warp: ordered chunks of 32 words reproduce the
+// sequential update exactly (word k reads words k + 1 and k + 397 before they
+// are updated and word k - 227 after, as the one-thread loop does, because
+// 397 and 227 both exceed the chunk width).
+__device__ void mt_twist_warp(uint32_t* mt, int lane) {
+  for (int k0 = 0; k0 < kMT; k0 += 32) {
+    const int k = k0 + lane;
+    uint32_t nv = 0u;
+    if (k < kMT) {
+      const uint32_t y = (mt[k] & 0x80000000u) | (mt[(k + 1) % kMT] & 0x7fffffffu);
+      nv = mt[(k + 397) % kMT] ^ (y >> 1) ^ ((y & 1u) ? 0x9908b0dfu : 0u);
+    }
+    __syncwarp();
+    if (k < kMT) mt[k] = nv;
+    __syncwarp();
   }
 }
 
-__device__ __forceinline__ uint32_t mt_next(uint32_t* mt, int& idx) {
-  if (idx >= kMT) {
-    mt_twist(mt);
-    idx = 0;
-  }
-  uint32_t y = mt[idx++];
+__device__ __forceinline__ uint32_t mt_temper(uint32_t y) {
   y ^= y >> 11;
   y ^= (y << 7) & 0x9d2c5680u;
   y ^= (y << 15) & 0xefc60000u;
@@ -145,19 +152,93 @@ __device__ __forceinline__ uint32_t mt_next(uint32_t* mt, int& idx) {
   return y;
 }
 
-// random.Random.shuffle on values[0..count) (any address space).
+// random.Random.shuffle by one warp, draw for draw the same as CPython.  The
+// 624 tempered outputs of the current state block sit in `out`.  Each round
+// takes the next (up to) 32 draws at once.  Step i (descending) draws
+// r = getrandbits(k), k = bit_length(i + 1), until r <= i (_randbelow).  A
+// round covers the next m <= 32 steps that share k; a draw with r <= i - m + 1
+// is accepted and one with r > i rejected whatever the earlier lanes decide, so
+// the lanes' decisions and, by a prefix count, their steps follow at once; the
+// round stops after the first draw that needs its exact step (i - m + 1 < r <= i,
+// decided then) or at the m-th acceptance.  A round's accepted swaps (s, j) cover consecutive steps s_max .. s_min;
+// they commute when no j lies in [s_min, s_max] (other than j = s) and no two j
+// coincide (a bit per position in `seen`, zero on entry and on return, finds
+// repeats), and are then made by all lanes at once, otherwise by lane 0 in step
+// order.  idx: position in the block (warp-uniform).
 template <class T>
-__device__ void py_shuffle(uint32_t* mt, int& idx, T* values, int count) {
-  for (int i = count - 1; i >= 1; --i) {
-    const uint32_t range = (uint32_t)i + 1u;
-    const int k = 32 - __clz(range);  // bit_length(i + 1)
-    uint32_t r;
-    do {
-      r = mt_next(mt, idx) >> (32 - k);
-    } while (r >= range);
-    const T t = values[i];
-    values[i] = values[r];
-    values[r] = t;
+__device__ void py_shuffle_warp(uint32_t* mt, uint32_t* out, int& idx, T* values, int count, uint32_t* seen,
+                                int lane) {
+  for (int k = lane; k < kMT; k += 32) out[k] = mt_temper(mt[k]);
+  __syncwarp();
+  const unsigned below = (1u << lane) - 1u;
+  int i = count - 1;
+  while (i >= 1) {
+    if (idx >= kMT) {
+      mt_twist_warp(mt, lane);
+      for (int k = lane; k < kMT; k += 32) out[k] = mt_temper(mt[k]);
+      __syncwarp();
+      idx = 0;
+    }
+    const int shift = __clz((uint32_t)i + 1u);  // 32 - bit_length(i + 1)
+    // steps i .. i - m + 1 share the draw width: their ranges are >= 2^(bit_length(i + 1) - 1)
+    const int m = min(32, i + 2 - (1 << (31 - shift)));
+    const int draws = min(32, kMT - idx);
+    uint32_t r = 0u;
+    bool acc = false, amb = false;
+    if (lane < draws) {
+      r = out[idx + lane] >> shift;
+      acc = (int)r <= i - (m - 1);
+      amb = !acc && (int)r <= i;
+    }
+    const unsigned amb_mask = __ballot_sync(0xffffffffu, amb);
+    const int a = amb_mask ? __ffs(amb_mask) - 1 : draws;  // first draw that needs its exact step
+    unsigned acc_mask = __ballot_sync(0xffffffffu, acc) & ((a < 32 ? (1u << a) : 0u) - 1u);
+    int used = a;
+    if (__popc(acc_mask) < m && a < draws) {  // decide draw a with its step i - (accepted draws before it)
+      const int sa = i - __popc(acc_mask);
+      if ((int)__shfl_sync(0xffffffffu, r, a) <= sa) acc_mask |= 1u << a;
+      used = a + 1;
+    }
+    if (__popc(acc_mask) >= m) {  // the m-th acceptance ends the round (the next step draws wider or
+                                  // narrower, or there is none); later draws stay unused
+      unsigned mm = acc_mask;
+      for (int c = 1; c < m; ++c) mm &= mm - 1u;  // drop the first m - 1 set bits
+      const int z = __ffs(mm) - 1;
+      acc_mask &= z < 31 ? (2u << z) - 1u : 0xffffffffu;
+      used = z + 1;
+    }
+    const int nb = __popc(acc_mask);
+    const int s_max = i, s_min = s_max - nb + 1;
+    // an accepted draw swaps its step s = s_max - (accepted draws before it) with j = r;
+    // a j inside [s_min, s_max] (other than s) or met twice orders the swaps
+    const bool mine = (acc_mask >> lane) & 1u;
+    const int sm = s_max - __popc(acc_mask & below), jm = (int)r;
+    bool conflict = false;
+    if (mine) {
+      conflict = jm >= s_min && jm != sm;
+      const uint32_t bit = 1u << (jm & 31);
+      conflict |= (atomicOr(&seen[jm >> 5], bit) & bit) != 0u;
+    }
+    if (!__any_sync(0xffffffffu, conflict)) {
+      if (mine && jm != sm) {
+        const T t = values[sm];
+        values[sm] = values[jm];
+        values[jm] = t;
+      }
+    } else {
+      for (int l = 0; l < 32; ++l) {  // in step order: lane order of the accepted draws
+        const int sl = __shfl_sync(0xffffffffu, sm, l), jl = __shfl_sync(0xffffffffu, jm, l);
+        if (lane == 0 && ((acc_mask >> l) & 1u)) {
+          const T t = values[sl];
+          values[sl] = values[jl];
+          values[jl] = t;
+        }
+      }
+    }
+    if (mine) atomicAnd(&seen[jm >> 5], ~(1u << (jm & 31)));
+    __syncwarp();
+    i -= nb;
+    idx += used;
   }
 }
 
@@ -191,13 +272,14 @@ __global__ void py_seed_kernel(uint32_t* state, uint64_t seed) {
 }
 
 __global__ void py_shuffle_kernel(uint32_t* state, int32_t* values, int count) {
-  __shared__ uint32_t mt[kMT];
+  __shared__ uint32_t mt[kMT], out[kMT], seen[65536 / 32];
   for (int i = threadIdx.x; i < kMT; i += blockDim.x) mt[i] = state[i];
+  for (int i = threadIdx.x; i < 65536 / 32; i += blockDim.x) seen[i] = 0u;
   __syncthreads();
-  if (threadIdx.x == 0) {
+  if (threadIdx.x < 32) {
     int idx = (int)state[kMT];
-    py_shuffle(mt, idx, values, count);
-    state[kMT] = (uint32_t)idx;
+    py_shuffle_warp(mt, out, idx, values, count, seen, threadIdx.x);
+    if (threadIdx.x == 0) state[kMT] = (uint32_t)idx;
   }
   __syncthreads();
   for (int i = threadIdx.x; i < kMT; i += blockDim.x) state[i] = mt[i];
@@ -257,6 +339,7 @@ __global__ void __launch_bounds__(kSelThreads, 1) select_kernel(const SelArgs A)
   __shared__ uint32_t hist[256];
   __shared__ int warp_tot[32];
   __shared__ int s_misc[4];
+  __shared__ uint32_t mt_out[kMT];  // tempered outputs of the current state block
   if (A.status[1] == 0) return;  // uniform: the search has reached E = 0
   const int64_t limit = A.status[1] + (int64_t)A.energy_window;
   for (int i = tid; i < kMaxPopulation / 32; i += kSelThreads) mark[i] = 0u;
@@ -270,9 +353,16 @@ __global__ void __launch_bounds__(kSelThreads, 1) select_kernel(const SelArgs A)
   for (int shift = 24; shift >= 0; shift -= 8) {
     for (int i = tid; i < 256; i += kSelThreads) hist[i] = 0u;
     __syncthreads();
-    for (int i = lo; i < hi; ++i) {
-      const uint32_t x = (uint32_t)A.scores[i];
-      if ((x & mask) == prefix) atomicAdd(&hist[(x >> shift) & 255u], 1u);
+    for (int b = 0; b < chunk; ++b) {  // warp-uniform trip count; equal digits add once per warp
+      const int i = lo + b;
+      const uint32_t x = i < hi ? (uint32_t)A.scores[i] : 0u;
+      const bool valid = i < hi && (x & mask) == prefix;
+      const unsigned act = __ballot_sync(0xffffffffu, valid);
+      if (valid) {
+        const uint32_t digit = (x >> shift) & 255u;
+        const unsigned peers = __match_any_sync(act, digit);
+        if ((threadIdx.x & 31) == __ffs(peers) - 1) atomicAdd(&hist[digit], (uint32_t)__popc(peers));
+      }
     }
     __syncthreads();
     if (tid == 0) {
@@ -345,11 +435,13 @@ __global__ void __launch_bounds__(kSelThreads, 1) select_kernel(const SelArgs A)
   }
   __syncthreads();
 
-  // 4. one thread: the shuffle and the pick (gpu_device_search.py:340-373)
-  if (tid == 0) {
+  // 4. warp 0: the shuffle; thread 0: the pick (gpu_device_search.py:340-373)
+  if (tid < 32) {
     int idx = (int)A.rng[kMT];
-    py_shuffle(mt, idx, window, n_window);
-    A.rng[kMT] = (uint32_t)idx;
+    py_shuffle_warp(mt, mt_out, idx, window, n_window, mark, tid);  // mark: all zero here
+    if (tid == 0) A.rng[kMT] = (uint32_t)idx;
+  }
+  if (tid == 0) {
     int sel = 0;
     const int quality_keep = max(1, E / 4);
     for (int r = 0; r < quality_keep; ++r) {
