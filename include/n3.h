@@ -288,6 +288,29 @@ int n3_neighborhood_scan(const int32_t* p, const int32_t* q, int n, int anchor, 
                          unsigned long long* best, unsigned long long* legal, void* stream);
 
 /* ---------------------------------------------------------------------------
+ * Line-weighted energies of breakout search (src/no_three_75/breakout.py:39-86):
+ * a line (a, b, c), the points with a*row + b*col + c == 0, of weight w > 1
+ * adds (w - 1) * C(occupancy, 3) to E; weights <= 1 add nothing.
+ * lines int32 [n_lines][3], weights int32 [n_lines] (n_lines <= 4096).
+ * ------------------------------------------------------------------------- */
+
+/* weighted_candidate_scores (breakout.py:39-75): for the selected slot u and each
+ * partner slot v, scores[v] = raw[v] + the weighted extra of the state after
+ * u and v exchange columns (u to (row u, column v), v to (row v, column u)),
+ * occupancies counted as the reference counts them.  raw, scores int64 [2n]
+ * (raw as evaluate_two_switches returns it, sentinels included). */
+int n3_weighted_switch_scores(const int32_t* p, const int32_t* q, int n, int u, const int64_t* raw,
+                              const int32_t* lines, const int32_t* weights, int n_lines, int64_t* scores,
+                              void* stream);
+
+/* weighted_state_score (breakout.py:78-86) over a population: scores[b] =
+ * raw[b] + sum over weighted lines of (w - 1) C(occupancy, 3).
+ * p, q int32 [B][n]; raw, scores int64 [B]. */
+int n3_weighted_state_scores(const int32_t* p, const int32_t* q, int B, int n, const int64_t* raw,
+                             const int32_t* lines, const int32_t* weights, int n_lines, int64_t* scores,
+                             void* stream);
+
+/* ---------------------------------------------------------------------------
  * Device-resident beam search: the generation loop of
  * src/no_three_75/gpu_device_search.py:254-432 (gpu_device_beam_search) with
  * mutation, scoring, selection (including its random.Random shuffle) and

@@ -363,3 +363,47 @@ def neighborhood_scan(p, q, anchor: int, *, kind: str, threads: int = 0):
         best = int(scores[i])
         best_values = cand[i].reshape(n, 2)
     return best, int(len(targets)), int(legal.sum()), best_values[:, 0].copy(), best_values[:, 1].copy()
+
+
+# --------------------------------------------------------------------------
+# Line weights of breakout search (breakout.py:39-86), restated with NumPy.
+# --------------------------------------------------------------------------
+def _c3(k):
+    k = np.asarray(k, np.int64)
+    return np.where(k >= 3, k * (k - 1) * (k - 2) // 6, 0)
+
+
+def weighted_switch_scores(p, q, u: int, raw, keys, vals) -> np.ndarray:
+    """breakout.py:39-75 with weights as parallel arrays (keys [L, 3], vals [L])."""
+    p, q = np.asarray(p, np.int64), np.asarray(q, np.int64)
+    n = len(p)
+    rows = np.repeat(np.arange(n, dtype=np.int64), 2)
+    cols = np.empty(2 * n, np.int64)
+    cols[0::2], cols[1::2] = p, q
+    out = np.asarray(raw, np.int64).copy()
+    keys = np.asarray(keys, np.int64).reshape(-1, 3)
+    vals = np.asarray(vals, np.int64)
+    for (a, b, c), w in zip(keys, vals):
+        if w <= 1:
+            continue
+        member = a * rows + b * cols + c == 0
+        occ = int(member.sum())
+        new_u = a * rows[u] + b * cols + c == 0          # u to (row u, column v)
+        new_v = a * rows + b * cols[u] + c == 0          # v to (row v, column u)
+        k = occ - int(member[u]) - member.astype(np.int64) + new_u + new_v
+        out += (w - 1) * _c3(k)
+    return out
+
+
+def weighted_state_score(p, q, raw_score: int, keys, vals) -> int:
+    """breakout.py:78-86."""
+    p, q = np.asarray(p, np.int64), np.asarray(q, np.int64)
+    n = len(p)
+    rows = np.concatenate([np.arange(n), np.arange(n)])
+    cols = np.concatenate([p, q])
+    value = int(raw_score)
+    for (a, b, c), w in zip(np.asarray(keys, np.int64).reshape(-1, 3), np.asarray(vals, np.int64)):
+        if w <= 1:
+            continue
+        value += int((w - 1) * _c3(int(np.count_nonzero(a * rows + b * cols + c == 0))))
+    return value
