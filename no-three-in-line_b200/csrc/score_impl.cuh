@@ -133,4 +133,46 @@ __device__ __forceinline__ int slope_state(const int* __restrict__ cs, int n, co
   return total;
 }
 
+// Forward slope count of one state: for each anchor a, only the slots b > a are
+// binned by direction.  On a line holding slots p1 < .. < pk, anchor p_i sees the
+// k - i later ones, C(k - i, 2) pairs, and the sum over i is C(k, 3): the sum over
+// anchors is E itself, from half the insertions of slope_state (no per-slot
+// badness).  Returns this lane's share; hist is left zeroed.
+__device__ __forceinline__ int slope_forward_state(const int* __restrict__ cs, int n,
+                                                   const uint16_t* __restrict__ lutf,
+                                                   uint32_t* __restrict__ hist, int lane) {
+  constexpr int kT = (kMaxM + 31) / 32;
+  const int m = 2 * n;
+  int key[kT], row[kT];
+#pragma unroll
+  for (int t = 0; t < kT; ++t) {
+    const int b = lane + 32 * t;
+    row[t] = b < m ? b >> 1 : -1;
+    key[t] = b < m ? (b >> 1) * kLutW + cs[b] : 0;
+  }
+  int pairs = 0;
+  for (int a = 0; a < m - 2; ++a) {
+    const int ra = a >> 1;
+    const uint16_t* base = lutf + kFullLutCentre - (ra * kLutW + cs[a]);
+    int ids[kT];
+#pragma unroll
+    for (int t = 0; t < kT; ++t) {
+      ids[t] = -1;
+      if (32 * t + 31 <= a) continue;  // warp-uniform: every slot of this group precedes a
+      const int b = lane + 32 * t;
+      if (b > a && row[t] >= 0 && row[t] != ra) {
+        const int id = base[key[t]];
+        ids[t] = id;
+        pairs += hist_add(hist, id);
+      }
+    }
+    __syncwarp();
+#pragma unroll
+    for (int t = 0; t < kT; ++t)
+      if (ids[t] >= 0) hist_clear(hist, ids[t]);
+    __syncwarp();
+  }
+  return pairs;
+}
+
 }  // namespace n3

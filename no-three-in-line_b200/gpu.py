@@ -102,10 +102,12 @@ class CheckedScores:
     error_word: int     # device error bits (1 column range, 2 duplicate point, 4 mismatch)
 
 
-def score_checked_gpu(columns, *, stream=None, raise_on_mismatch: bool = True) -> CheckedScores:
+def score_checked_gpu(columns, *, stream=None, raise_on_mismatch: bool = True, badness: bool = True) -> CheckedScores:
     """Fused determinant + slope scoring with the on-device cross-check.
     Raises AssertionError on any disagreement (the reference's exact_match
-    audit, src/no_three_75/gpu.py:131, made fatal) unless told not to."""
+    audit, src/no_three_75/gpu.py:131, made fatal) unless told not to.  With
+    ``badness=False`` the slope side counts E alone (each triple once from its
+    first slot) and ``badness`` of the result is None."""
     t = _lib.torch()
     device = _lib.require_device()
     host = not _lib.is_tensor(columns)
@@ -113,7 +115,7 @@ def score_checked_gpu(columns, *, stream=None, raise_on_mismatch: bool = True) -
     B, n = int(c.shape[0]), int(c.shape[1]) // 2
     _check_n(n)
     scores = t.empty(B, dtype=t.int32, device=device)
-    bad = t.empty((B, 2 * n), dtype=t.int32, device=device)
+    bad = t.empty((B, 2 * n), dtype=t.int32, device=device) if badness else None
     flags = t.zeros(2, dtype=t.int32, device=device)
     _lib.call("n3_score_checked", _lib.ptr(c), B, n, _lib.ptr(scores), _lib.ptr(bad), flags.data_ptr(),
               flags.data_ptr() + 4, _lib.stream_ptr(stream))
@@ -122,7 +124,7 @@ def score_checked_gpu(columns, *, stream=None, raise_on_mismatch: bool = True) -
     if raise_on_mismatch and (mism or err):
         raise AssertionError(f"checked scoring: {mism} state(s) disagree, device error bits {err:#x}")
     if host:
-        return CheckedScores(scores.cpu().numpy(), bad.cpu().numpy(), mism, err)
+        return CheckedScores(scores.cpu().numpy(), bad.cpu().numpy() if badness else None, mism, err)
     return CheckedScores(scores, bad, mism, err)
 
 

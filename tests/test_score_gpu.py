@@ -63,6 +63,8 @@ def test_every_size_matches_oracle(n, oracle, cuda):
     assert np.array_equal(s2, ref_s) and np.array_equal(b2, ref_b)
     chk = gpu.score_checked_gpu(cols)
     assert np.array_equal(chk.scores, ref_s) and chk.mismatches == 0
+    fwd = gpu.score_checked_gpu(cols, badness=False)  # forward slope count of E
+    assert np.array_equal(fwd.scores, ref_s) and fwd.mismatches == 0 and fwd.badness is None
 
 
 def test_degenerate_dense_collinear_states(oracle, cuda):
@@ -75,6 +77,8 @@ def test_degenerate_dense_collinear_states(oracle, cuda):
     assert np.array_equal(s, ref_s) and np.array_equal(b, ref_b)
     chk = gpu.score_checked_gpu(state.pq_to_columns(p, q))
     assert np.array_equal(chk.scores, ref_s) and np.array_equal(chk.badness, ref_b) and chk.mismatches == 0
+    fwd = gpu.score_checked_gpu(state.pq_to_columns(p, q), badness=False)
+    assert np.array_equal(fwd.scores, ref_s) and fwd.mismatches == 0
 
 
 def test_empty_batch_and_shape_errors(cuda):
@@ -93,9 +97,10 @@ def test_checked_scoring_flags_invalid_states(cuda):
     cols = state.pq_to_columns(p, q)
     cols[1, 7] = 25          # column outside [0, 20)
     cols[2, 9] = cols[2, 8]  # duplicate point in row 4
-    chk = gpu.score_checked_gpu(cols, raise_on_mismatch=False)
-    assert chk.error_word & 1 and chk.error_word & 2
-    assert chk.mismatches == 2 and chk.scores[1] == -1 and chk.scores[2] == -1
+    for badness in (True, False):
+        chk = gpu.score_checked_gpu(cols, raise_on_mismatch=False, badness=badness)
+        assert chk.error_word & 1 and chk.error_word & 2
+        assert chk.mismatches == 2 and chk.scores[1] == -1 and chk.scores[2] == -1
     with pytest.raises(AssertionError):
         gpu.score_checked_gpu(cols)
 
