@@ -77,12 +77,12 @@ constexpr int kFullLutSize = kLutW * kLutW;  // 22,201 entries
 constexpr size_t kFullLutBytes = ((sizeof(uint16_t) * kFullLutSize + 15) / 16) * 16;
 constexpr int kFullLutCentre = (kMaxN - 1) * kLutW + (kMaxN - 1);
 
-// Fills the full table from the compact (dx >= 0) one; all threads of the block call it.
-__device__ __forceinline__ void full_lut_fill(uint16_t* __restrict__ dst, const uint16_t* __restrict__ half) {
-  for (int e = threadIdx.x; e < kFullLutSize; e += blockDim.x) {
-    const int dx = e / kLutW - (kMaxN - 1), dy = e % kLutW - (kMaxN - 1);
-    dst[e] = (dx == 0 && dy == 0) ? (uint16_t)0 : (uint16_t)dir_id(half, dx, dy);
-  }
+// Copies the full table built once per device (n3host::dir_lut_full_device_ptr)
+// into shared memory, 16 bytes at a time; all threads of the block call it.
+__device__ __forceinline__ void full_lut_copy(uint16_t* __restrict__ dst, const uint16_t* __restrict__ full) {
+  const uint4* s = reinterpret_cast<const uint4*>(full);
+  uint4* d = reinterpret_cast<uint4*>(dst);
+  for (int i = threadIdx.x; i < (int)(kFullLutBytes / 16); i += blockDim.x) d[i] = s[i];
 }
 
 __device__ __forceinline__ int dir_id_full(const uint16_t* __restrict__ lutf, int dx, int dy) {
@@ -126,4 +126,6 @@ namespace n3host {
 // Device address of the direction table on the current device (set-up on
 // first use by ensure_device_tables).
 const uint16_t* dir_lut_device_ptr();
+// Device address of the full signed table built from it (kFullLutBytes).
+const uint16_t* dir_lut_full_device_ptr();
 }  // namespace n3host

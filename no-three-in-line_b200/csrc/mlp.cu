@@ -535,8 +535,9 @@ __global__ void __launch_bounds__(kStepWarps * 32, 1) learned_step_kernel(const 
   uint32_t* hist_all = reinterpret_cast<uint32_t*>(smem + kFullLutBytes);
   int* cs_all = reinterpret_cast<int*>(hist_all + kStepWarps * kDirWords);
   int* bs_all = cs_all + kStepWarps * kMaxM;
-  full_lut_fill(lut, A.lut);
-  for (int i = threadIdx.x; i < kStepWarps * kDirWords; i += blockDim.x) hist_all[i] = 0u;
+  full_lut_copy(lut, A.lut);
+  for (int i = threadIdx.x; i < kStepWarps * kDirWords / 4; i += blockDim.x)
+    reinterpret_cast<uint4*>(hist_all)[i] = make_uint4(0u, 0u, 0u, 0u);
   __syncthreads();
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int c = blockIdx.x * kStepWarps + warp;
@@ -554,93 +555,102 @@ __global__ void __launch_bounds__(kStepWarps * 32, 1) learned_step_kernel(const 
   const float T = A.temps[temp];
   // softmax(-pred / T) over the legal candidates, sampled by inverse CDF;
   // with moves > 1 the step draws again without replacement after each move
-  // (candidates are re-checked for legality on the current state).
-  float w[kCand / 32];
+  // (candidates are re-checked for legality on the current state).  Lane l
+  // holds candidates 4l .. 4l + 3 (weights, codes and predictions in registers),
+  // so a draw needs one warp scan of the lane totals.
+  constexpr int kPer = kCand / 32;
+  static_assert(kPer == 4, "four candidates per lane");
+  const int4 cw4 = reinterpret_cast<const int4*>(A.cand + (size_t)c * kCand)[lane];
+  const float4 pr4 = reinterpret_cast<const float4*>(A.pred + (size_t)c * kCand)[lane];
+  const int cwv[kPer] = {cw4.x, cw4.y, cw4.z, cw4.w};
+  const float prv[kPer] = {pr4.x, pr4.y, pr4.z, pr4.w};
+  float w[kPer];
   float mx = -INFINITY;
 #pragma unroll
-  for (int q = 0; q < kCand / 32; ++q) {
-    const int j = lane + 32 * q;
-    const int cw = A.cand[(size_t)c * kCand + j];
-    w[q] = cw < 0 ? -A.pred[(size_t)c * kCand + j] / T : -INFINITY;
+  for (int q = 0; q < kPer; ++q) {
+    w[q] = cwv[q] < 0 ? -prv[q] / T : -INFINITY;
     mx = fmaxf(mx, w[q]);
   }
 #pragma unroll
   for (int o = 16; o; o >>= 1) mx = fmaxf(mx, __shfl_xor_sync(0xffffffffu, mx, o));
 #pragma unroll
-  for (int q = 0; q < kCand / 32; ++q) w[q] = w[q] > -INFINITY ? __expf(w[q] - mx) : 0.f;
+  for (int q = 0; q < kPer; ++q) w[q] = w[q] > -INFINITY ? __expf(w[q] - mx) : 0.f;
   const uint64_t step = *A.step;
   const uint32_t* thr = ch.acc_thresh + (size_t)temp * ch.acc_width;
   int E = ch.energy[c];
   int bestE = ch.best_energy[c];
-  uint32_t err = 0;
+  uint32_t err = 0, n_acc = 0;
   float st_abs = 0.f, st_n = 0.f, st_acc = 0.f, st_dE = 0.f;  // this chain's statistics (lane-uniform)
   for (int k = 0; k < A.moves; ++k) {
     const U4 r = philox4x32_10(U4{(uint32_t)step, (uint32_t)(step >> 32), (uint32_t)c,
                                   kTagCandidate | 0xFF00u | (uint32_t)k}, A.k0, A.k1);
-    // inclusive prefix sums of the weights, candidate order j = lane + 32 q (by q, then lane)
-    float laneq[kCand / 32], qtot[kCand / 32], acc_w = 0.f;
+    // inclusive prefix of the weights in candidate order: within the lane, then across lanes
+    float pre[kPer];
+    pre[0] = w[0];
 #pragma unroll
-    for (int q = 0; q < kCand / 32; ++q) {
-      float x = w[q];
+    for (int q = 1; q < kPer; ++q) pre[q] = pre[q - 1] + w[q];
+    float incl = pre[kPer - 1];
 #pragma unroll
-      for (int o = 1; o < 32; o <<= 1) {
-        const float y = __shfl_up_sync(0xffffffffu, x, o);
-        if (lane >= o) x += y;
-      }
-      laneq[q] = x;
-      qtot[q] = __shfl_sync(0xffffffffu, x, 31);
-      acc_w += qtot[q];
+    for (int o = 1; o < 32; o <<= 1) {
+      const float y = __shfl_up_sync(0xffffffffu, incl, o);
+      if (lane >= o) incl += y;
     }
+    const float acc_w = __shfl_sync(0xffffffffu, incl, 31);
     if (!(acc_w > 0.f)) break;  // no legal candidate left
+    const float base = incl - pre[kPer - 1];
     const float target = ((float)(r.x >> 8) + 0.5f) * (1.0f / 16777216.0f) * acc_w;
-    float before = 0.f;
-    int pick = -1;
+    int q_hit = -1;
 #pragma unroll
-    for (int q = 0; q < kCand / 32; ++q) {
-      if (pick < 0 && target < before + qtot[q]) {
-        const unsigned hit = __ballot_sync(0xffffffffu, w[q] > 0.f && before + laneq[q] > target);
-        if (hit) pick = 32 * q + (__ffs(hit) - 1);
-      }
-      before += qtot[q];
-    }
-    if (pick < 0) {  // rounding at the top end: the last candidate with weight
+    for (int q = kPer - 1; q >= 0; --q)
+      if (w[q] > 0.f && base + pre[q] > target) q_hit = q;  // the first such q
+    unsigned hit = __ballot_sync(0xffffffffu, q_hit >= 0);
+    int owner, q_pick;
+    if (hit) {
+      owner = __ffs(hit) - 1;
+      q_pick = __shfl_sync(0xffffffffu, q_hit, owner);
+    } else {  // rounding at the top end: the last candidate with weight
+      int q_last = -1;
 #pragma unroll
-      for (int q = 0; q < kCand / 32; ++q) {
-        const unsigned hit = __ballot_sync(0xffffffffu, w[q] > 0.f);
-        if (hit) pick = 32 * q + (31 - __clz(hit));
-      }
+      for (int q = 0; q < kPer; ++q)
+        if (w[q] > 0.f) q_last = q;
+      hit = __ballot_sync(0xffffffffu, q_last >= 0);
+      owner = 31 - __clz(hit);
+      q_pick = __shfl_sync(0xffffffffu, q_last, owner);
     }
-    if (lane == (pick & 31)) w[pick >> 5] = 0.f;  // without replacement
-    __syncwarp();
-    const int cw = A.cand[(size_t)c * kCand + pick];
+    int cw_mine = cwv[0];
+    float p_mine = prv[0];
+#pragma unroll
+    for (int q = 1; q < kPer; ++q)
+      if (q == q_pick) {
+        cw_mine = cwv[q];
+        p_mine = prv[q];
+      }
+    const int cw = __shfl_sync(0xffffffffu, cw_mine, owner);
+    const float p = __shfl_sync(0xffffffffu, p_mine, owner);
+    if (lane == owner) {  // without replacement
+#pragma unroll
+      for (int q = 0; q < kPer; ++q)
+        if (q == q_pick) w[q] = 0.f;
+    }
     const int u = cw & 0xFF, v = (cw >> 8) & 0xFF;
     if (k > 0 && !legal_swap(cs, u, v)) continue;  // an earlier move of this step made it illegal
-    const float p = A.pred[(size_t)c * kCand + pick];
-    // tuple: features of the state before the move
+    // tuple: features of the state before the move (lane i writes feature i)
     const uint64_t tuple = (step * (uint64_t)ch.n_chains + (uint64_t)c) * (uint64_t)A.moves + (uint64_t)k;
     const int64_t slot = (int64_t)(tuple % (uint64_t)A.rb_cap);
-    if (lane == 0) {
-      float f[kCandFeat];
-      const int sidx[4] = {u, v, u ^ 1, v ^ 1};
-      const float inv_n = 1.0f / (float)n;
-#pragma unroll
-      for (int i = 0; i < 4; ++i) {
-        f[i] = (float)bs[sidx[i]] * (1.0f / 16.0f);
-        f[4 + i] = (float)(sidx[i] >> 1) * inv_n;
-        f[8 + i] = (float)cs[sidx[i]] * inv_n;
-      }
-#pragma unroll
-      for (int i = 0; i < kCandFeat; ++i) A.rb_feat[slot * kCandFeat + i] = bf16_bits(f[i]);
+    if (lane < kCandFeat) {
+      const int which = lane & 3;
+      const int sidx = which == 0 ? u : which == 1 ? v : which == 2 ? (u ^ 1) : (v ^ 1);
+      const float f = lane < 4 ? (float)bs[sidx] * (1.0f / 16.0f)
+                               : (float)(lane < 8 ? (sidx >> 1) : cs[sidx]) * (1.0f / (float)n);
+      A.rb_feat[slot * kCandFeat + lane] = bf16_bits(f);
     }
     for (int s = lane; s < kChainFeat; s += 32)
       A.rb_bad[slot * kChainFeat + s] = (uint8_t)(s < m ? min(bs[s], 255) : 0);
     __syncwarp();
     int dE = 0;
     const int acc = move_exact(cs, bs, m, lut, hist, lane, u, v, r.y, thr, ch.acc_width, E, err, &dE);
-    if (lane == 0) {
-      A.rb_dE[slot] = (int16_t)max(-32768, min(32767, dE));
-      if (acc) ch.accepted[c] += 1;
-    }
+    if (lane == 0) A.rb_dE[slot] = (int16_t)max(-32768, min(32767, dE));
+    n_acc += acc ? 1u : 0u;
     st_abs += fabsf(p - (float)dE);
     st_n += 1.0f;
     if (acc) {
@@ -659,6 +669,7 @@ __global__ void __launch_bounds__(kStepWarps * 32, 1) learned_step_kernel(const 
   if (lane == 0) {
     ch.energy[c] = E;
     ch.best_energy[c] = bestE;
+    ch.accepted[c] += n_acc;
     if (err && ch.error_word) atomicOr(ch.error_word, err);
     if (ch.global_best) atomicMin(ch.global_best, E);
     // one set of statistics atomics per chain and step, not per move
@@ -962,7 +973,7 @@ int n3_mlp_step(const n3_chains* ch, const n3_mlp* M, const float* temps, uint64
   N3_TRY(n3host::allow_smem(reinterpret_cast<const void*>(learned_step_kernel), smem));
   StepArgs A;
   A.ch = *ch;
-  A.lut = n3host::dir_lut_device_ptr();
+  A.lut = n3host::dir_lut_full_device_ptr();
   A.temps = temps;
   A.cand = M->cand;
   A.pred = M->pred;

@@ -98,7 +98,7 @@ __global__ void __launch_bounds__(kWarps * 32) three_cycle_kernel(const int32_t*
   uint16_t* lutf = reinterpret_cast<uint16_t*>(smem);
   uint32_t* hist_all = reinterpret_cast<uint32_t*>(smem + kFullLutBytes);
   int* cs = reinterpret_cast<int*>(hist_all + kWarps * kDirWords);
-  full_lut_fill(lutf, g_lut);
+  full_lut_copy(lutf, g_lut);
   for (int i = threadIdx.x; i < kWarps * kDirWords; i += blockDim.x) hist_all[i] = 0u;
   const int m = 2 * n;
   for (int s = threadIdx.x; s < m; s += blockDim.x) cs[s] = (s & 1) ? q[s >> 1] : p[s >> 1];
@@ -177,7 +177,7 @@ __global__ void __launch_bounds__(kWarps * 32) scan_kernel(const ScanArgs A) {
   int* cs = reinterpret_cast<int*>(hist_all + kWarps * kDirWords);
   __shared__ int jt_all[kWarps][12][12];  // points of A on the line between two candidate positions
   __shared__ int tn_all[kWarps][12];      // t_A of each candidate position
-  full_lut_fill(lutf, A.lut);
+  full_lut_copy(lutf, A.lut);
   for (int i = threadIdx.x; i < kWarps * kDirWords; i += blockDim.x) hist_all[i] = 0u;
   const int n = A.n, m = 2 * n;
   for (int s = threadIdx.x; s < m; s += blockDim.x) cs[s] = (s & 1) ? A.q[s >> 1] : A.p[s >> 1];
@@ -281,7 +281,7 @@ int n3_three_cycle_scores(const int32_t* p, const int32_t* q, int n, const int32
   const int want = (count + n3::multi::kWarps - 1) / n3::multi::kWarps;
   const int grid = want < 2 * n3host::sm_count() ? want : 2 * n3host::sm_count();
   n3::multi::three_cycle_kernel<<<grid, n3::multi::kWarps * 32, n3::multi::kSmem, (cudaStream_t)stream>>>(
-      p, q, n, candidates, count, current, n3host::dir_lut_device_ptr(), scores);
+      p, q, n, candidates, count, current, n3host::dir_lut_full_device_ptr(), scores);
   return n3host::check_launch("three_cycle_kernel");
 }
 
@@ -304,7 +304,7 @@ int n3_neighborhood_scan(const int32_t* p, const int32_t* q, int n, int anchor, 
   A.anchor = anchor;
   A.base = current;
   A.combos = (n - 1) * (n - 2) * (n - 3) / 6;
-  A.lut = n3host::dir_lut_device_ptr();
+  A.lut = n3host::dir_lut_full_device_ptr();
   A.best = best;
   A.legal = legal;
   const int warps = A.combos * 8;

@@ -28,6 +28,7 @@
 namespace n3 {
 
 __device__ uint16_t g_dir_lut[kLutSize];
+__device__ __align__(16) uint16_t g_dir_lut_full[kFullLutBytes / 2];
 __device__ int g_dir_count;
 
 __device__ __forceinline__ int gcd_dev(int a, int b) {
@@ -81,6 +82,14 @@ __global__ void __launch_bounds__(1024) build_dir_lut_kernel() {
     }
     g_dir_lut[e] = v;
   }
+}
+
+// The full signed table from the compact one (one entry per thread).
+__global__ void build_full_lut_kernel() {
+  const int e = blockIdx.x * blockDim.x + threadIdx.x;
+  if (e >= kFullLutSize) return;
+  const int dx = e / kLutW - (kMaxN - 1), dy = e % kLutW - (kMaxN - 1);
+  g_dir_lut_full[e] = (dx == 0 && dy == 0) ? (uint16_t)0 : (uint16_t)dir_id(g_dir_lut, dx, dy);
 }
 
 struct PQSource {
@@ -161,7 +170,7 @@ __global__ void __launch_bounds__(kSlopeWarps * 32) slope_kernel(ColSource src, 
   uint32_t* hist_all = reinterpret_cast<uint32_t*>(smem + kFullLutBytes);
   int* cs_all = reinterpret_cast<int*>(hist_all + kDirWords * kSlopeWarps);
   int* bad_all = cs_all + kMaxM * kSlopeWarps;
-  full_lut_fill(lut, g_dir_lut);
+  full_lut_copy(lut, g_dir_lut_full);
   for (int i = threadIdx.x; i < kDirWords * kSlopeWarps; i += blockDim.x) hist_all[i] = 0u;
   __syncthreads();
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -228,6 +237,8 @@ namespace n3host {
 int build_dir_lut(cudaStream_t st) {
   n3::build_dir_lut_kernel<<<1, 1024, 0, st>>>();
   N3_TRY(check_launch("build_dir_lut_kernel"));
+  n3::build_full_lut_kernel<<<(n3::kFullLutSize + 255) / 256, 256, 0, st>>>();
+  N3_TRY(check_launch("build_full_lut_kernel"));
   int count = 0;
   if (cudaMemcpyFromSymbolAsync(&count, n3::g_dir_count, sizeof(int), 0, cudaMemcpyDeviceToHost, st) != cudaSuccess ||
       cudaStreamSynchronize(st) != cudaSuccess)
@@ -240,6 +251,12 @@ int build_dir_lut(cudaStream_t st) {
 const uint16_t* dir_lut_device_ptr() {
   void* p = nullptr;
   if (cudaGetSymbolAddress(&p, n3::g_dir_lut) != cudaSuccess) return nullptr;
+  return static_cast<const uint16_t*>(p);
+}
+
+const uint16_t* dir_lut_full_device_ptr() {
+  void* p = nullptr;
+  if (cudaGetSymbolAddress(&p, n3::g_dir_lut_full) != cudaSuccess) return nullptr;
   return static_cast<const uint16_t*>(p);
 }
 

@@ -38,7 +38,7 @@ namespace n3 {
 struct TemperArgs {
   n3_chains ch;
   n3_temper_config cfg;
-  const uint16_t* lut;  // direction table (device)
+  const uint16_t* lut;  // full signed direction table (device)
   int cluster;          // CTAs per ladder (1: whole ladders per CTA)
 };
 
@@ -121,7 +121,7 @@ __global__ void __launch_bounds__(512, 1) temper_kernel(const TemperArgs A) {
   int* bs = bs_all + warp * kMaxM;
   uint32_t* hist = hist_all + (size_t)warp * kDirWords;
 
-  full_lut_fill(lut, A.lut);
+  full_lut_copy(lut, A.lut);
   for (int i = threadIdx.x; i < cpb * kDirWords; i += blockDim.x) hist_all[i] = 0u;
   for (int s = lane; s < m; s += 32) {
     cs[s] = ch.cols[(size_t)c * kMaxM + s];
@@ -235,7 +235,7 @@ __global__ void __launch_bounds__(kAuditWarps * 32) audit_kernel(const n3_chains
   uint32_t* hist_all = reinterpret_cast<uint32_t*>(smem + kFullLutBytes);
   int* cs_all = reinterpret_cast<int*>(hist_all + kAuditWarps * kDirWords);
   int* bs_all = cs_all + kAuditWarps * kMaxM;
-  full_lut_fill(lut, g_lut);
+  full_lut_copy(lut, g_lut);
   for (int i = threadIdx.x; i < kAuditWarps * kDirWords; i += blockDim.x) hist_all[i] = 0u;
   __syncthreads();
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -299,7 +299,7 @@ int temper_launch(const n3_chains* ch, const n3_temper_config* cfg, cudaStream_t
   N3_TRY(ensure_device_tables());
   n3::TemperArgs args;
   args.ch = *ch;
-  args.lut = dir_lut_device_ptr();
+  args.lut = dir_lut_full_device_ptr();
   args.cfg = *cfg;
   args.cluster = cluster;
   const size_t smem = n3::TemperSmem::bytes(cpb);
@@ -345,7 +345,7 @@ int n3_temper_audit(const n3_chains* chains, int32_t* mismatch, void* stream) {
   N3_TRY(n3host::allow_smem(reinterpret_cast<const void*>(n3::audit_kernel), smem));
   const int want = (ch.n_chains + n3::kAuditWarps - 1) / n3::kAuditWarps;
   const int grid = want < n3host::sm_count() * 4 ? want : n3host::sm_count() * 4;
-  n3::audit_kernel<<<grid, n3::kAuditWarps * 32, smem, (cudaStream_t)stream>>>(ch, n3host::dir_lut_device_ptr(),
+  n3::audit_kernel<<<grid, n3::kAuditWarps * 32, smem, (cudaStream_t)stream>>>(ch, n3host::dir_lut_full_device_ptr(),
                                                                                  mismatch);
   return n3host::check_launch("audit_kernel");
 }
