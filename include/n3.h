@@ -365,6 +365,11 @@ typedef struct n3_beam {
   int32_t* best_q;          /* [n] */
   int32_t* history;         /* [history_len][2] per generation: its best E, best E so far (or NULL) */
   int history_len;
+  int32_t* child_parent;    /* [population] the elite each child copies */
+  int32_t* child_moves;     /* [population][max_strength] its swaps, u | v << 8, in order */
+  int32_t* child_nmoves;    /* [population] how many */
+  int32_t* child_badness;   /* [population][2n] badness of each child */
+  uint32_t* error_word;     /* device error bits (16: a maintained badness failed its re-check), or NULL */
 } n3_beam;
 
 /* Set-up: elite rows [0, base_count) hold the initial state and any supplied
@@ -372,7 +377,9 @@ typedef struct n3_beam {
  * and seeds the shuffle RNG with the search seed (gpu_device_search.py:279-313). */
 int n3_beam_init(const n3_beam* beam, int base_count, void* stream);
 /* One generation (gpu_device_search.py:315-411): mutate the elites into
- * population children, score them, keep the best quarter plus a shuffled pick
+ * population children, score them (each child's E and badness from its parent's
+ * by the exact delta of each of its swaps, the reference rescoring every child
+ * in full), keep the best quarter plus a shuffled pick
  * of the children within energy_window of the best, fill from the score order,
  * rank by (E, max badness, sum of squared badness) and update the best.  Does
  * nothing once a generation has reached E = 0.  population <= 65536,

@@ -1,12 +1,14 @@
 // Device-resident beam search: the generation loop of
 // src/no_three_75/gpu_device_search.py:254-432 (gpu_device_beam_search) on the
 // GPU.  Per generation, five launches on one stream and no host round trip:
-//   mutate_kernel      children from the ranked elites (gpu_device_search.py:27-114)
-//   det scorer         E of every child (n3_score_population)
+//   mutate_kernel      children from the ranked elites (gpu_device_search.py:27-114),
+//                      recording each child's parent and swaps
+//   child_delta_kernel E and badness of every child from its parent's by the exact
+//                      delta of each swap (the reference rescores every child)
 //   select_kernel      stable score order prefix, the children within the energy
 //                      window in index order, their random.Random shuffle, the
 //                      pick of elite_size children (gpu_device_search.py:343-373)
-//   gather_kernel      + det scorer with badness on the picked children
+//   gather_kernel      the picked children's rows, E and badness
 //   rank_kernel        rank_elites order (gpu_device_search.py:185-197) and the
 //                      best-so-far update by elite_key (:200-203, :388-396)
 // The reference does the selection and ranking on the host with a copy of
@@ -18,6 +20,8 @@
 // first rejected draw).
 #include <stdint.h>
 
+#include "chain_move.cuh"
+#include "dirs.cuh"
 #include "n3_common.cuh"
 
 namespace n3 {
@@ -45,6 +49,10 @@ struct MutArgs {
   uint64_t seed;
   int32_t* cp;
   int32_t* cq;
+  int32_t* child_parent;  // optional: each child's parent and swaps (u | v << 8), for the delta scoring
+  int32_t* child_moves;
+  int32_t* child_nmoves;
+  int moves_cap;
 };
 
 // One thread per child, as the reference's kernel; same draws in the same order.
@@ -77,7 +85,13 @@ __global__ void __launch_bounds__(128) mutate_kernel(const MutArgs A) {
     P[r] = src_p[r];
     Q[r] = src_q[r];
   }
-  if (child < parent_count) return;
+  const bool record = A.child_moves != nullptr;
+  if (record) A.child_parent[child] = parent;
+  int nmoves = 0;
+  if (child < parent_count) {
+    if (record) A.child_nmoves[child] = 0;
+    return;
+  }
   const int32_t* bad = A.pbad + (size_t)parent * m;
   int total = 0;
   for (int e = 0; e < m; ++e) total += bad[e];
@@ -114,9 +128,75 @@ __global__ void __launch_bounds__(128) mutate_kernel(const MutArgs A) {
       if (cv == ou || cu == ov) continue;
       *su = cv;
       *sv = cu;
+      if (record && nmoves < A.moves_cap) A.child_moves[(size_t)child * A.moves_cap + nmoves] = u | (v << 8);
+      ++nmoves;
       break;
     }
   }
+  if (record) A.child_nmoves[child] = nmoves;
+}
+
+// --------------------------------------------------------------------------
+// Children's scores by exact deltas: warp per child, the parent's columns and
+// badness in shared memory, then each recorded swap applied with its exact dE
+// and the exact update of every badness (move_exact_t<true>, the tempering
+// move without the Metropolis test).  E and badness equal a full recount.
+// --------------------------------------------------------------------------
+constexpr int kDeltaWarps = 16;
+constexpr size_t kDeltaSmem = kFullLutBytes + kDeltaWarps * (sizeof(uint32_t) * kDirWords + 2 * sizeof(int) * kMaxM);
+
+struct DeltaArgs {
+  const int32_t* ep;
+  const int32_t* eq;
+  const int32_t* ebad;
+  const int32_t* es;
+  const int32_t* parent;
+  const int32_t* moves;
+  const int32_t* nmoves;
+  int moves_cap, n, population;
+  const int64_t* status;
+  const uint16_t* lutf;
+  int32_t* scores;
+  int32_t* badness;
+  uint32_t* error_word;
+};
+
+__global__ void __launch_bounds__(kDeltaWarps * 32, 1) child_delta_kernel(const DeltaArgs A) {
+  extern __shared__ __align__(16) unsigned char smem[];
+  if (A.status[1] == 0) return;  // uniform: the search has reached E = 0
+  uint16_t* lutf = reinterpret_cast<uint16_t*>(smem);
+  uint32_t* hist_all = reinterpret_cast<uint32_t*>(smem + kFullLutBytes);
+  int* cs_all = reinterpret_cast<int*>(hist_all + kDeltaWarps * kDirWords);
+  int* bs_all = cs_all + kDeltaWarps * kMaxM;
+  full_lut_copy(lutf, A.lutf);
+  for (int i = threadIdx.x; i < kDeltaWarps * kDirWords / 4; i += blockDim.x)
+    reinterpret_cast<uint4*>(hist_all)[i] = make_uint4(0u, 0u, 0u, 0u);
+  __syncthreads();
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int n = A.n, m = 2 * n;
+  int* cs = cs_all + warp * kMaxM;
+  int* bs = bs_all + warp * kMaxM;
+  uint32_t* hist = hist_all + warp * kDirWords;
+  uint32_t err = 0;
+  for (int c = blockIdx.x * kDeltaWarps + warp; c < A.population; c += gridDim.x * kDeltaWarps) {
+    const int par = A.parent[c];
+    for (int s = lane; s < m; s += 32) {
+      cs[s] = (s & 1) ? A.eq[(size_t)par * n + (s >> 1)] : A.ep[(size_t)par * n + (s >> 1)];
+      bs[s] = A.ebad[(size_t)par * m + s];
+    }
+    __syncwarp();
+    int E = A.es[par];
+    const int k_end = min(A.nmoves[c], A.moves_cap);
+    for (int k = 0; k < k_end; ++k) {
+      const int mv = A.moves[(size_t)c * A.moves_cap + k];
+      int dE;
+      move_exact_t<true>(cs, bs, m, lutf, hist, lane, mv & 0xFF, (mv >> 8) & 0xFF, 0u, nullptr, 0, E, err, &dE);
+    }
+    if (lane == 0) A.scores[c] = E;
+    for (int s = lane; s < m; s += 32) A.badness[(size_t)c * m + s] = bs[s];
+    __syncwarp();
+  }
+  if (lane == 0 && err && A.error_word) atomicOr(A.error_word, err);
 }
 
 // --------------------------------------------------------------------------
@@ -473,14 +553,16 @@ constexpr size_t kSelSmem = sizeof(uint64_t) * kMaxElite + sizeof(uint32_t) * kM
 
 // pick rows r = child rows selected[r]
 __global__ void gather_kernel(const int32_t* __restrict__ cp, const int32_t* __restrict__ cq,
-                              const int32_t* __restrict__ cs, const int32_t* __restrict__ selected, int n,
-                              const int64_t* status, int32_t* pp, int32_t* pq, int32_t* ps) {
+                              const int32_t* __restrict__ cs, const int32_t* __restrict__ cbad,
+                              const int32_t* __restrict__ selected, int n, const int64_t* status, int32_t* pp,
+                              int32_t* pq, int32_t* ps, int32_t* pbad) {
   if (status[1] == 0) return;
   const int r = blockIdx.x, c = selected[r];
   for (int i = threadIdx.x; i < n; i += blockDim.x) {
     pp[(size_t)r * n + i] = cp[(size_t)c * n + i];
     pq[(size_t)r * n + i] = cq[(size_t)c * n + i];
   }
+  for (int i = threadIdx.x; i < 2 * n; i += blockDim.x) pbad[(size_t)r * 2 * n + i] = cbad[(size_t)c * 2 * n + i];
   if (threadIdx.x == 0) ps[r] = cs[c];
 }
 
@@ -597,12 +679,14 @@ static int check_beam(const n3_beam* b) {
     return set_error(N3_ERR_RANGE, "beam: elite_size must lie in [2, %d]", n3::beam::kMaxElite);
   if (b->population < b->elite_size || b->population > n3::beam::kMaxPopulation)
     return set_error(N3_ERR_RANGE, "beam: population must lie in [elite_size, %d]", n3::beam::kMaxPopulation);
-  if (b->max_strength < 1) return set_error(N3_ERR_RANGE, "beam: max_strength must be positive");
+  if (b->max_strength < 1 || b->max_strength > 4096)
+    return set_error(N3_ERR_RANGE, "beam: max_strength must lie in [1, 4096]");
   if (b->bad_bias < 0 || b->bad_bias > 100) return set_error(N3_ERR_RANGE, "beam: bad_bias must lie in [0, 100]");
   if (b->energy_window < 0) return set_error(N3_ERR_RANGE, "beam: energy_window must be non-negative");
   const void* ptrs[] = {b->elite_p, b->elite_q, b->elite_badness, b->elite_scores, b->child_p, b->child_q,
                         b->child_scores, b->pick_p, b->pick_q, b->pick_badness, b->pick_scores, b->selected,
-                        b->rng, b->status, b->best_p, b->best_q};
+                        b->rng, b->status, b->best_p, b->best_q, b->child_parent, b->child_moves,
+                        b->child_nmoves, b->child_badness};
   for (const void* p : ptrs)
     if (p == nullptr) return set_error(N3_ERR_ARG, "beam: null buffer");
   return N3_OK;
@@ -660,6 +744,8 @@ int n3_beam_mutate(const int32_t* parent_p, const int32_t* parent_q, const int32
   A.seed = seed;
   A.cp = child_p;
   A.cq = child_q;
+  A.child_parent = A.child_moves = A.child_nmoves = nullptr;
+  A.moves_cap = 0;
   n3::beam::mutate_kernel<<<(population + 127) / 128, 128, 0, (cudaStream_t)stream>>>(A);
   return n3host::check_launch("beam mutate_kernel");
 }
@@ -710,9 +796,34 @@ int n3_beam_generation(const n3_beam* b, int generation, void* stream) {
   M.seed = b->seed;
   M.cp = b->child_p;
   M.cq = b->child_q;
+  M.child_parent = b->child_parent;
+  M.child_moves = b->child_moves;
+  M.child_nmoves = b->child_nmoves;
+  M.moves_cap = b->max_strength;
   n3::beam::mutate_kernel<<<(b->population + 127) / 128, 128, 0, st>>>(M);
   N3_TRY(n3host::check_launch("beam mutate_kernel"));
-  N3_TRY(n3_score_population(b->child_p, b->child_q, b->population, b->n, b->child_scores, nullptr, stream));
+  N3_TRY(n3host::ensure_device_tables());
+  N3_TRY(n3host::allow_smem(reinterpret_cast<const void*>(n3::beam::child_delta_kernel), n3::beam::kDeltaSmem));
+  n3::beam::DeltaArgs D;
+  D.ep = b->elite_p;
+  D.eq = b->elite_q;
+  D.ebad = b->elite_badness;
+  D.es = b->elite_scores;
+  D.parent = b->child_parent;
+  D.moves = b->child_moves;
+  D.nmoves = b->child_nmoves;
+  D.moves_cap = b->max_strength;
+  D.n = b->n;
+  D.population = b->population;
+  D.status = b->status;
+  D.lutf = n3host::dir_lut_full_device_ptr();
+  D.scores = b->child_scores;
+  D.badness = b->child_badness;
+  D.error_word = b->error_word;
+  const int dgrid = (b->population + n3::beam::kDeltaWarps - 1) / n3::beam::kDeltaWarps;
+  n3::beam::child_delta_kernel<<<dgrid < n3host::sm_count() ? dgrid : n3host::sm_count(), n3::beam::kDeltaWarps * 32,
+                                 n3::beam::kDeltaSmem, st>>>(D);
+  N3_TRY(n3host::check_launch("beam child_delta_kernel"));
   N3_TRY(n3host::allow_smem(reinterpret_cast<const void*>(n3::beam::select_kernel), n3::beam::kSelSmem));
   n3::beam::SelArgs S;
   S.scores = b->child_scores;
@@ -724,10 +835,10 @@ int n3_beam_generation(const n3_beam* b, int generation, void* stream) {
   S.selected = b->selected;
   n3::beam::select_kernel<<<1, n3::beam::kSelThreads, n3::beam::kSelSmem, st>>>(S);
   N3_TRY(n3host::check_launch("beam select_kernel"));
-  n3::beam::gather_kernel<<<b->elite_size, 128, 0, st>>>(b->child_p, b->child_q, b->child_scores, b->selected, b->n,
-                                                          b->status, b->pick_p, b->pick_q, b->pick_scores);
+  n3::beam::gather_kernel<<<b->elite_size, 128, 0, st>>>(b->child_p, b->child_q, b->child_scores, b->child_badness,
+                                                          b->selected, b->n, b->status, b->pick_p, b->pick_q,
+                                                          b->pick_scores, b->pick_badness);
   N3_TRY(n3host::check_launch("beam gather_kernel"));
-  N3_TRY(n3_score_population(b->pick_p, b->pick_q, b->elite_size, b->n, b->pick_scores, b->pick_badness, stream));
   n3::beam::rank_kernel<<<1, n3::beam::kRankThreads, 0, st>>>(n3host::rank_args(b, b->elite_size, generation));
   return n3host::check_launch("beam rank_kernel");
 }

@@ -14,10 +14,12 @@ namespace n3 {
 // threshold row `thr` (width W) with the 32-bit uniform z, and on acceptance
 // the exact update of every slot's badness, the columns and E.  The caller
 // has checked legality.  Returns 1 if accepted; *dE_out receives dE.
-__device__ __forceinline__ int move_exact(int* __restrict__ cs, int* __restrict__ bs, int m,
-                                          const uint16_t* __restrict__ lutf, uint32_t* __restrict__ hist, int lane,
-                                          int u, int v, uint32_t z, const uint32_t* __restrict__ thr, int W, int& E,
-                                          uint32_t& err, int* dE_out) {
+// FORCE: the move is applied whatever its dE (no Metropolis test).
+template <bool FORCE>
+__device__ __forceinline__ int move_exact_t(int* __restrict__ cs, int* __restrict__ bs, int m,
+                                            const uint16_t* __restrict__ lutf, uint32_t* __restrict__ hist, int lane,
+                                            int u, int v, uint32_t z, const uint32_t* __restrict__ thr, int W, int& E,
+                                            uint32_t& err, int* dE_out) {
   const int ru = u >> 1, rv = v >> 1, cu = cs[u], cv = cs[v];
   int ids[kSlotsPerLane], cnt_new[kSlotsPerLane];
   // centre u' = (r_u, c_v)
@@ -50,7 +52,7 @@ __device__ __forceinline__ int move_exact(int* __restrict__ cs, int* __restrict_
   const int t_a = sum_ab & 0xFFFF, t_b = sum_ab >> 16;
   const int dE = (t_a + t_b + j_new) - (bs[u] + bs[v] - sum_joint);
   *dE_out = dE;
-  const bool accept = dE <= 0 || (dE < W && z < thr[dE]);
+  const bool accept = FORCE || dE <= 0 || (dE < W && z < thr[dE]);
   if (!accept) {
     __syncwarp();
     return 0;
@@ -92,6 +94,13 @@ __device__ __forceinline__ int move_exact(int* __restrict__ cs, int* __restrict_
   __syncwarp();
   E += dE;
   return 1;
+}
+
+__device__ __forceinline__ int move_exact(int* __restrict__ cs, int* __restrict__ bs, int m,
+                                          const uint16_t* __restrict__ lutf, uint32_t* __restrict__ hist, int lane,
+                                          int u, int v, uint32_t z, const uint32_t* __restrict__ thr, int W, int& E,
+                                          uint32_t& err, int* dE_out) {
+  return move_exact_t<false>(cs, bs, m, lutf, hist, lane, u, v, z, thr, W, E, err, dE_out);
 }
 
 // One uniform proposal (tempering.py:50-58 draws u, v uniformly; here from a

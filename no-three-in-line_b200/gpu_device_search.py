@@ -8,7 +8,9 @@ the children within ``energy_window`` of the best, the same rank_elites order
 and elite_key best-so-far rule.  The difference is where it runs: every
 generation is five kernel launches on one stream (libn3 ``n3_beam_generation``)
 with no copy back to the host, where the reference copies every child's score
-to the host, sorts and shuffles in Python and copies the elites back.  Without
+to the host, sorts and shuffles in Python and copies the elites back.  Each
+child is scored from its parent by the exact delta of each of its swaps (the
+reference rescores every child in full); the result is the same integer.  Without
 a callback the host synchronises only to stop early (every ``report_every``
 generations) and at the end; with a callback it reads an 8-word status after
 each generation (the reference's reporting rule needs to know whether the
@@ -41,7 +43,9 @@ class BeamDesc(ctypes.Structure):
                [(name, _P) for name in ("elite_p", "elite_q", "elite_badness", "elite_scores", "child_p", "child_q",
                                         "child_scores", "pick_p", "pick_q", "pick_badness", "pick_scores",
                                         "selected", "rng", "status", "best_p", "best_q", "history")] + \
-               [("history_len", _I)]
+               [("history_len", _I)] + \
+               [(name, _P) for name in ("child_parent", "child_moves", "child_nmoves", "child_badness",
+                                        "error_word")]
 
 
 _lib.register("n3_beam_mutate", [_P, _P, _P] + [_I] * 7 + [ctypes.c_uint64, _I, _P, _P, _P])
@@ -150,6 +154,10 @@ class DeviceBeam:
         self.status = z(STATUS_WORDS, dtype=t.int64)
         self.best_p, self.best_q = z(n), z(n)
         self.history = z(max(1, history_len), 2)
+        self.child_parent, self.child_nmoves = z(population), z(population)
+        self.child_moves = z(population, max_strength)
+        self.child_badness = z(population, 2 * n)
+        self.error_word = z(1)
         self.desc = BeamDesc(n, population, elite_size, energy_window, max_strength, bad_bias,
                              seed & (2**64 - 1),
                              *[_lib.ptr(x) for x in (self.elite_p, self.elite_q, self.elite_badness,
@@ -157,7 +165,9 @@ class DeviceBeam:
                                                      self.child_scores, self.pick_p, self.pick_q, self.pick_badness,
                                                      self.pick_scores, self.selected, self.rng, self.status,
                                                      self.best_p, self.best_q, self.history)],
-                             history_len)
+                             history_len,
+                             *[_lib.ptr(x) for x in (self.child_parent, self.child_moves, self.child_nmoves,
+                                                     self.child_badness, self.error_word)])
 
     def init(self, base: np.ndarray, stream=None) -> None:
         t = _lib.torch()
@@ -170,7 +180,12 @@ class DeviceBeam:
         _lib.call("n3_beam_generation", ctypes.byref(self.desc), g, _lib.stream_ptr(stream))
 
     def read_status(self) -> np.ndarray:
-        return self.status.cpu().numpy()
+        """The 8 status words; raises AssertionError if a child's maintained
+        badness failed its re-check (device error bit 16)."""
+        st = self.status.cpu().numpy()
+        if int(self.error_word.item()):
+            raise AssertionError(f"beam search: device error bits {int(self.error_word.item()):#x}")
+        return st
 
 
 def gpu_device_beam_search(
