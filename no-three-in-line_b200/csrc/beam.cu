@@ -14,10 +14,9 @@
 // The reference does the selection and ranking on the host with a copy of
 // every child's score each generation.  Here the selection is one CTA: a radix
 // select of the elite_size-th smallest score, a bitonic sort of the scores
-// below it, ordered compactions by block scans, and the shuffle by one warp on
-// a copy of the window list in shared memory (the shuffle must consume exactly
-// CPython's draws: the warp tries 32 steps per round and keeps those before the
-// first rejected draw).
+// below it, ordered compactions by per-warp counts, the shuffle's draws by one
+// warp (they must be exactly CPython's: the warp tries 32 steps per round), and
+// the first elite_size shuffled positions traced back through the draws.
 #include <stdint.h>
 
 #include "chain_move.cuh"
@@ -245,7 +244,9 @@ __device__ __forceinline__ uint32_t mt_temper(uint32_t y) {
 // coincide (a bit per position in `seen`, zero on entry and on return, finds
 // repeats), and are then made by all lanes at once, otherwise by lane 0 in step
 // order.  idx: position in the block (warp-uniform).
-template <class T>
+// STORE: instead of swapping, record j of every step s in values[s] (T must
+// hold count - 1); the swaps are then traced back only for the positions needed.
+template <class T, bool STORE = false>
 __device__ void py_shuffle_warp(uint32_t* mt, uint32_t* out, int& idx, T* values, int count, uint32_t* seen,
                                 int lane) {
   for (int k = lane; k < kMT; k += 32) out[k] = mt_temper(mt[k]);
@@ -281,14 +282,19 @@ __device__ void py_shuffle_warp(uint32_t* mt, uint32_t* out, int& idx, T* values
     }
     if (__popc(acc_mask) >= m) {  // the m-th acceptance ends the round (the next step draws wider or
                                   // narrower, or there is none); later draws stay unused
-      unsigned mm = acc_mask;
-      for (int c = 1; c < m; ++c) mm &= mm - 1u;  // drop the first m - 1 set bits
-      const int z = __ffs(mm) - 1;
-      acc_mask &= z < 31 ? (2u << z) - 1u : 0xffffffffu;
+      const int z = __ffs(__ballot_sync(0xffffffffu, ((acc_mask >> lane) & 1u) &&
+                                                      __popc(acc_mask & ((2u << lane) - 1u)) == m)) - 1;
+      acc_mask &= (2u << z) - 1u;  // 2u << 31 wraps to 0: all bits
       used = z + 1;
     }
     const int nb = __popc(acc_mask);
     const int s_max = i, s_min = s_max - nb + 1;
+    if (STORE) {
+      if ((acc_mask >> lane) & 1u) values[s_max - __popc(acc_mask & below)] = (T)r;
+      i -= nb;
+      idx += used;
+      continue;
+    }
     // an accepted draw swaps its step s = s_max - (accepted draws before it) with j = r;
     // a j inside [s_min, s_max] (other than s) or met twice orders the swaps
     const bool mine = (acc_mask >> lane) & 1u;
@@ -372,33 +378,8 @@ constexpr int kSelThreads = 1024;
 constexpr int kMaxPopulation = 65536;
 constexpr int kMaxElite = 2048;
 
-// Exclusive block scan of one value per thread; returns this thread's offset and
-// writes the total to *total (all threads).  `warp_tot`: shared int[32].
-__device__ __forceinline__ int block_exclusive_scan(int v, int* warp_tot, int* total) {
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  int x = v;
-#pragma unroll
-  for (int o = 1; o < 32; o <<= 1) {
-    const int y = __shfl_up_sync(0xffffffffu, x, o);
-    if (lane >= o) x += y;
-  }
-  if (lane == 31) warp_tot[warp] = x;
-  __syncthreads();
-  if (warp == 0) {
-    int w = lane < (int)(blockDim.x >> 5) ? warp_tot[lane] : 0;
-#pragma unroll
-    for (int o = 1; o < 32; o <<= 1) {
-      const int y = __shfl_up_sync(0xffffffffu, w, o);
-      if (lane >= o) w += y;
-    }
-    warp_tot[lane] = w;  // inclusive prefix of the warp totals
-  }
-  __syncthreads();
-  const int before = (warp > 0 ? warp_tot[warp - 1] : 0) + x - v;
-  *total = warp_tot[(blockDim.x >> 5) - 1];
-  __syncthreads();
-  return before;
-}
+constexpr int kSelWarps = kSelThreads / 32;
+static_assert(kSelWarps == 32, "the per-warp offsets are scanned by one warp, one lane per warp");
 
 struct SelArgs {
   const int32_t* scores;  // [population]
@@ -408,40 +389,62 @@ struct SelArgs {
   int32_t* selected;      // [elite_size]
 };
 
+// Warp w owns the children [w * seg, (w + 1) * seg) (seg a multiple of 32) and
+// reads them 32 at a time, so every pass over the scores is coalesced and every
+// ordered compaction is a per-warp running count plus one scan over the warps.
 __global__ void __launch_bounds__(kSelThreads, 1) select_kernel(const SelArgs A) {
   extern __shared__ __align__(16) unsigned char smem[];
   const int P = A.population, E = A.elite_size, tid = threadIdx.x;
+  const int lane = tid & 31, warp = tid >> 5;
+  const unsigned below = (1u << lane) - 1u;
   uint64_t* keys = reinterpret_cast<uint64_t*>(smem);                 // [kMaxElite]
   uint32_t* mt = reinterpret_cast<uint32_t*>(keys + kMaxElite);       // [624]
   int32_t* order = reinterpret_cast<int32_t*>(mt + kMT);              // [kMaxElite] score-order prefix
   uint32_t* mark = reinterpret_cast<uint32_t*>(order + kMaxElite);    // [kMaxPopulation / 32]
-  uint16_t* window = reinterpret_cast<uint16_t*>(mark + kMaxPopulation / 32);  // [population]
+  uint16_t* jstep = reinterpret_cast<uint16_t*>(mark + kMaxPopulation / 32);  // [population] j of shuffle step s
   __shared__ uint32_t hist[256];
-  __shared__ int warp_tot[32];
+  __shared__ int tie_off[kSelWarps], win_off[kSelWarps];
   __shared__ int s_misc[4];
   __shared__ uint32_t mt_out[kMT];  // tempered outputs of the current state block
   if (A.status[1] == 0) return;  // uniform: the search has reached E = 0
   const int64_t limit = A.status[1] + (int64_t)A.energy_window;
   for (int i = tid; i < kMaxPopulation / 32; i += kSelThreads) mark[i] = 0u;
   for (int i = tid; i < kMT; i += kSelThreads) mt[i] = A.rng[i];
-  const int chunk = (P + kSelThreads - 1) / kSelThreads;
-  const int lo = min(P, tid * chunk), hi = min(P, lo + chunk);
+  const int seg = (P + kSelThreads - 1) / kSelThreads * 32;
+  const int s_lo = min(P, warp * seg), s_hi = min(P, s_lo + seg);
+  if (tid == 0) s_misc[2] = 0;
 
-  // 1. T = the E-th smallest score (radix select over 32-bit scores, 8 bits a pass)
+  // 1. T = the E-th smallest score: radix select over the 32-bit scores, 8 bits
+  //    a pass, from the highest byte that any score uses
+  uint32_t top = 0u;
+  for (int b = s_lo; b < s_hi; b += 32)
+    if (b + lane < s_hi) top = max(top, (uint32_t)A.scores[b + lane]);
+  top = __reduce_max_sync(0xffffffffu, top);
+  if (lane == 0) hist[warp] = top;
+  __syncthreads();
+  if (warp == 0) {
+    const uint32_t m = __reduce_max_sync(0xffffffffu, hist[lane]);
+    if (lane == 0) s_misc[3] = (int)m;
+  }
+  __syncthreads();
+  top = (uint32_t)s_misc[3];
+  int shift = 24;
+  while (shift > 0 && (top >> shift) == 0u) shift -= 8;  // the skipped high bytes are zero in every score
   uint32_t prefix = 0u, mask = 0u;
   int remaining = E;  // 1-based rank of the E-th element among those matching prefix
-  for (int shift = 24; shift >= 0; shift -= 8) {
+  for (; shift >= 0; shift -= 8) {
     for (int i = tid; i < 256; i += kSelThreads) hist[i] = 0u;
     __syncthreads();
-    for (int b = 0; b < chunk; ++b) {  // warp-uniform trip count; equal digits add once per warp
-      const int i = lo + b;
-      const uint32_t x = i < hi ? (uint32_t)A.scores[i] : 0u;
-      const bool valid = i < hi && (x & mask) == prefix;
+#pragma unroll 4
+    for (int b = s_lo; b < s_hi; b += 32) {  // warp-uniform trip count; equal digits add once per warp
+      const int i = b + lane;
+      const uint32_t x = i < s_hi ? (uint32_t)A.scores[i] : 0u;
+      const bool valid = i < s_hi && (x & mask) == prefix;
       const unsigned act = __ballot_sync(0xffffffffu, valid);
       if (valid) {
         const uint32_t digit = (x >> shift) & 255u;
         const unsigned peers = __match_any_sync(act, digit);
-        if ((threadIdx.x & 31) == __ffs(peers) - 1) atomicAdd(&hist[digit], (uint32_t)__popc(peers));
+        if (lane == __ffs(peers) - 1) atomicAdd(&hist[digit], (uint32_t)__popc(peers));
       }
     }
     __syncthreads();
@@ -463,18 +466,62 @@ __global__ void __launch_bounds__(kSelThreads, 1) select_kernel(const SelArgs A)
   const uint32_t T = prefix;
   const int n_less = E - remaining;  // scores below T; then `remaining` ties at T by index
 
-  // 2. scores below T, sorted by (score, index): a bitonic sort of at most E - 1 keys
-  if (tid == 0) s_misc[2] = 0;
-  __syncthreads();
-  for (int i = lo; i < hi; ++i) {
-    const uint32_t x = (uint32_t)A.scores[i];
-    if (x < T) keys[atomicAdd(&s_misc[2], 1)] = ((uint64_t)x << 32) | (uint32_t)i;
+  // 2. one pass: the keys below T (at most E - 1), and per warp the ties at T
+  //    and the children within the energy window
+  int c_tie = 0, c_win = 0;
+#pragma unroll 4
+  for (int b = s_lo; b < s_hi; b += 32) {
+    const int i = b + lane;
+    const int x = i < s_hi ? A.scores[i] : 0;
+    const unsigned lt = __ballot_sync(0xffffffffu, i < s_hi && (uint32_t)x < T);
+    if (lt) {
+      int at = 0;
+      if (lane == 0) at = atomicAdd(&s_misc[2], __popc(lt));
+      at = __shfl_sync(0xffffffffu, at, 0);
+      if ((lt >> lane) & 1u) keys[at + __popc(lt & below)] = ((uint64_t)(uint32_t)x << 32) | (uint32_t)i;
+    }
+    c_tie += __popc(__ballot_sync(0xffffffffu, i < s_hi && (uint32_t)x == T));
+    c_win += __popc(__ballot_sync(0xffffffffu, i < s_hi && (int64_t)x <= limit));
+  }
+  if (lane == 0) {
+    tie_off[warp] = c_tie;
+    win_off[warp] = c_win;
   }
   __syncthreads();
+  if (warp == 0) {  // exclusive scans over the warps
+    int t = tie_off[lane], w = win_off[lane];
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const int yt = __shfl_up_sync(0xffffffffu, t, o), yw = __shfl_up_sync(0xffffffffu, w, o);
+      if (lane >= o) {
+        t += yt;
+        w += yw;
+      }
+    }
+    tie_off[lane] = t - tie_off[lane];
+    if (lane == 31) s_misc[0] = w;  // the window's size
+    win_off[lane] = w - win_off[lane];
+  }
   int width = 1;
   while (width < n_less) width <<= 1;
   for (int i = n_less + tid; i < width; i += kSelThreads) keys[i] = ~0ull;
   __syncthreads();
+  const int n_window = s_misc[0];
+
+  // 3. the first `remaining` ties at T in index order; the keys below T sorted
+  //    by (score, index) with a bitonic sort
+  {
+    int o = tie_off[warp];
+    for (int b = s_lo; b < s_hi && o < remaining; b += 32) {
+      const int i = b + lane;
+      const unsigned m = __ballot_sync(0xffffffffu, i < s_hi && (uint32_t)A.scores[i] == T);
+      if ((m >> lane) & 1u) {
+        const int r = o + __popc(m & below);
+        if (r < remaining) order[n_less + r] = i;
+      }
+      o += __popc(m);
+    }
+  }
   for (int size = 2; size <= width; size <<= 1) {
     for (int stride = size >> 1; stride > 0; stride >>= 1) {
       for (int i = tid; i < width; i += kSelThreads) {
@@ -493,34 +540,56 @@ __global__ void __launch_bounds__(kSelThreads, 1) select_kernel(const SelArgs A)
   }
   for (int i = tid; i < n_less; i += kSelThreads) order[i] = (int32_t)(uint32_t)keys[i];
 
-  // 3. the first `remaining` ties at T in index order, then the window list in
-  //    index order (both by ordered compaction over the threads' chunks)
-  int c_tie = 0, c_win = 0;
-  for (int i = lo; i < hi; ++i) {
-    const int x = A.scores[i];
-    c_tie += (uint32_t)x == T;
-    c_win += (int64_t)x <= limit;
-  }
-  int total;
-  int o_tie = block_exclusive_scan(c_tie, warp_tot, &total);
-  int o_win = block_exclusive_scan(c_win, warp_tot, &total);
-  const int n_window = total;
-  for (int i = lo; i < hi; ++i) {
-    const int x = A.scores[i];
-    if ((uint32_t)x == T) {
-      if (o_tie < remaining) order[n_less + o_tie] = i;
-      ++o_tie;
-    }
-    if ((int64_t)x <= limit) window[o_win++] = (uint16_t)i;
+  // 4. warp 0 draws the shuffle of the window list (gpu_device_search.py:340-373):
+  //    the j of every step s, jstep[s]; the swaps themselves are not applied
+  if (warp == 0) {
+    int idx = (int)A.rng[kMT];
+    py_shuffle_warp<uint16_t, true>(mt, mt_out, idx, jstep, n_window, mark, lane);
+    if (lane == 0) A.rng[kMT] = (uint32_t)idx;
   }
   __syncthreads();
 
-  // 4. warp 0: the shuffle; thread 0: the pick (gpu_device_search.py:340-373)
-  if (tid < 32) {
-    int idx = (int)A.rng[kMT];
-    py_shuffle_warp(mt, mt_out, idx, window, n_window, mark, tid);  // mark: all zero here
-    if (tid == 0) A.rng[kMT] = (uint32_t)idx;
+  // 5. the first K = min(E, window) shuffled positions, one warp each.  Step s
+  //    fixes position s for good, so position p holds what sat at j_p before
+  //    step p; going back through the later steps p+1, p+2, ... (applied before
+  //    it), the item moves only where a step's j equals its position, to that
+  //    step.  The window position found is then mapped to its child through
+  //    the per-warp window offsets.
+  const int K = min(E, n_window);
+  int32_t* picked = reinterpret_cast<int32_t*>(keys);  // [K]; keys is free once order is written
+  for (int p = warp; p < K; p += kSelWarps) {
+    int pos = p == 0 ? 0 : (int)jstep[p];
+    for (int b = p + 1; b < n_window; b += 32) {
+      const int st = b + lane;
+      const int js = st < n_window ? (int)jstep[st] : -1;
+      unsigned hit = __ballot_sync(0xffffffffu, js == pos);
+      while (hit) {  // uniform
+        const int f = __ffs(hit) - 1;
+        pos = b + f;
+        hit = __ballot_sync(0xffffffffu, js == pos) & ~((2u << f) - 1u);
+      }
+    }
+    const unsigned owners = __ballot_sync(0xffffffffu, win_off[lane] <= pos);  // bit 0 always set
+    const int w = 31 - __clz(owners);
+    int rank = pos - win_off[w];
+    const int w_lo = min(P, w * seg), w_hi = min(P, w_lo + seg);
+    int child = -1;
+    for (int b = w_lo; b < w_hi; b += 32) {
+      const int i = b + lane;
+      const unsigned m = __ballot_sync(0xffffffffu, i < w_hi && (int64_t)A.scores[i] <= limit);
+      const int c = __popc(m);
+      if (rank < c) {  // uniform
+        const unsigned hitl = __ballot_sync(0xffffffffu, ((m >> lane) & 1u) && __popc(m & below) == rank);
+        child = b + __ffs(hitl) - 1;
+        break;
+      }
+      rank -= c;
+    }
+    if (lane == 0) picked[p] = child;
   }
+  __syncthreads();
+
+  // 6. thread 0: the pick (gpu_device_search.py:340-373)
   if (tid == 0) {
     int sel = 0;
     const int quality_keep = max(1, E / 4);
@@ -529,9 +598,9 @@ __global__ void __launch_bounds__(kSelThreads, 1) select_kernel(const SelArgs A)
       mark[c >> 5] |= 1u << (c & 31);
       A.selected[sel++] = c;
     }
-    for (int k = 0; k < n_window && sel < E; ++k) {
-      const int c = window[k];
-      if (!(mark[c >> 5] & (1u << (c & 31)))) {
+    for (int k = 0; k < K && sel < E; ++k) {
+      const int c = picked[k];
+      if (c >= 0 && !(mark[c >> 5] & (1u << (c & 31)))) {
         mark[c >> 5] |= 1u << (c & 31);
         A.selected[sel++] = c;
       }
