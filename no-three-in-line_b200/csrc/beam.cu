@@ -52,87 +52,148 @@ struct MutArgs {
   int32_t* child_moves;
   int32_t* child_nmoves;
   int moves_cap;
+  int prefix_cap;  // parents whose badness prefix sums the CTA stages in shared memory
 };
 
-// One thread per child, as the reference's kernel; same draws in the same order.
-// The parent's total badness is summed once per child instead of once per attempt
-// (it does not change), which leaves every draw and result unchanged.
-__global__ void __launch_bounds__(128) mutate_kernel(const MutArgs A) {
-  const int child = blockIdx.x * blockDim.x + threadIdx.x;
-  if (child >= A.population) return;
+// One thread per child, the reference's draws in the reference's order.  The
+// CTA's 64 children live in shared memory (slot layout s = 2 * row + layer)
+// from the parent copy to one coalesced write of their rows.  When the parents'
+// badness prefix sums fit in shared memory (prefix_cap parents), the CTA builds
+// them once and the roulette draw becomes a binary search: with no negative
+// badness, the linear scan `t -= bad[u]` stops at the first u whose inclusive
+// prefix exceeds t, which the search finds.  A negative badness anywhere, or
+// one large enough for a sum to overflow (neither is a state's badness), sends
+// the CTA back to the linear scan, so every draw and result stays the
+// reference's for any input.  The parent's total badness is
+// taken once per child instead of once per attempt (it does not change).
+constexpr int kMutThreads = 64;
+constexpr size_t kMutPrefixMaxBytes = 96 * 1024;
+
+constexpr size_t kMutSmemMax = sizeof(int32_t) * kMutThreads * kMaxM + kMutPrefixMaxBytes;
+
+__global__ void __launch_bounds__(kMutThreads) mutate_kernel(const MutArgs A) {
+  extern __shared__ __align__(16) unsigned char smem[];
+  __shared__ int s_parent[kMutThreads];
   int parent_count = A.parent_count, quality_count = A.quality_count, active = A.active_strength;
   if (A.status != nullptr) {
-    if (A.status[1] == 0) return;  // the search has reached E = 0
+    if (A.status[1] == 0) return;  // uniform: the search has reached E = 0
     parent_count = (int)A.status[0];
     quality_count = max(1, min(parent_count, A.elite_size / 4));
     active = min(A.max_strength, 2 + (A.generation - (int)A.status[4]) / 10);
   }
-  const int n = A.n, m = 2 * n;
+  const int n = A.n, m = 2 * n, tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const int child0 = blockIdx.x * kMutThreads, child = child0 + tid;
+  const int nc = min(kMutThreads, A.population - child0);
+  int32_t* rows = reinterpret_cast<int32_t*>(smem);  // [kMutThreads][m]
+  int32_t* prefix = rows + kMutThreads * m;          // [prefix_cap][m] inclusive prefix sums
   uint64_t rng = A.seed ^ (0x9e3779b97f4a7c15ULL * (uint64_t)(child + 1)) ^
                  (0xbf58476d1ce4e5b9ULL * (uint64_t)(A.generation + 1));
   int parent = child;
-  if (child >= parent_count) {
+  if (child < A.population && child >= parent_count) {
     const uint64_t pick = xs64(rng);
     const int pool = (pick & 255ULL) < 160ULL ? quality_count : parent_count;
     parent = (int)(xs64(rng) % (uint64_t)pool);
   }
-  int32_t* P = A.cp + (size_t)child * n;
-  int32_t* Q = A.cq + (size_t)child * n;
-  const int32_t* src_p = A.pp + (size_t)parent * n;
-  const int32_t* src_q = A.pq + (size_t)parent * n;
-  for (int r = 0; r < n; ++r) {
-    P[r] = src_p[r];
-    Q[r] = src_q[r];
-  }
-  const bool record = A.child_moves != nullptr;
-  if (record) A.child_parent[child] = parent;
-  int nmoves = 0;
-  if (child < parent_count) {
-    if (record) A.child_nmoves[child] = 0;
-    return;
-  }
-  const int32_t* bad = A.pbad + (size_t)parent * m;
-  int total = 0;
-  for (int e = 0; e < m; ++e) total += bad[e];
-  int strength;
-  if ((xs64(rng) & 31ULL) == 0ULL)
-    strength = 1 + (int)(xs64(rng) % (uint64_t)A.max_strength);
-  else
-    strength = 1 + (int)(xs64(rng) % (uint64_t)active);
-  for (int step = 0; step < strength; ++step) {
-    for (int attempt = 0; attempt < 32; ++attempt) {
-      int u;
-      if ((int)(xs64(rng) % 100ULL) < A.bad_bias) {
-        if (total) {
-          int t = (int)(xs64(rng) % (uint64_t)total);
-          for (u = 0; u < m - 1; ++u) {
-            t -= bad[u];
-            if (t < 0) break;
-          }
-        } else {
-          u = (int)(xs64(rng) % (uint64_t)m);
-        }
-      } else {
-        u = (int)(xs64(rng) % (uint64_t)m);
+  s_parent[tid] = parent;
+  bool use_prefix = parent_count <= A.prefix_cap;  // uniform
+  if (use_prefix) {  // warp w: parents w, w + 2, ...; a lane sums a run of `per` slots
+    const int per = (m + 31) / 32, e0 = min(m, lane * per), e1 = min(m, e0 + per);
+    bool negative = false;
+    for (int p = warp; p < parent_count; p += kMutThreads / 32) {
+      const int32_t* bad = A.pbad + (size_t)p * m;
+      int sum = 0;
+      for (int e = e0; e < e1; ++e) {
+        const int b = bad[e];
+        negative |= b < 0 || b > 0x7fffffff / kMaxM;  // keeps every prefix sum below 2^31
+        sum += b;
       }
-      const int v = (int)(xs64(rng) % (uint64_t)m);
-      const int ru = u >> 1, rv = v >> 1;
-      if (ru == rv) continue;
-      int32_t* su = (u & 1) ? &Q[ru] : &P[ru];
-      int32_t* sv = (v & 1) ? &Q[rv] : &P[rv];
-      const int cu = *su, cv = *sv;
-      if (cu == cv) continue;
-      const int ou = (u & 1) ? P[ru] : Q[ru];
-      const int ov = (v & 1) ? P[rv] : Q[rv];
-      if (cv == ou || cu == ov) continue;
-      *su = cv;
-      *sv = cu;
-      if (record && nmoves < A.moves_cap) A.child_moves[(size_t)child * A.moves_cap + nmoves] = u | (v << 8);
-      ++nmoves;
-      break;
+      int incl = sum;
+#pragma unroll
+      for (int o = 1; o < 32; o <<= 1) {
+        const int y = __shfl_up_sync(0xffffffffu, incl, o);
+        if (lane >= o) incl += y;
+      }
+      int acc = incl - sum;
+      for (int e = e0; e < e1; ++e) prefix[p * m + e] = acc += bad[e];
+    }
+    use_prefix = !__syncthreads_or(negative);
+  } else {
+    __syncthreads();
+  }
+  for (int i = tid; i < nc * m; i += kMutThreads) {  // the parents' rows into the children's
+    const int c = i / m, s = i - c * m;
+    const size_t at = (size_t)s_parent[c] * n + (s >> 1);
+    rows[i] = (s & 1) ? A.pq[at] : A.pp[at];
+  }
+  __syncthreads();
+  const bool record = A.child_moves != nullptr;
+  if (child < A.population) {
+    if (record) A.child_parent[child] = parent;
+    if (child < parent_count) {
+      if (record) A.child_nmoves[child] = 0;
+    } else {
+      int32_t* cs = rows + tid * m;
+      const int32_t* bad = A.pbad + (size_t)parent * m;
+      const int32_t* pre = prefix + parent * m;
+      int total = 0;
+      if (use_prefix) {
+        total = pre[m - 1];
+      } else {
+        for (int e = 0; e < m; ++e) total += bad[e];
+      }
+      int strength, nmoves = 0;
+      if ((xs64(rng) & 31ULL) == 0ULL)
+        strength = 1 + (int)(xs64(rng) % (uint64_t)A.max_strength);
+      else
+        strength = 1 + (int)(xs64(rng) % (uint64_t)active);
+      for (int step = 0; step < strength; ++step) {
+        for (int attempt = 0; attempt < 32; ++attempt) {
+          int u;
+          if ((int)(xs64(rng) % 100ULL) < A.bad_bias) {
+            if (total) {
+              const int t = (int)(xs64(rng) % (uint64_t)total);
+              if (use_prefix) {  // first u with prefix[u] > t; prefix[m - 1] = total > t
+                int lo = 0, hi = m - 1;
+                while (lo < hi) {
+                  const int mid = (lo + hi) >> 1;
+                  if (pre[mid] > t) hi = mid;
+                  else lo = mid + 1;
+                }
+                u = lo;
+              } else {
+                int r = t;
+                for (u = 0; u < m - 1; ++u) {
+                  r -= bad[u];
+                  if (r < 0) break;
+                }
+              }
+            } else {
+              u = (int)(xs64(rng) % (uint64_t)m);
+            }
+          } else {
+            u = (int)(xs64(rng) % (uint64_t)m);
+          }
+          const int v = (int)(xs64(rng) % (uint64_t)m);
+          if ((u >> 1) == (v >> 1)) continue;
+          const int cu = cs[u], cv = cs[v];
+          if (cu == cv) continue;
+          if (cv == cs[u ^ 1] || cu == cs[v ^ 1]) continue;  // the other point of each row
+          cs[u] = cv;
+          cs[v] = cu;
+          if (record && nmoves < A.moves_cap) A.child_moves[(size_t)child * A.moves_cap + nmoves] = u | (v << 8);
+          ++nmoves;
+          break;
+        }
+      }
+      if (record) A.child_nmoves[child] = nmoves;
     }
   }
-  if (record) A.child_nmoves[child] = nmoves;
+  __syncthreads();
+  for (int i = tid; i < nc * n; i += kMutThreads) {  // coalesced: the CTA's rows are contiguous
+    const int c = i / n, r = i - c * n;
+    A.cp[(size_t)child0 * n + i] = rows[c * m + 2 * r];
+    A.cq[(size_t)child0 * n + i] = rows[c * m + 2 * r + 1];
+  }
 }
 
 // --------------------------------------------------------------------------
@@ -141,7 +202,7 @@ __global__ void __launch_bounds__(128) mutate_kernel(const MutArgs A) {
 // and the exact update of every badness (move_exact_t<true>, the tempering
 // move without the Metropolis test).  E and badness equal a full recount.
 // --------------------------------------------------------------------------
-constexpr int kDeltaWarps = 16;
+constexpr int kDeltaWarps = 22;
 constexpr size_t kDeltaSmem = kFullLutBytes + kDeltaWarps * (sizeof(uint32_t) * kDirWords + 2 * sizeof(int) * kMaxM);
 
 struct DeltaArgs {
@@ -741,6 +802,19 @@ __global__ void __launch_bounds__(kRankThreads, 1) rank_kernel(const RankArgs A)
 
 namespace n3host {
 
+// mutate_kernel over `population` children; the parents' prefix sums are staged
+// when at most `parents_bound` parents fit in kMutPrefixMaxBytes.
+static int launch_mutate(n3::beam::MutArgs A, int parents_bound, cudaStream_t st) {
+  using namespace n3::beam;
+  const int m = 2 * A.n;
+  const int cap = (int)(kMutPrefixMaxBytes / (sizeof(int32_t) * (size_t)m));
+  A.prefix_cap = parents_bound <= cap ? parents_bound : 0;
+  const size_t bytes = sizeof(int32_t) * (size_t)m * (kMutThreads + A.prefix_cap);
+  N3_TRY(allow_smem(reinterpret_cast<const void*>(mutate_kernel), kMutSmemMax));
+  mutate_kernel<<<(A.population + kMutThreads - 1) / kMutThreads, kMutThreads, bytes, st>>>(A);
+  return check_launch("beam mutate_kernel");
+}
+
 static int check_beam(const n3_beam* b) {
   if (b == nullptr) return set_error(N3_ERR_ARG, "null beam descriptor");
   if (b->n < 3 || b->n > N3_MAX_N) return set_error(N3_ERR_RANGE, "beam: n must lie in [3, %d]", N3_MAX_N);
@@ -815,8 +889,7 @@ int n3_beam_mutate(const int32_t* parent_p, const int32_t* parent_q, const int32
   A.cq = child_q;
   A.child_parent = A.child_moves = A.child_nmoves = nullptr;
   A.moves_cap = 0;
-  n3::beam::mutate_kernel<<<(population + 127) / 128, 128, 0, (cudaStream_t)stream>>>(A);
-  return n3host::check_launch("beam mutate_kernel");
+  return n3host::launch_mutate(A, parent_count, (cudaStream_t)stream);
 }
 
 int n3_py_random_seed(uint32_t* state, uint64_t seed, void* stream) {
@@ -869,8 +942,7 @@ int n3_beam_generation(const n3_beam* b, int generation, void* stream) {
   M.child_moves = b->child_moves;
   M.child_nmoves = b->child_nmoves;
   M.moves_cap = b->max_strength;
-  n3::beam::mutate_kernel<<<(b->population + 127) / 128, 128, 0, st>>>(M);
-  N3_TRY(n3host::check_launch("beam mutate_kernel"));
+  N3_TRY(n3host::launch_mutate(M, b->elite_size, st));
   N3_TRY(n3host::ensure_device_tables());
   N3_TRY(n3host::allow_smem(reinterpret_cast<const void*>(n3::beam::child_delta_kernel), n3::beam::kDeltaSmem));
   n3::beam::DeltaArgs D;

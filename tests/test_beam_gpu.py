@@ -36,6 +36,43 @@ def test_device_mutation_matches_reference_kernel(cuda, beam_golden):
     assert np.array_equal(cp_, g["mut_child_p"]) and np.array_equal(cq_, g["mut_child_q"])
 
 
+@pytest.mark.parametrize("parents,population,badness", [
+    (40, 1000, "states"),    # prefix sums staged per CTA; a ragged last CTA
+    (200, 777, "states"),    # 200 n=75 parents exceed the staged prefix sums: linear scan
+    (12, 300, "zeros"),      # zero badness in runs, some parents with none at all
+    (12, 300, "negative"),   # a negative badness: the CTA falls back to the linear scan
+])
+def test_mutation_roulette_paths_match_oracle(cuda, oracle, parents, population, badness):
+    """n3_beam_mutate through the C ABI against the oracle's restatement of the
+    mutation kernel, with the parents' badness given explicitly."""
+    import torch
+
+    from no_three_in_line_b200 import _lib
+
+    n, rng = 75, np.random.default_rng(parents + population)
+    states = [state.random_state(n, Random(300 + k)) for k in range(parents)]
+    pp = np.asarray([s.P for s in states], np.int32)
+    pq = np.asarray([s.Q for s in states], np.int32)
+    bad = rng.integers(0, 9, size=(parents, 2 * n)).astype(np.int32)
+    if badness == "zeros":
+        bad[:, 10:90] = 0
+        bad[::3] = 0
+    elif badness == "negative":
+        bad[5, 17] = -3
+    quality = max(1, parents // 4)
+    args = dict(quality_count=quality, population=population, active_strength=4, max_strength=9, bad_bias=85,
+                seed=2**40 + 77, generation=3)
+    ref_p, ref_q = oracle.beam_mutate(pp, pq, bad, **args)
+    dev = torch.device("cuda", 0)
+    dp, dq, db = (torch.from_numpy(x).to(dev) for x in (pp, pq, bad))
+    cp_ = torch.empty((population, n), dtype=torch.int32, device=dev)
+    cq_ = torch.empty_like(cp_)
+    _lib.call("n3_beam_mutate", _lib.ptr(dp), _lib.ptr(dq), _lib.ptr(db), parents, quality, n, population,
+              args["active_strength"], args["max_strength"], args["bad_bias"], args["seed"], args["generation"],
+              _lib.ptr(cp_), _lib.ptr(cq_), None)
+    assert np.array_equal(cp_.cpu().numpy(), ref_p) and np.array_equal(cq_.cpu().numpy(), ref_q)
+
+
 def run_device(initial_p, initial_q, extra, *, seed, generations, population, elite_size, max_strength,
                energy_window, bad_bias=85):
     """Generation by generation through DeviceBeam, reading the ranked elites back."""
