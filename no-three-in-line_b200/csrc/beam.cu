@@ -96,14 +96,19 @@ __global__ void __launch_bounds__(kMutThreads) mutate_kernel(const MutArgs A) {
   }
   s_parent[tid] = parent;
   bool use_prefix = parent_count <= A.prefix_cap;  // uniform
-  if (use_prefix) {  // warp w: parents w, w + 2, ...; a lane sums a run of `per` slots
+  if (use_prefix) {
+    const int count = parent_count * m;
+#pragma unroll 8
+    for (int i = tid; i < count; i += kMutThreads) prefix[i] = A.pbad[i];  // coalesced, loads in flight together
+    __syncthreads();
+    // in place, warp w: parents w, w + 2, ...; a lane sums its own run of `per` slots
     const int per = (m + 31) / 32, e0 = min(m, lane * per), e1 = min(m, e0 + per);
     bool negative = false;
     for (int p = warp; p < parent_count; p += kMutThreads / 32) {
-      const int32_t* bad = A.pbad + (size_t)p * m;
+      int32_t* row = prefix + p * m;
       int sum = 0;
       for (int e = e0; e < e1; ++e) {
-        const int b = bad[e];
+        const int b = row[e];
         negative |= b < 0 || b > 0x7fffffff / kMaxM;  // keeps every prefix sum below 2^31
         sum += b;
       }
@@ -114,12 +119,13 @@ __global__ void __launch_bounds__(kMutThreads) mutate_kernel(const MutArgs A) {
         if (lane >= o) incl += y;
       }
       int acc = incl - sum;
-      for (int e = e0; e < e1; ++e) prefix[p * m + e] = acc += bad[e];
+      for (int e = e0; e < e1; ++e) row[e] = acc += row[e];
     }
     use_prefix = !__syncthreads_or(negative);
   } else {
     __syncthreads();
   }
+#pragma unroll 4
   for (int i = tid; i < nc * m; i += kMutThreads) {  // the parents' rows into the children's
     const int c = i / m, s = i - c * m;
     const size_t at = (size_t)s_parent[c] * n + (s >> 1);
