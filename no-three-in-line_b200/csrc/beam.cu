@@ -14,9 +14,10 @@
 // The reference does the selection and ranking on the host with a copy of
 // every child's score each generation.  Here the selection is one CTA: a radix
 // select of the elite_size-th smallest score, a bitonic sort of the scores
-// below it, ordered compactions by per-warp counts, the shuffle's draws by one
-// warp (they must be exactly CPython's: the warp tries 32 steps per round), and
-// the first elite_size shuffled positions traced back through the draws.
+// below it, ordered compactions by per-warp counts, the MT19937 state blocks
+// twisted by the whole CTA, the shuffle's draws by one warp (they must be
+// exactly CPython's: the warp tries 32 steps per round), and the first
+// elite_size shuffled positions traced back through the draws.
 #include <stdint.h>
 
 #include "chain_move.cuh"
@@ -101,35 +102,29 @@ __global__ void __launch_bounds__(kMutThreads) mutate_kernel(const MutArgs A) {
 #pragma unroll 8
     for (int i = tid; i < count; i += kMutThreads) prefix[i] = A.pbad[i];  // coalesced, loads in flight together
     __syncthreads();
-    // in place, warp w: parents w, w + 2, ...; a lane sums its own run of `per` slots
-    const int per = (m + 31) / 32, e0 = min(m, lane * per), e1 = min(m, e0 + per);
     bool negative = false;
-    for (int p = warp; p < parent_count; p += kMutThreads / 32) {
+    for (int p = tid; p < parent_count; p += kMutThreads) {  // in place, a thread per parent
       int32_t* row = prefix + p * m;
-      int sum = 0;
-      for (int e = e0; e < e1; ++e) {
+      int acc = 0;
+#pragma unroll 10
+      for (int e = 0; e < m; ++e) {
         const int b = row[e];
         negative |= b < 0 || b > 0x7fffffff / kMaxM;  // keeps every prefix sum below 2^31
-        sum += b;
+        row[e] = acc += b;
       }
-      int incl = sum;
-#pragma unroll
-      for (int o = 1; o < 32; o <<= 1) {
-        const int y = __shfl_up_sync(0xffffffffu, incl, o);
-        if (lane >= o) incl += y;
-      }
-      int acc = incl - sum;
-      for (int e = e0; e < e1; ++e) row[e] = acc += row[e];
     }
     use_prefix = !__syncthreads_or(negative);
   } else {
     __syncthreads();
   }
-#pragma unroll 4
-  for (int i = tid; i < nc * m; i += kMutThreads) {  // the parents' rows into the children's
-    const int c = i / m, s = i - c * m;
-    const size_t at = (size_t)s_parent[c] * n + (s >> 1);
-    rows[i] = (s & 1) ? A.pq[at] : A.pp[at];
+  for (int c = warp; c < nc; c += kMutThreads / 32) {  // the parents' rows into the children's, a warp per child
+    const int32_t* src_p = A.pp + (size_t)s_parent[c] * n;
+    const int32_t* src_q = A.pq + (size_t)s_parent[c] * n;
+    int32_t* dst = rows + c * m;
+    for (int r = lane; r < n; r += 32) {
+      dst[2 * r] = src_p[r];
+      dst[2 * r + 1] = src_q[r];
+    }
   }
   __syncthreads();
   const bool record = A.child_moves != nullptr;
@@ -195,10 +190,14 @@ __global__ void __launch_bounds__(kMutThreads) mutate_kernel(const MutArgs A) {
     }
   }
   __syncthreads();
-  for (int i = tid; i < nc * n; i += kMutThreads) {  // coalesced: the CTA's rows are contiguous
-    const int c = i / n, r = i - c * n;
-    A.cp[(size_t)child0 * n + i] = rows[c * m + 2 * r];
-    A.cq[(size_t)child0 * n + i] = rows[c * m + 2 * r + 1];
+  for (int c = warp; c < nc; c += kMutThreads / 32) {  // coalesced rows, a warp per child
+    const int32_t* src = rows + c * m;
+    int32_t* dst_p = A.cp + (size_t)(child0 + c) * n;
+    int32_t* dst_q = A.cq + (size_t)(child0 + c) * n;
+    for (int r = lane; r < n; r += 32) {
+      dst_p[r] = src[2 * r];
+      dst_q[r] = src[2 * r + 1];
+    }
   }
 }
 
@@ -311,9 +310,7 @@ __device__ __forceinline__ uint32_t mt_temper(uint32_t y) {
 // coincide (a bit per position in `seen`, zero on entry and on return, finds
 // repeats), and are then made by all lanes at once, otherwise by lane 0 in step
 // order.  idx: position in the block (warp-uniform).
-// STORE: instead of swapping, record j of every step s in values[s] (T must
-// hold count - 1); the swaps are then traced back only for the positions needed.
-template <class T, bool STORE = false>
+template <class T>
 __device__ void py_shuffle_warp(uint32_t* mt, uint32_t* out, int& idx, T* values, int count, uint32_t* seen,
                                 int lane) {
   for (int k = lane; k < kMT; k += 32) out[k] = mt_temper(mt[k]);
@@ -356,12 +353,6 @@ __device__ void py_shuffle_warp(uint32_t* mt, uint32_t* out, int& idx, T* values
     }
     const int nb = __popc(acc_mask);
     const int s_max = i, s_min = s_max - nb + 1;
-    if (STORE) {
-      if ((acc_mask >> lane) & 1u) values[s_max - __popc(acc_mask & below)] = (T)r;
-      i -= nb;
-      idx += used;
-      continue;
-    }
     // an accepted draw swaps its step s = s_max - (accepted draws before it) with j = r;
     // a j inside [s_min, s_max] (other than s) or met twice orders the swaps
     const bool mine = (acc_mask >> lane) & 1u;
@@ -438,12 +429,74 @@ __global__ void py_shuffle_kernel(uint32_t* state, int32_t* values, int count) {
   for (int i = threadIdx.x; i < kMT; i += blockDim.x) state[i] = mt[i];
 }
 
+// The state twist by a whole CTA, out of place: dst = twist(src).  Word k of the
+// sequential in-place update reads the old words k, k + 1 and k + 397 (k < 227)
+// or the new word k - 227 (k >= 227; for k = 623 also the new word 0), so three
+// phases of at most 227 words each reproduce it.  Every thread calls it.
+__device__ __forceinline__ uint32_t mt_mix(uint32_t hi_word, uint32_t lo_word, uint32_t far) {
+  const uint32_t y = (hi_word & 0x80000000u) | (lo_word & 0x7fffffffu);
+  return far ^ (y >> 1) ^ ((y & 1u) ? 0x9908b0dfu : 0u);
+}
+
+__device__ void mt_twist_cta(const uint32_t* src, uint32_t* dst) {
+  const int t = threadIdx.x;
+  if (t < 227) dst[t] = mt_mix(src[t], src[t + 1], src[t + 397]);
+  __syncthreads();
+  if (t < 227) dst[227 + t] = mt_mix(src[227 + t], src[228 + t], dst[t]);
+  __syncthreads();
+  if (t < 170) {
+    const int k = 454 + t;
+    dst[k] = mt_mix(src[k], k == kMT - 1 ? dst[0] : src[k + 1], dst[k - 227]);
+  }
+  __syncthreads();
+}
+
+// The shuffle's draws by one warp, as py_shuffle_warp resolves them, from the
+// untempered state words words[0, avail) (consecutive blocks of the stream),
+// starting at word pos, for steps i, i - 1, ... >= 1: the j of step s goes to
+// jstep[s] and no swap is made.  Stops when the steps end or the words do (a
+// round near the end uses the words left); i and pos advance.
+__device__ void shuffle_draws_warp(const uint32_t* words, int avail, int& pos, int& i, uint16_t* jstep, int lane) {
+  const unsigned below = (1u << lane) - 1u;
+  while (i >= 1 && pos < avail) {
+    const int shift = __clz((uint32_t)i + 1u);
+    const int m = min(32, i + 2 - (1 << (31 - shift)));
+    const int draws = min(32, avail - pos);
+    uint32_t r = 0u;
+    bool acc = false, amb = false;
+    if (lane < draws) {
+      r = mt_temper(words[pos + lane]) >> shift;
+      acc = (int)r <= i - (m - 1);
+      amb = !acc && (int)r <= i;
+    }
+    const unsigned amb_mask = __ballot_sync(0xffffffffu, amb);
+    const int a = amb_mask ? __ffs(amb_mask) - 1 : draws;
+    unsigned acc_mask = __ballot_sync(0xffffffffu, acc) & ((a < 32 ? (1u << a) : 0u) - 1u);
+    int used = a;
+    if (__popc(acc_mask) < m && a < draws) {
+      const int sa = i - __popc(acc_mask);
+      if ((int)__shfl_sync(0xffffffffu, r, a) <= sa) acc_mask |= 1u << a;
+      used = a + 1;
+    }
+    if (__popc(acc_mask) >= m) {
+      const int z = __ffs(__ballot_sync(0xffffffffu, ((acc_mask >> lane) & 1u) &&
+                                                      __popc(acc_mask & ((2u << lane) - 1u)) == m)) - 1;
+      acc_mask &= (2u << z) - 1u;
+      used = z + 1;
+    }
+    if ((acc_mask >> lane) & 1u) jstep[i - __popc(acc_mask & below)] = (uint16_t)r;
+    i -= __popc(acc_mask);
+    pos += used;
+  }
+}
+
 // --------------------------------------------------------------------------
 // Selection (one CTA of kSelThreads threads).
 // --------------------------------------------------------------------------
 constexpr int kSelThreads = 1024;
 constexpr int kMaxPopulation = 65536;
 constexpr int kMaxElite = 2048;
+constexpr int kSelBatch = 16;  // MT state blocks generated per batch for the shuffle's draws
 
 constexpr int kSelWarps = kSelThreads / 32;
 static_assert(kSelWarps == 32, "the per-warp offsets are scanned by one warp, one lane per warp");
@@ -468,11 +521,11 @@ __global__ void __launch_bounds__(kSelThreads, 1) select_kernel(const SelArgs A)
   uint32_t* mt = reinterpret_cast<uint32_t*>(keys + kMaxElite);       // [624]
   int32_t* order = reinterpret_cast<int32_t*>(mt + kMT);              // [kMaxElite] score-order prefix
   uint32_t* mark = reinterpret_cast<uint32_t*>(order + kMaxElite);    // [kMaxPopulation / 32]
-  uint16_t* jstep = reinterpret_cast<uint16_t*>(mark + kMaxPopulation / 32);  // [population] j of shuffle step s
+  uint32_t* words = mark + kMaxPopulation / 32;                        // [kSelBatch][624] untempered MT blocks
+  uint16_t* jstep = reinterpret_cast<uint16_t*>(words + kSelBatch * kMT);  // [population] j of shuffle step s
   __shared__ uint32_t hist[256];
   __shared__ int tie_off[kSelWarps], win_off[kSelWarps];
   __shared__ int s_misc[4];
-  __shared__ uint32_t mt_out[kMT];  // tempered outputs of the current state block
   if (A.status[1] == 0) return;  // uniform: the search has reached E = 0
   const int64_t limit = A.status[1] + (int64_t)A.energy_window;
   for (int i = tid; i < kMaxPopulation / 32; i += kSelThreads) mark[i] = 0u;
@@ -607,12 +660,39 @@ __global__ void __launch_bounds__(kSelThreads, 1) select_kernel(const SelArgs A)
   }
   for (int i = tid; i < n_less; i += kSelThreads) order[i] = (int32_t)(uint32_t)keys[i];
 
-  // 4. warp 0 draws the shuffle of the window list (gpu_device_search.py:340-373):
-  //    the j of every step s, jstep[s]; the swaps themselves are not applied
-  if (warp == 0) {
-    int idx = (int)A.rng[kMT];
-    py_shuffle_warp<uint16_t, true>(mt, mt_out, idx, jstep, n_window, mark, lane);
-    if (lane == 0) A.rng[kMT] = (uint32_t)idx;
+  // 4. the draws of the window list's shuffle (gpu_device_search.py:340-373):
+  //    the j of every step s in jstep[s], no swap made.  The CTA twists the MT
+  //    state blocks kSelBatch at a time; warp 0 resolves the draws from them.
+  //    The state left is the block of the last draw, as CPython leaves it.
+  int steps_left = n_window - 1;  // uniform
+  if (steps_left >= 1) {
+    int pos = (int)A.rng[kMT];
+    if (pos < kMT) {
+      for (int k = tid; k < kMT; k += kSelThreads) words[k] = mt[k];
+      __syncthreads();
+    } else {  // the current block is used up: the first draw twists
+      mt_twist_cta(mt, words);
+      pos = 0;
+    }
+    for (;;) {
+      for (int g = 1; g < kSelBatch; ++g) mt_twist_cta(words + (g - 1) * kMT, words + g * kMT);
+      if (warp == 0) {
+        shuffle_draws_warp(words, kSelBatch * kMT, pos, steps_left, jstep, lane);
+        if (lane == 0) {
+          s_misc[0] = steps_left;
+          s_misc[1] = pos;
+        }
+      }
+      __syncthreads();
+      steps_left = s_misc[0];
+      pos = s_misc[1];
+      if (steps_left < 1) break;  // uniform
+      mt_twist_cta(words + (kSelBatch - 1) * kMT, words);  // the next batch starts after the last block
+      pos = 0;
+    }
+    const int last = pos - 1;  // >= 0: every round uses at least one draw
+    for (int k = tid; k < kMT; k += kSelThreads) mt[k] = words[(last / kMT) * kMT + k];
+    if (tid == 0) A.rng[kMT] = (uint32_t)(last % kMT + 1);
   }
   __syncthreads();
 
@@ -685,7 +765,9 @@ __global__ void __launch_bounds__(kSelThreads, 1) select_kernel(const SelArgs A)
 }
 
 constexpr size_t kSelSmem = sizeof(uint64_t) * kMaxElite + sizeof(uint32_t) * kMT + sizeof(int32_t) * kMaxElite +
-                            sizeof(uint32_t) * (kMaxPopulation / 32) + sizeof(uint16_t) * kMaxPopulation;
+                            sizeof(uint32_t) * (kMaxPopulation / 32) + sizeof(uint32_t) * kSelBatch * kMT +
+                            sizeof(uint16_t) * kMaxPopulation;
+static_assert(kSelSmem <= 227 * 1024 - 2048, "select_kernel shared memory");
 
 // pick rows r = child rows selected[r]
 __global__ void gather_kernel(const int32_t* __restrict__ cp, const int32_t* __restrict__ cq,
