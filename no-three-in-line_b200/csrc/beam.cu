@@ -452,23 +452,20 @@ __device__ void mt_twist_cta(const uint32_t* src, uint32_t* dst) {
 }
 
 // The shuffle's draws by one warp, as py_shuffle_warp resolves them, from the
-// untempered state words words[0, avail) (consecutive blocks of the stream),
-// starting at word pos, for steps i, i - 1, ... >= 1: the j of step s goes to
-// jstep[s] and no swap is made.  Stops when the steps end or the words do (a
-// round near the end uses the words left); i and pos advance.
-__device__ void shuffle_draws_warp(const uint32_t* words, int avail, int& pos, int& i, uint16_t* jstep, int lane) {
+// tempered outputs out[0, avail) (consecutive blocks of the stream; out holds 32
+// more words, read and ignored), starting at output pos, for steps i, i - 1,
+// ... >= 1: the j of step s goes to jstep[s] and no swap is made.  Stops when
+// the steps end or the outputs do (a round near the end uses the outputs left);
+// i and pos advance.
+__device__ void shuffle_draws_warp(const uint32_t* out, int avail, int& pos, int& i, uint16_t* jstep, int lane) {
   const unsigned below = (1u << lane) - 1u;
   while (i >= 1 && pos < avail) {
     const int shift = __clz((uint32_t)i + 1u);
     const int m = min(32, i + 2 - (1 << (31 - shift)));
     const int draws = min(32, avail - pos);
-    uint32_t r = 0u;
-    bool acc = false, amb = false;
-    if (lane < draws) {
-      r = mt_temper(words[pos + lane]) >> shift;
-      acc = (int)r <= i - (m - 1);
-      amb = !acc && (int)r <= i;
-    }
+    const uint32_t r = out[pos + lane] >> shift;
+    const bool acc = lane < draws && (int)r <= i - (m - 1);
+    const bool amb = lane < draws && !acc && (int)r <= i;
     const unsigned amb_mask = __ballot_sync(0xffffffffu, amb);
     const int a = amb_mask ? __ffs(amb_mask) - 1 : draws;
     unsigned acc_mask = __ballot_sync(0xffffffffu, acc) & ((a < 32 ? (1u << a) : 0u) - 1u);
@@ -496,7 +493,7 @@ __device__ void shuffle_draws_warp(const uint32_t* words, int avail, int& pos, i
 constexpr int kSelThreads = 1024;
 constexpr int kMaxPopulation = 65536;
 constexpr int kMaxElite = 2048;
-constexpr int kSelBatch = 16;  // MT state blocks generated per batch for the shuffle's draws
+constexpr int kSelBatch = 8;  // MT state blocks generated per batch for the shuffle's draws
 
 constexpr int kSelWarps = kSelThreads / 32;
 static_assert(kSelWarps == 32, "the per-warp offsets are scanned by one warp, one lane per warp");
@@ -508,6 +505,19 @@ struct SelArgs {
   uint32_t* rng;          // [625]
   int32_t* selected;      // [elite_size]
 };
+
+// One group of 32 steps b .. b + 31 (lane l holds j of step b + l, or -1) in
+// the trace back of one shuffled position: the item moves to every step whose
+// j equals its position, in step order.
+__device__ __forceinline__ int trace_group(int js, int b, int pos, int lane) {
+  unsigned hit = __ballot_sync(0xffffffffu, js == pos);
+  while (hit) {  // uniform
+    const int f = __ffs(hit) - 1;
+    pos = b + f;
+    hit = __ballot_sync(0xffffffffu, js == pos) & ~((2u << f) - 1u);
+  }
+  return pos;
+}
 
 // Warp w owns the children [w * seg, (w + 1) * seg) (seg a multiple of 32) and
 // reads them 32 at a time, so every pass over the scores is coalesced and every
@@ -522,7 +532,8 @@ __global__ void __launch_bounds__(kSelThreads, 1) select_kernel(const SelArgs A)
   int32_t* order = reinterpret_cast<int32_t*>(mt + kMT);              // [kMaxElite] score-order prefix
   uint32_t* mark = reinterpret_cast<uint32_t*>(order + kMaxElite);    // [kMaxPopulation / 32]
   uint32_t* words = mark + kMaxPopulation / 32;                        // [kSelBatch][624] untempered MT blocks
-  uint16_t* jstep = reinterpret_cast<uint16_t*>(words + kSelBatch * kMT);  // [population] j of shuffle step s
+  uint32_t* tw = words + kSelBatch * kMT;                              // [kSelBatch * 624 + 32] their outputs
+  uint16_t* jstep = reinterpret_cast<uint16_t*>(tw + kSelBatch * kMT + 32);  // [population] j of shuffle step s
   __shared__ uint32_t hist[256];
   __shared__ int tie_off[kSelWarps], win_off[kSelWarps];
   __shared__ int s_misc[4];
@@ -674,10 +685,13 @@ __global__ void __launch_bounds__(kSelThreads, 1) select_kernel(const SelArgs A)
       mt_twist_cta(mt, words);
       pos = 0;
     }
+    if (tid < 32) tw[kSelBatch * kMT + tid] = 0u;  // the padding a last round reads
     for (;;) {
       for (int g = 1; g < kSelBatch; ++g) mt_twist_cta(words + (g - 1) * kMT, words + g * kMT);
+      for (int k = tid; k < kSelBatch * kMT; k += kSelThreads) tw[k] = mt_temper(words[k]);
+      __syncthreads();
       if (warp == 0) {
-        shuffle_draws_warp(words, kSelBatch * kMT, pos, steps_left, jstep, lane);
+        shuffle_draws_warp(tw, kSelBatch * kMT, pos, steps_left, jstep, lane);
         if (lane == 0) {
           s_misc[0] = steps_left;
           s_misc[1] = pos;
@@ -706,15 +720,18 @@ __global__ void __launch_bounds__(kSelThreads, 1) select_kernel(const SelArgs A)
   int32_t* picked = reinterpret_cast<int32_t*>(keys);  // [K]; keys is free once order is written
   for (int p = warp; p < K; p += kSelWarps) {
     int pos = p == 0 ? 0 : (int)jstep[p];
-    for (int b = p + 1; b < n_window; b += 32) {
+    int b = p + 1;
+    for (; b + 128 <= n_window; b += 128) {  // four groups of 32 steps, loaded together
+      const int j0 = jstep[b + lane], j1 = jstep[b + 32 + lane], j2 = jstep[b + 64 + lane],
+                j3 = jstep[b + 96 + lane];
+      pos = trace_group(j0, b, pos, lane);
+      pos = trace_group(j1, b + 32, pos, lane);
+      pos = trace_group(j2, b + 64, pos, lane);
+      pos = trace_group(j3, b + 96, pos, lane);
+    }
+    for (; b < n_window; b += 32) {
       const int st = b + lane;
-      const int js = st < n_window ? (int)jstep[st] : -1;
-      unsigned hit = __ballot_sync(0xffffffffu, js == pos);
-      while (hit) {  // uniform
-        const int f = __ffs(hit) - 1;
-        pos = b + f;
-        hit = __ballot_sync(0xffffffffu, js == pos) & ~((2u << f) - 1u);
-      }
+      pos = trace_group(st < n_window ? (int)jstep[st] : -1, b, pos, lane);
     }
     const unsigned owners = __ballot_sync(0xffffffffu, win_off[lane] <= pos);  // bit 0 always set
     const int w = 31 - __clz(owners);
@@ -765,7 +782,7 @@ __global__ void __launch_bounds__(kSelThreads, 1) select_kernel(const SelArgs A)
 }
 
 constexpr size_t kSelSmem = sizeof(uint64_t) * kMaxElite + sizeof(uint32_t) * kMT + sizeof(int32_t) * kMaxElite +
-                            sizeof(uint32_t) * (kMaxPopulation / 32) + sizeof(uint32_t) * kSelBatch * kMT +
+                            sizeof(uint32_t) * (kMaxPopulation / 32) + sizeof(uint32_t) * (2 * kSelBatch * kMT + 32) +
                             sizeof(uint16_t) * kMaxPopulation;
 static_assert(kSelSmem <= 227 * 1024 - 2048, "select_kernel shared memory");
 
