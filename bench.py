@@ -56,7 +56,7 @@ def parse():
     ap.add_argument("--impl", choices=["b200", "reference"], default="b200")
     ap.add_argument("--states", type=int, default=STATES)
     ap.add_argument("--mode", choices=["checked", "det", "slope", "tempering", "learned", "time-to-target", "beam",
-                                       "scan"],
+                                       "scan", "lines"],
                     default="checked",
                     help="kernel a step runs: fused checked scoring (default), determinant only, slope only; "
                          "tempering / learned chain rounds; one device beam-search generation (beam); one "
@@ -358,6 +358,72 @@ def run_search_mode(args):
     return 0
 
 
+def run_lines_mode(args):
+    """--mode lines: the line tables of the 75 x 75 grid (precompute.py:35-57)
+    built once on the device (timed alone), then one step = score_pair_table and
+    score_csr (:60-89) of 4096 seeded n = 75 states, inputs resident in HBM."""
+    import torch
+
+    from no_three_in_line_b200 import _lib, precompute, state
+
+    _lib.require_device()
+    stream = torch.cuda.current_stream()
+    t0, t1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    precompute.build_geometry_tables(N)  # warm-up: module load, allocator
+    torch.cuda.synchronize()
+    t0.record(stream)
+    tables = precompute.build_geometry_tables(N)
+    t1.record(stream)
+    t1.synchronize()
+    build_ms = t0.elapsed_time(t1)
+    p, q = state.seeded_population(N, args.states)
+    ids = np.concatenate(precompute._population_ids(p, q, N))
+    dev = torch.device("cuda")
+    d_ids = torch.from_numpy(ids).to(dev)
+    d_starts = torch.arange(0, 2 * N * (args.states + 1), 2 * N, dtype=torch.int64, device=dev)
+    d = tables.device
+    pair_scores = torch.empty(args.states, dtype=torch.int64, device=dev)
+    csr_scores = torch.empty_like(pair_scores)
+    occ = torch.empty(((args.states + 31) // 32) * N * N, dtype=torch.int32, device=dev)
+    err = torch.zeros(2, dtype=torch.int32, device=dev)
+    L = _lib.lib()
+    sp = int(stream.cuda_stream)
+
+    def step():
+        _lib.check(L.n3_lines_score_pairs(d_ids.data_ptr(), d_starts.data_ptr(), args.states, N,
+                                          d.pair_to_line.data_ptr(), pair_scores.data_ptr(), err.data_ptr(), sp),
+                   "n3_lines_score_pairs")
+        _lib.check(L.n3_lines_score_csr(d_ids.data_ptr(), d_starts.data_ptr(), args.states, N, tables.line_count,
+                                        d.offsets.data_ptr(), d.indices.data_ptr(), occ.data_ptr(),
+                                        csr_scores.data_ptr(), err.data_ptr() + 4, sp), "n3_lines_score_csr")
+
+    for _ in range(max(3, args.warmup)):
+        step()
+    torch.cuda.synchronize()
+    want = np.asarray(__import__("no_three_in_line_b200.gpu", fromlist=["gpu"]).score_population_gpu(p, q))
+    if not (np.array_equal(pair_scores.cpu().numpy(), want) and np.array_equal(csr_scores.cpu().numpy(), want)
+            and int(err.abs().sum()) == 0):
+        raise AssertionError("line-table scores differ from the determinant scores")
+    start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with ClockSampler(torch.cuda.current_device()) as clocks:
+        start.record(stream)
+        for _ in range(args.steps):
+            step()
+        end.record(stream)
+        end.synchronize()
+    secs = start.elapsed_time(end) / 1e3
+    line = {"metric": METRIC, "value": args.states * args.steps / secs, "unit": "states/s", "n_gpus": 1,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * secs / args.steps,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "int32",
+            "data": "synthetic: random_state(75, Random(91001+i)) states",
+            "config": {"workload": f"n=75 line tables: score_pair_table + score_csr of {args.states} states",
+                       "mode": "lines", "line_count": tables.line_count, "line_incidences": int(len(tables.indices)),
+                       "pair_table_bytes": int(tables.pair_to_line.nbytes)},
+            "table_build_ms_with_host_copies": build_ms, "gpu_launches": 3 * args.steps, "clocks": clocks.summary()}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
 def run_time_to_target(args):
     from no_three_in_line_b200 import compare
 
@@ -621,7 +687,7 @@ def main():
     if args.mode in ("tempering", "learned"):
         return run_chain_mode(args)
     if args.mode in ("beam", "scan"):
-        return run_search_mode(args)
+        return run_search_mode(args) if args.mode != "lines" else run_lines_mode(args)
     return run_b200(args)
 
 

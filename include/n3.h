@@ -311,6 +311,44 @@ int n3_weighted_state_scores(const int32_t* p, const int32_t* q, int B, int n, c
                              void* stream);
 
 /* ---------------------------------------------------------------------------
+ * Line tables of the n x n grid (src/no_three_75/precompute.py:18-57,
+ * build_geometry_tables, over src/no_three_75/cp_sat.py:109-157,
+ * _multi_point_lines on the whole grid): every line with three or more grid
+ * points that is neither a row nor a column, numbered as the reference numbers
+ * it; members listed in row-major order (point id = row * n + column).
+ * 1 <= n <= N3_MAX_N.  Built in two calls: the sizes, then the tables.
+ * ------------------------------------------------------------------------- */
+
+/* The lines whose first (row-major) member is each point.  line_at,
+ * incidence_at: device int64 [n*n + 1], left as exclusive scans (the first
+ * line id and the first CSR position of each point's lines); totals: HOST
+ * int64 [2] = {line count, total incidences}.  Synchronises the stream. */
+int n3_line_tables_count(int n, int64_t* line_at, int64_t* incidence_at, int64_t* totals, void* stream);
+
+/* The tables of GeometryTables: offsets int64 [line_count + 1] (CSR),
+ * indices int32 [incidences], pair_to_line int32 [n*n (n*n - 1) / 2] (the
+ * line of each unordered pair of grid points in triangular_pair_index order,
+ * precompute.py:28-33, or -1). */
+int n3_line_tables_build(int n, const int64_t* line_at, const int64_t* incidence_at, int64_t line_count,
+                         int64_t* offsets, int32_t* indices, int32_t* pair_to_line, void* stream);
+
+/* score_pair_table (precompute.py:60-81) for `lists` point lists: list i holds
+ * point ids ids[starts[i] .. starts[i+1]) (at most 512 points, ids distinct and
+ * in [0, n*n)); scores int64 [lists] = sum over the table's lines of C(k, 3).
+ * error_word (device uint32) gets bit 0 for an id out of range, bit 1 for an id
+ * listed twice (the reference raises ValueError for both). */
+int n3_lines_score_pairs(const int32_t* ids, const int64_t* starts, int lists, int n, const int32_t* pair_to_line,
+                         int64_t* scores, uint32_t* error_word, void* stream);
+
+/* score_csr (precompute.py:84-89) for `lists` point lists (any size; a point
+ * listed twice counts once).  occupancy: device uint32 scratch
+ * [ceil(lists / 32)][n*n]; scores int64 [lists]; error_word bit 0 for an id
+ * out of [0, n*n). */
+int n3_lines_score_csr(const int32_t* ids, const int64_t* starts, int lists, int n, int64_t line_count,
+                       const int64_t* offsets, const int32_t* indices, uint32_t* occupancy, int64_t* scores,
+                       uint32_t* error_word, void* stream);
+
+/* ---------------------------------------------------------------------------
  * Device-resident beam search: the generation loop of
  * src/no_three_75/gpu_device_search.py:254-432 (gpu_device_beam_search) with
  * mutation, scoring, selection (including its random.Random shuffle) and

@@ -407,3 +407,102 @@ def weighted_state_score(p, q, raw_score: int, keys, vals) -> int:
             continue
         value += int((w - 1) * _c3(int(np.count_nonzero(a * rows + b * cols + c == 0))))
     return value
+
+
+# --------------------------------------------------------------------------
+# Line tables (precompute.py:18-94).  Pure NumPy restatements.
+# --------------------------------------------------------------------------
+def triangular_pair_index(left: int, right: int, point_count: int) -> int:
+    """precompute.py:28-33: index of the unordered pair {left, right} in the
+    row-major upper triangle of point_count x point_count."""
+    if left > right:
+        left, right = right, left
+    if left == right or left < 0 or right >= point_count:
+        raise ValueError("pair index requires two distinct in-range points")
+    return left * (2 * point_count - left - 1) // 2 + right - left - 1
+
+
+def geometry_tables(n: int) -> dict:
+    """build_geometry_tables (precompute.py:35-57) over the lines that
+    _multi_point_lines (cp_sat.py:129-157) finds on the whole grid: every line
+    with three or more grid points that is neither a row nor a column (pairs in
+    one row or column are skipped there).  A line enters the reference's dict at
+    its second pair, (first member, third member) in the row-major pair loop, so
+    the line ids follow (first member, third member).  For one first member the
+    third is (r0 + 2a, c0 + 2b) for the line's primitive step (a >= 1, b != 0),
+    so the order is that of (a, b).  Members are listed in row-major order."""
+    from math import gcd
+
+    N = n * n
+    rr, cc = np.divmod(np.arange(N), n)
+    recs = []  # (first member, a, b, length)
+    for a in range(1, n):
+        for b in range(-(n - 1), n):
+            if b == 0 or gcd(a, abs(b)) != 1:
+                continue
+            start = ~((rr - a >= 0) & (cc - b >= 0) & (cc - b < n))  # no grid point before
+            third = (rr + 2 * a < n) & (cc + 2 * b >= 0) & (cc + 2 * b < n)
+            sel = np.nonzero(start & third)[0]
+            if len(sel) == 0:
+                continue
+            steps_r = (n - 1 - rr[sel]) // a
+            steps_c = (n - 1 - cc[sel]) // b if b > 0 else cc[sel] // (-b)
+            length = 1 + np.minimum(steps_r, steps_c)
+            recs.append(np.stack([sel, np.full_like(sel, a), np.full_like(sel, b), length], 1))
+    if recs:
+        lines = np.concatenate(recs)
+        lines = lines[np.lexsort((lines[:, 2], lines[:, 1], lines[:, 0]))]
+    else:
+        lines = np.zeros((0, 4), np.int64)
+    lengths = lines[:, 3]
+    offsets = np.zeros(len(lines) + 1, np.int64)
+    np.cumsum(lengths, out=offsets[1:])
+    indices = np.empty(int(offsets[-1]), np.int32)
+    pair_to_line = np.full(N * (N - 1) // 2, -1, np.int32)
+    for k in np.unique(lengths):
+        ids = np.nonzero(lengths == k)[0]
+        t = np.arange(k)
+        r = rr[lines[ids, 0]][:, None] + lines[ids, 1][:, None] * t
+        c = cc[lines[ids, 0]][:, None] + lines[ids, 2][:, None] * t
+        members = r * n + c  # increasing along the line (a >= 1)
+        indices[(offsets[ids][:, None] + t).ravel()] = members.ravel()
+        i, j = np.triu_indices(k, 1)
+        left, right = members[:, i], members[:, j]
+        tri = left * (2 * N - left - 1) // 2 + right - left - 1
+        pair_to_line[tri.ravel()] = np.repeat(ids, len(i)).astype(np.int32)
+    return {"n": n, "pair_to_line": pair_to_line, "offsets": offsets, "indices": indices, "line_count": len(lines)}
+
+
+def score_pair_table(points, tables: dict) -> int:
+    """precompute.py:60-81: sum of C(k, 3) over the table's lines from the
+    pair counts of the points' pairs."""
+    from itertools import combinations
+    from math import comb, isqrt
+
+    n = tables["n"]
+    ids = sorted(row * n + column for row, column in points)
+    N = n * n
+    pairs = np.fromiter((triangular_pair_index(a, b, N) for a, b in combinations(ids, 2)), dtype=np.int64)
+    line_ids = tables["pair_to_line"][pairs]
+    line_ids = line_ids[line_ids >= 0]
+    score = 0
+    for count in np.unique(line_ids, return_counts=True)[1]:
+        d = 1 + 8 * int(count)
+        root = isqrt(d)
+        if root * root != d:
+            raise AssertionError("selected pair count is not triangular")
+        k = (1 + root) // 2
+        score += comb(k, 3) if k >= 3 else 0
+    return score
+
+
+def score_csr(points, tables: dict) -> int:
+    """precompute.py:84-89: occupancy summed over each line's members."""
+    n = tables["n"]
+    occupied = np.zeros(n * n, dtype=np.int8)
+    occupied[[row * n + column for row, column in points]] = 1
+    if tables["line_count"] == 0:
+        return 0
+    counts = np.add.reduceat(occupied[tables["indices"]], tables["offsets"][:-1]).astype(np.int64)
+    counts = counts[counts >= 3]
+    return int(np.sum(counts * (counts - 1) * (counts - 2) // 6))
