@@ -336,7 +336,8 @@ int n3_line_tables_build(int n, const int64_t* line_at, const int64_t* incidence
  * point ids ids[starts[i] .. starts[i+1]) (at most 512 points, ids distinct and
  * in [0, n*n)); scores int64 [lists] = sum over the table's lines of C(k, 3).
  * error_word (device uint32) gets bit 0 for an id out of range, bit 1 for an id
- * listed twice (the reference raises ValueError for both). */
+ * listed twice (the reference raises ValueError for both), bit 2 if a list's
+ * lines overflow the per-warp hash (not possible within 512 points). */
 int n3_lines_score_pairs(const int32_t* ids, const int64_t* starts, int lists, int n, const int32_t* pair_to_line,
                          int64_t* scores, uint32_t* error_word, void* stream);
 

@@ -37,7 +37,7 @@ _lib.register("n3_lines_score_csr", [_lib._P, _lib._P, _lib._I, _lib._I, _lib._I
                                      _lib._P, _lib._P, _lib._P])
 
 MAX_PAIR_POINTS = 512  # points per list that the device pair-table scorer takes
-_ERR_RANGE, _ERR_TWICE = 1, 2
+_ERR_RANGE, _ERR_TWICE, _ERR_HASH = 1, 2, 4  # error-word bits of n3_lines_score_pairs
 
 
 @dataclass(frozen=True)
@@ -129,8 +129,10 @@ def _run_pairs(id_lists: list[np.ndarray], n: int, tables: GeometryTables) -> np
               _lib.ptr(d.pair_to_line) if d.pair_to_line.numel() else None, _lib.ptr(scores), _lib.ptr(err),
               _lib.stream_ptr())
     code = int(err.item())
-    if code:
+    if code & (_ERR_RANGE | _ERR_TWICE):
         raise ValueError("pair index requires two distinct in-range points")
+    if code:
+        raise RuntimeError(f"pair-table scorer: error word {code:#x}")
     return scores.cpu().numpy()
 
 
