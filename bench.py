@@ -60,8 +60,8 @@ def parse():
                     default="checked",
                     help="kernel a step runs: fused checked scoring (default), determinant only, slope only; "
                          "tempering / learned chain rounds; one device beam-search generation (beam); one "
-                         "four-cycle + double-switch neighbourhood scan (scan); or the learned-vs-plain "
-                         "time-to-target comparison")
+                         "four-cycle + double-switch neighbourhood scan (scan); the n = 75 line tables "
+                         "and both table scorers (lines); or the learned-vs-plain time-to-target comparison")
     ap.add_argument("--no-secondary", action="store_true", help="skip the delta/tempering/MLP measurements")
     ap.add_argument("--seeds", type=int, default=3, help="time-to-target: seeds per method")
     ap.add_argument("--budget", type=float, default=30.0, help="time-to-target: device seconds per run")
@@ -364,7 +364,7 @@ def run_lines_mode(args):
     score_csr (:60-89) of 4096 seeded n = 75 states, inputs resident in HBM."""
     import torch
 
-    from no_three_in_line_b200 import _lib, precompute, state
+    from no_three_in_line_b200 import _lib, gpu, precompute, state
 
     _lib.require_device()
     stream = torch.cuda.current_stream()
@@ -400,7 +400,7 @@ def run_lines_mode(args):
     for _ in range(max(3, args.warmup)):
         step()
     torch.cuda.synchronize()
-    want = np.asarray(__import__("no_three_in_line_b200.gpu", fromlist=["gpu"]).score_population_gpu(p, q))
+    want = np.asarray(gpu.score_population_gpu(p, q))
     if not (np.array_equal(pair_scores.cpu().numpy(), want) and np.array_equal(csr_scores.cpu().numpy(), want)
             and int(err.abs().sum()) == 0):
         raise AssertionError("line-table scores differ from the determinant scores")
