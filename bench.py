@@ -687,7 +687,9 @@ def main():
     if args.mode in ("tempering", "learned"):
         return run_chain_mode(args)
     if args.mode in ("beam", "scan"):
-        return run_search_mode(args) if args.mode != "lines" else run_lines_mode(args)
+        return run_search_mode(args)
+    if args.mode == "lines":
+        return run_lines_mode(args)
     return run_b200(args)
 
 
