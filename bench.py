@@ -165,6 +165,25 @@ def cpu_baseline(p, q, threads: int):
                       f"{threads} threads, {dt:.2f} s"}
 
 
+def lines_cpu_baseline(tables, p, q, sample: int = 8):
+    """score_pair_table + score_csr (precompute.py:60-89, restated in NumPy in
+    oracle/) on the first `sample` states, one host thread."""
+    from oracle import oracle
+
+    t = {"n": tables.n, "pair_to_line": tables.pair_to_line, "offsets": tables.offsets, "indices": tables.indices,
+         "line_count": tables.line_count}
+    n = tables.n
+    pts = [[(r, int(p[b, r])) for r in range(n)] + [(r, int(q[b, r])) for r in range(n)] for b in range(sample)]
+    t0 = time.perf_counter()
+    for x in pts:
+        oracle.score_pair_table(x, t)
+        oracle.score_csr(x, t)
+    dt = time.perf_counter() - t0
+    return {"value": sample / dt, "unit": "states/s", "cores": 1, "kind": "port",
+            "sample": f"{sample} n=75 states, score_pair_table + score_csr (precompute.py:60-89 restated in NumPy), "
+                      f"1 thread, {dt:.2f} s"}
+
+
 def secondary_measurements(dev, p, q):
     """Swap deltas/s and tempering / learned-proposal throughput at the
     configurations of the metric, each timed with CUDA events after warm-up."""
@@ -419,7 +438,8 @@ def run_lines_mode(args):
             "config": {"workload": f"n=75 line tables: score_pair_table + score_csr of {args.states} states",
                        "mode": "lines", "line_count": tables.line_count, "line_incidences": int(len(tables.indices)),
                        "pair_table_bytes": int(tables.pair_to_line.nbytes)},
-            "table_build_ms_with_host_copies": build_ms, "gpu_launches": 3 * args.steps, "clocks": clocks.summary()}
+            "table_build_ms_with_host_copies": build_ms, "gpu_launches": 3 * args.steps, "clocks": clocks.summary(),
+            "cpu_baseline": lines_cpu_baseline(tables, p, q)}
     print(json.dumps(line), flush=True)
     return 0
 
