@@ -65,8 +65,8 @@ struct MutArgs {
 // prefix exceeds t, which the search finds.  A negative badness anywhere, or
 // one large enough for a sum to overflow (neither is a state's badness), sends
 // the CTA back to the linear scan, so every draw and result stays the
-// reference's for any input.  The parent's total badness is
-// taken once per child instead of once per attempt (it does not change).
+// reference's for any input.  The parent's total badness is taken once per
+// child instead of once per attempt (it does not change).
 constexpr int kMutThreads = 64;
 constexpr size_t kMutPrefixMaxBytes = 96 * 1024;
 
@@ -672,8 +672,9 @@ __global__ void __launch_bounds__(kSelThreads, 1) select_kernel(const SelArgs A)
   for (int i = tid; i < n_less; i += kSelThreads) order[i] = (int32_t)(uint32_t)keys[i];
 
   // 4. the draws of the window list's shuffle (gpu_device_search.py:340-373):
-  //    the j of every step s in jstep[s], no swap made.  The CTA twists the MT
-  //    state blocks kSelBatch at a time; warp 0 resolves the draws from them.
+  //    the j of every step s in jstep[s], no swap made.  The CTA twists and
+  //    tempers the MT state blocks kSelBatch at a time; warp 0 resolves the
+  //    draws from the tempered words.
   //    The state left is the block of the last draw, as CPython leaves it.
   int steps_left = n_window - 1;  // uniform
   if (steps_left >= 1) {
