@@ -13,7 +13,8 @@ buffers (pinned H2D of the step's columns, D2H of its scores and flags).
 Under torchrun each rank scores its own population (weak scaling, no
 data-path collective); the step time is the max over ranks.
 ``--impl reference`` times the reference's CPU algorithm (the C restatement
-in oracle/, all host threads) on the same workload and metric.
+in oracle/, all host threads) on the same workload and metric: determinant
+count, slope line count with badness, and their comparison per state.
 """
 from __future__ import annotations
 
@@ -150,19 +151,71 @@ def measured_peaks():
     return {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0}, "fallback"
 
 
-def cpu_baseline(p, q, threads: int):
-    """The reference's CPU scoring algorithm (accelerated.py:14-37, restated in
-    oracle/) over the same states on all host threads."""
+def host_threads() -> int:
+    """Host threads this process may run on (its CPU affinity)."""
+    try:
+        return len(os.sched_getaffinity(0))
+    except AttributeError:  # not Linux
+        return os.cpu_count() or 1
+
+
+def host_description() -> dict:
+    model = "unknown"
+    try:
+        for ln in Path("/proc/cpuinfo").read_text().splitlines():
+            if ln.startswith("model name"):
+                model = ln.split(":", 1)[1].strip()
+                break
+    except OSError:
+        pass
+    return {"cpu": model, "nproc": os.cpu_count(), "affinity_threads": host_threads()}
+
+
+def cpu_checked_pass(p, q, threads: int) -> int:
+    """One CPU pass of the GPU step's work on the host: the reference's
+    determinant count (accelerated.py:14-37) and its normalised-slope line
+    count with badness (verifier_b.py:8-19 counted as conflicts.py:36-72 sums),
+    both restated in C in oracle/, then the per-state comparison.  Returns the
+    number of states whose counts differ."""
     from oracle import oracle
 
-    oracle.score_population(p[:8], q[:8], threads=1)  # load
-    sample = min(len(p), 4096)
+    det = oracle.score_population(p, q, threads=threads)
+    slope, _ = oracle.slope_population(p, q, threads=threads)
+    return int(np.count_nonzero(det != slope))
+
+
+def cpu_reference_rate(p, q, *, threads: int, steps: int, warmup: int, step_seconds: float = 0.5) -> dict:
+    """The CPU timing used by both the GPU arm's ``cpu_baseline`` and the
+    ``--impl reference`` arm: the sample per step is sized to about
+    ``step_seconds`` of work at this thread count, ``warmup`` untimed passes
+    come first, then ``steps`` timed passes over consecutive samples."""
+    cpu_checked_pass(p[:8], q[:8], 1)  # load the library
     t0 = time.perf_counter()
-    oracle.score_population(p[:sample], q[:sample], badness=True, threads=threads)
-    dt = time.perf_counter() - t0
-    return {"value": sample / dt, "unit": UNIT, "cores": threads, "kind": "port",
-            "sample": f"{sample} n=75 states, determinant count + badness (accelerated.py:14-37 restated in C), "
-                      f"{threads} threads, {dt:.2f} s"}
+    cpu_checked_pass(p[:64], q[:64], threads)
+    per_state = (time.perf_counter() - t0) / 64
+    sample = int(max(threads, min(len(p), step_seconds / max(per_state, 1e-9))))
+    for _ in range(warmup):
+        cpu_checked_pass(p[:sample], q[:sample], threads)
+    times = []
+    for k in range(steps):
+        lo = (k * sample) % max(1, len(p) - sample + 1)
+        t0 = time.perf_counter()
+        if cpu_checked_pass(p[lo:lo + sample], q[lo:lo + sample], threads):
+            raise AssertionError("CPU determinant and slope counts differ")
+        times.append(time.perf_counter() - t0)
+    total = sum(times)
+    return {"value": sample * steps / total, "unit": UNIT, "cores": threads, "kind": "port",
+            "sample": f"{sample} n=75 states per pass, {steps} timed passes after {warmup} warm-up passes: "
+                      f"determinant count (accelerated.py:14-37) + slope line count with badness "
+                      f"(verifier_b.py:8-19, conflicts.py:36-72) + comparison, restated in C, {threads} threads",
+            "host": host_description(), "seconds": total, "ms_per_step": 1e3 * total / steps}
+
+
+def bench_config(states: int, world: int) -> dict:
+    """The configuration both arms report for the default (checked) mode."""
+    return {"workload": WORKLOAD, "n": N, "states_per_gpu": states, "slots": 2 * N,
+            "triple_tests_per_state": TESTS_PER_STATE, "parallelism": f"shard{world}",
+            "l2": "256 MiB buffer written between GPU steps, outside the per-step CUDA events"}
 
 
 def lines_cpu_baseline(tables, p, q, sample: int = 8):
@@ -466,34 +519,16 @@ def run_reference(args):
     rank, world, _ = dist_env()
     if rank != 0:
         return 0
-    from oracle import oracle
-
-    threads = oracle.max_threads()
+    threads = host_threads()
     p, q, _ = population(N, args.states, 0)
-    oracle.score_population(p[:8], q[:8], threads=1)
-    # bounded sample per step: ~0.5 s of wall time at this host's thread count
-    t0 = time.perf_counter()
-    oracle.score_population(p[:64], q[:64], badness=True, threads=threads)
-    per_state = (time.perf_counter() - t0) / 64
-    sample = int(max(threads, min(args.states, 0.5 / max(per_state, 1e-9))))
-    for _ in range(args.warmup):
-        oracle.score_population(p[:sample], q[:sample], badness=True, threads=threads)
-    times = []
-    for k in range(args.steps):
-        lo = (k * sample) % max(1, args.states - sample + 1)
-        t0 = time.perf_counter()
-        oracle.score_population(p[lo:lo + sample], q[lo:lo + sample], badness=True, threads=threads)
-        times.append(time.perf_counter() - t0)
-    total = sum(times)
-    value = sample * args.steps / total
+    cpu = cpu_reference_rate(p, q, threads=threads, steps=args.steps, warmup=args.warmup)
+    value = cpu["value"]
     line = {"metric": METRIC, "value": value, "unit": UNIT, "impl": "reference", "n_gpus": args.gpus,
-            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * total / args.steps,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": cpu["ms_per_step"],
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "int32",
-            "data": "synthetic: random_state(75, Random(91001+i)) states",
-            "config": {"workload": WORKLOAD, "n": N, "states": args.states, "sample_states_per_step": sample},
-            "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "port",
-                             "sample": f"{sample} states per step, determinant count + badness "
-                                       f"(accelerated.py:14-37 restated in C), {threads} threads"},
+            "data": "synthetic: random_state(75, Random(91001+i)) states (the reference's seeding)",
+            "config": bench_config(args.states, world),
+            "cpu_baseline": cpu,
             "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
     return 0
@@ -658,10 +693,8 @@ def run_b200(args):
             "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "int32",
             "data": "synthetic: random_state(75, Random(91001+i)) states (the reference's seeding), resident in HBM",
-            "config": {"workload": WORKLOAD if args.mode == "checked" else f"{WORKLOAD} ({args.mode} kernel only)",
-                       "n": N, "states_per_gpu": B, "slots": 2 * N,
-                       "triple_tests_per_state": TESTS_PER_STATE, "parallelism": f"shard{world}",
-                       "l2": "256 MiB buffer written between steps, outside the per-step CUDA events"},
+            "config": dict(bench_config(B, world), **({} if args.mode == "checked" else
+                                                          {"workload": f"{WORKLOAD} ({args.mode} kernel only)"})),
             "triple_tests_per_s": tests_per_s,
             "e2e": {"value": world * B / (e2e_ms / 1e3), "unit": UNIT,
                     "h2d_bytes_per_step": int(cols_host.nbytes),
@@ -683,7 +716,8 @@ def run_b200(args):
             "wall_s_timed": wall,
             "clocks": clocks.summary(),
         }
-        line["cpu_baseline"] = cpu_baseline(p, q, threads=os.cpu_count() or 1)
+        # the same CPU timing as the reference arm, on a bounded sample (3 passes)
+        line["cpu_baseline"] = cpu_reference_rate(p, q, threads=host_threads(), steps=3, warmup=2)
         if world == 1 and not args.no_secondary and args.mode == "checked":
             line["secondary"], extra = secondary_measurements(dev, p, q)
             line["secondary"]["note"] = ("measured after the timed region; not part of value, e2e or gpu_launches")

@@ -167,6 +167,12 @@ typedef struct n3_chains {
   int32_t* hit;                 /* [4] first chain with E <= target: chain, counter, globaltimer lo/hi; or NULL */
   int32_t* stop;                /* [1] nonzero: stop at the next exchange boundary; or NULL */
   uint32_t* error_word;         /* [1] device error bits (16: incremental/full mismatch); or NULL */
+  /* Umbrella restraint on the distance to a reference state
+   * (src/no_three_75/tempering.py:57-63, 91-97).  NULL umbrella: no restraint. */
+  const int16_t* reference;     /* [150] slot columns of the reference state (rows as in cols) */
+  int32_t* removed;             /* [C] reference points missing from chain c, kept exact; NULL without umbrella */
+  const int64_t* umbrella;      /* [C][2] per replica position l*L+t: round(2^24 s), round(2^24 * 2 s center) */
+  const uint32_t* acc_frac;     /* [L][768] fraction factors floor(2^32 exp(-k/(2^j T))), j = 8, 16, 24, k < 256 */
 } n3_chains;
 
 typedef struct n3_temper_config {
@@ -178,12 +184,23 @@ typedef struct n3_temper_config {
   int round_proposals;          /* ... unless round_proposals > 0 */
   int exchange;                 /* 1: neighbour exchange after every round */
   int target_energy;            /* >= 0: record the first chain reaching E <= target (and raise *stop) */
+  int bad_bias;                 /* percent of proposals whose slot u is drawn by badness (tempering.py:51-55) */
 } n3_temper_config;
 
 /* Runs cfg->rounds rounds (proposals, then an exchange) on every ladder in one
  * persistent launch: grid C/cpb CTAs of cpb warps, clusters of L/cpb CTAs
  * when a ladder spans several CTAs.  Capturable in a CUDA graph (fixed
- * arguments; the per-device tables must have been set up by an earlier call). */
+ * arguments; the per-device tables must have been set up by an earlier call).
+ *
+ * A proposal is the reference walk's (tempering.py:49-58): slot u uniform, or,
+ * with probability bad_bias/100 while E > 0, drawn in proportion to badness
+ * (the first slot whose running badness sum exceeds a uniform integer below
+ * 3E); slot v uniform; legal iff E > 0 and the swap duplicates no point.
+ * With chains->umbrella set, the acceptance energy adds the reference's
+ * restraint s ((removed - center + dd)^2 - (removed - center)^2) in units of
+ * 2^-24 (tempering.py:93-94), and an accepted move updates removed by dd.
+ * The reference disables exchanges under an umbrella (tempering.py:173-174):
+ * so does n3_temper_run (N3_ERR_ARG when exchange is requested). */
 int n3_temper_run(const n3_chains* chains, const n3_temper_config* config, void* stream);
 
 /* Recomputes every chain's E (determinant count) and badness (slope count)
@@ -231,8 +248,10 @@ int n3_mlp_scratch_floats(int batch);
 int n3_mlp_pack(const n3_mlp* mlp, void* stream);
 /* Draws 128 candidates per chain for the current step (Philox keyed by seed,
  * counter = step, chain, candidate), writes a1_img, badn, cand, and c1 (the
- * chain part of layer 1, one GEMM over all chains). */
-int n3_mlp_candidates(const n3_chains* chains, const n3_mlp* mlp, uint64_t seed, void* stream);
+ * chain part of layer 1, one GEMM over all chains).  bad_bias (0..100) is the
+ * percentage of candidates whose slot u is drawn in proportion to badness, as
+ * in the reference walk (src/no_three_75/tempering.py:51-55). */
+int n3_mlp_candidates(const n3_chains* chains, const n3_mlp* mlp, uint64_t seed, int bad_bias, void* stream);
 /* pred[t][j] for `tiles` tiles of 128 candidates from a1_img and c1 (tcgen05). */
 int n3_mlp_infer(const n3_mlp* mlp, int tiles, void* stream);
 /* Samples, scores exactly, accepts and records `moves` moves per chain

@@ -14,12 +14,35 @@ namespace n3 {
 // threshold row `thr` (width W) with the 32-bit uniform z, and on acceptance
 // the exact update of every slot's badness, the columns and E.  The caller
 // has checked legality.  Returns 1 if accepted; *dE_out receives dE.
+// Metropolis test of an acceptance energy e = dE + umb_q / 2^24 (umb_q: an
+// umbrella restraint term in units of 2^-24): accept iff e <= 0 or z is below
+// thr[a] x f1[b >> 16] x f2[(b >> 8) & 255] x f3[b & 255] (32-bit fixed-point
+// products), where e = a + b / 2^24.  thr[a] = floor(2^32 exp(-a/T)); frac
+// holds f1, f2, f3 (256 each): floor(2^32 exp(-k/(2^8 T))), exp(-k/(2^16 T)),
+// exp(-k/(2^24 T)).  A factor whose index is 0 is skipped, so umb_q = 0 is the
+// plain test.
+__device__ __forceinline__ bool umbrella_accept(int dE, int64_t umb_q, uint32_t z, const uint32_t* __restrict__ thr,
+                                                int W, const uint32_t* __restrict__ frac) {
+  const int64_t e = ((int64_t)dE << 24) + umb_q;
+  if (e <= 0) return true;
+  const int64_t a = e >> 24;
+  if (a >= W) return false;
+  uint32_t t = thr[a];
+  const int b = (int)(e & 0xFFFFFF);
+  if (b >> 16) t = (uint32_t)(((uint64_t)t * frac[b >> 16]) >> 32);
+  if ((b >> 8) & 255) t = (uint32_t)(((uint64_t)t * frac[256 + ((b >> 8) & 255)]) >> 32);
+  if (b & 255) t = (uint32_t)(((uint64_t)t * frac[512 + (b & 255)]) >> 32);
+  return z < t;
+}
+
 // FORCE: the move is applied whatever its dE (no Metropolis test).
-template <bool FORCE>
+// UMB: the test adds the umbrella term umb_q (umbrella_accept).
+template <bool FORCE, bool UMB = false>
 __device__ __forceinline__ int move_exact_t(int* __restrict__ cs, int* __restrict__ bs, int m,
                                             const uint16_t* __restrict__ lutf, uint32_t* __restrict__ hist, int lane,
                                             int u, int v, uint32_t z, const uint32_t* __restrict__ thr, int W, int& E,
-                                            uint32_t& err, int* dE_out) {
+                                            uint32_t& err, int* dE_out, int64_t umb_q = 0,
+                                            const uint32_t* __restrict__ frac = nullptr) {
   const int ru = u >> 1, rv = v >> 1, cu = cs[u], cv = cs[v];
   int ids[kSlotsPerLane], cnt_new[kSlotsPerLane];
   // centre u' = (r_u, c_v)
@@ -52,7 +75,8 @@ __device__ __forceinline__ int move_exact_t(int* __restrict__ cs, int* __restric
   const int t_a = sum_ab & 0xFFFF, t_b = sum_ab >> 16;
   const int dE = (t_a + t_b + j_new) - (bs[u] + bs[v] - sum_joint);
   *dE_out = dE;
-  const bool accept = FORCE || dE <= 0 || (dE < W && z < thr[dE]);
+  const bool accept = FORCE || (UMB ? umbrella_accept(dE, umb_q, z, thr, W, frac)
+                                     : (dE <= 0 || (dE < W && z < thr[dE])));
   if (!accept) {
     __syncwarp();
     return 0;
@@ -103,16 +127,83 @@ __device__ __forceinline__ int move_exact(int* __restrict__ cs, int* __restrict_
   return move_exact_t<false>(cs, bs, m, lutf, hist, lane, u, v, z, thr, W, E, err, dE_out);
 }
 
-// One uniform proposal (tempering.py:50-58 draws u, v uniformly; here from a
-// Philox block).  Returns 1 if accepted.
-__device__ __forceinline__ int propose(int* __restrict__ cs, int* __restrict__ bs, int m,
-                                       const uint16_t* __restrict__ lutf, uint32_t* __restrict__ hist, int lane,
-                                       U4 rnd, const uint32_t* __restrict__ thr, int W, int& E, uint32_t& err) {
-  const int u = (int)__umulhi(rnd.x, (unsigned)m);
+// Slot of a badness-weighted draw (tempering.py:52-54): the first slot whose
+// running badness sum exceeds `target` (target < 3E = the sum of all badness),
+// and at most m - 1.  Lane l sums slots 5l .. 5l + 4 (stride-5 shared-memory
+// reads, no bank conflicts); one warp scan gives the running sums, and the
+// slot is the number of running sums not above the target.
+__device__ __forceinline__ int bias_pick(const int* __restrict__ bs, int m, uint32_t target, int lane) {
+  const int s0 = lane * kSlotsPerLane;
+  int val[kSlotsPerLane];
+  int local = 0;
+#pragma unroll
+  for (int t = 0; t < kSlotsPerLane; ++t) {
+    val[t] = s0 + t < m ? bs[s0 + t] : 0;
+    local += val[t];
+  }
+  int incl = local;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    const int y = __shfl_up_sync(0xffffffffu, incl, o);
+    if (lane >= o) incl += y;
+  }
+  int run = incl - local, cnt = 0;
+#pragma unroll
+  for (int t = 0; t < kSlotsPerLane; ++t) {
+    run += val[t];
+    cnt += (s0 + t < m && (uint32_t)run <= target) ? 1 : 0;
+  }
+  cnt = warp_sum(cnt);
+  return cnt < m - 1 ? cnt : m - 1;
+}
+
+// Change of the umbrella distance `removed` (reference points missing from the
+// state) when slot u takes column c_v and slot v takes c_u: the reference's
+// distance_delta (tempering.py:59-63) over the reference state's rows.
+__device__ __forceinline__ int umbrella_distance_delta(const int16_t* __restrict__ ref, int u, int v, int cu, int cv) {
+  const int ur = u & ~1, vr = v & ~1;
+  const int a0 = ref[ur], a1 = ref[ur + 1], b0 = ref[vr], b1 = ref[vr + 1];
+  return (int)(cu == a0 || cu == a1) + (int)(cv == b0 || cv == b1) - (int)(cv == a0 || cv == a1) -
+         (int)(cu == b0 || cu == b1);
+}
+
+// What a walk proposal needs beyond the chain's state.
+struct WalkParams {
+  int bad_bias;                  // percent of proposals with a badness-weighted u
+  uint32_t k0, k1;               // Philox key
+  const int16_t* ref;            // umbrella reference slot columns (UMB)
+  const uint32_t* frac;          // fraction factors of this chain's temperature (UMB)
+  int64_t s_q, c2s_q;            // round(2^24 s), round(2^24 * 2 s center) of this chain's position (UMB)
+};
+
+// One walk proposal (tempering.py:49-58): u uniform, or with probability
+// bad_bias/100 drawn by badness (second Philox block, counter `ctr`, tag
+// kTagBias); v uniform; legal iff E > 0 and no point is duplicated.  rnd is
+// the proposal's Philox block: x -> u, y -> v, z the Metropolis uniform,
+// w the bias coin.  With UMB the acceptance energy carries the umbrella
+// restraint s((off + dd)^2 - off^2), off = removed - center (tempering.py:93-94),
+// and an accepted move adds dd to `removed`.  Returns 1 if accepted.
+template <bool BIAS, bool UMB>
+__device__ __forceinline__ int propose_walk(int* __restrict__ cs, int* __restrict__ bs, int m,
+                                            const uint16_t* __restrict__ lutf, uint32_t* __restrict__ hist, int lane,
+                                            U4 rnd, uint64_t ctr, int chain, const uint32_t* __restrict__ thr, int W,
+                                            int& E, uint32_t& err, const WalkParams& P, int& removed) {
+  if (E <= 0) return 0;
+  int u = (int)__umulhi(rnd.x, (unsigned)m);
   const int v = (int)__umulhi(rnd.y, (unsigned)m);
+  if (BIAS && __umulhi(rnd.w, 100u) < (unsigned)P.bad_bias) {
+    const U4 r2 = philox4x32_10(U4{(uint32_t)ctr, (uint32_t)(ctr >> 32), (uint32_t)chain, kTagBias}, P.k0, P.k1);
+    u = bias_pick(bs, m, __umulhi(r2.x, 3u * (unsigned)E), lane);
+  }
   if (!legal_swap(cs, u, v)) return 0;
   int dE;
-  return move_exact(cs, bs, m, lutf, hist, lane, u, v, rnd.z, thr, W, E, err, &dE);
+  if (!UMB) return move_exact(cs, bs, m, lutf, hist, lane, u, v, rnd.z, thr, W, E, err, &dE);
+  const int dd = umbrella_distance_delta(P.ref, u, v, cs[u], cs[v]);
+  const int64_t umb = P.s_q * (int64_t)(2 * removed * dd + dd * dd) - P.c2s_q * (int64_t)dd;
+  const int acc = move_exact_t<false, true>(cs, bs, m, lutf, hist, lane, u, v, rnd.z, thr, W, E, err, &dE, umb,
+                                            P.frac);
+  if (acc) removed += dd;
+  return acc;
 }
 
 }  // namespace n3

@@ -117,6 +117,7 @@ struct CandArgs {
   int32_t* cand;           // [C][128]: u | v << 8 | legal << 31
   const uint64_t* step;    // device step counter
   uint32_t k0, k1;
+  int bad_bias;            // percent of candidates with a badness-weighted slot u
 };
 
 template <class ColT, class BadT>
@@ -133,7 +134,7 @@ __device__ __forceinline__ void candidate_features(const ColT* cols, const BadT*
 }
 
 __global__ void __launch_bounds__(kCand) candidates_kernel(const CandArgs A) {
-  __shared__ int s_cols[kChainFeat], s_bad[kChainFeat];
+  __shared__ int s_cols[kChainFeat], s_bad[kChainFeat], s_pre[kChainFeat];
   const int c = blockIdx.x;
   const int n = A.ladder_n[c / A.ladder_size], m = 2 * n;
   for (int s = threadIdx.x; s < kChainFeat; s += blockDim.x) {
@@ -143,11 +144,51 @@ __global__ void __launch_bounds__(kCand) candidates_kernel(const CandArgs A) {
     A.badn[(size_t)c * kChainFeat + s] = s < m ? (float)b * (1.0f / 16.0f) : 0.f;
   }
   __syncthreads();
+  if (A.bad_bias > 0 && threadIdx.x < 32) {  // running badness sums (warp 0, five slots a lane)
+    const int lane = threadIdx.x, s0 = lane * kSlotsPerLane;
+    int val[kSlotsPerLane], local = 0;
+#pragma unroll
+    for (int t = 0; t < kSlotsPerLane; ++t) {
+      val[t] = s0 + t < m ? s_bad[s0 + t] : 0;
+      local += val[t];
+    }
+    int incl = local;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const int y = __shfl_up_sync(0xffffffffu, incl, o);
+      if (lane >= o) incl += y;
+    }
+    int run = incl - local;
+#pragma unroll
+    for (int t = 0; t < kSlotsPerLane; ++t) {
+      run += val[t];
+      if (s0 + t < m) s_pre[s0 + t] = run;
+    }
+  }
+  __syncthreads();
   const int j = threadIdx.x;
   const uint64_t step = *A.step;
   const U4 r = philox4x32_10(U4{(uint32_t)step, (uint32_t)(step >> 32), (uint32_t)c, kTagCandidate | (uint32_t)j},
                              A.k0, A.k1);
-  const int u = (int)__umulhi(r.x, (unsigned)m), v = (int)__umulhi(r.y, (unsigned)m);
+  int u = (int)__umulhi(r.x, (unsigned)m);
+  const int v = (int)__umulhi(r.y, (unsigned)m);
+  if (A.bad_bias > 0) {
+    // the reference walk's badness-weighted u (tempering.py:51-55): the first
+    // slot whose running badness sum exceeds a uniform integer below 3E
+    const int total = s_pre[m - 1];
+    if (total > 0 && __umulhi(r.z, 100u) < (unsigned)A.bad_bias) {
+      const int target = (int)__umulhi(r.w, (unsigned)total);
+      int lo = 0, hi = m - 1;
+      while (lo < hi) {
+        const int mid = (lo + hi) >> 1;
+        if (s_pre[mid] > target)
+          hi = mid;
+        else
+          lo = mid + 1;
+      }
+      u = lo;
+    }
+  }
   const int cu = s_cols[u], cv = s_cols[v];
   const bool legal = (u >> 1) != (v >> 1) && cu != cv && s_cols[u ^ 1] != cv && s_cols[v ^ 1] != cu;
   float f[kCandFeat];
@@ -921,9 +962,10 @@ int n3_mlp_pack(const n3_mlp* M, void* stream) {
   return n3host::launch_pack(M, (cudaStream_t)stream);
 }
 
-int n3_mlp_candidates(const n3_chains* ch, const n3_mlp* M, uint64_t seed, void* stream) {
+int n3_mlp_candidates(const n3_chains* ch, const n3_mlp* M, uint64_t seed, int bad_bias, void* stream) {
   using namespace n3::mlp;
   if (!ch || !M) return n3host::set_error(N3_ERR_ARG, "null descriptor");
+  if (bad_bias < 0 || bad_bias > 100) return n3host::set_error(N3_ERR_ARG, "bad_bias %d outside [0, 100]", bad_bias);
   CandArgs A;
   A.cols = ch->cols;
   A.badness = ch->badness;
@@ -936,6 +978,7 @@ int n3_mlp_candidates(const n3_chains* ch, const n3_mlp* M, uint64_t seed, void*
   A.step = M->counters;
   A.k0 = (uint32_t)seed;
   A.k1 = (uint32_t)(seed >> 32);
+  A.bad_bias = bad_bias;
   cudaStream_t st = (cudaStream_t)stream;
   candidates_kernel<<<ch->n_chains, kCand, 0, st>>>(A);
   N3_TRY(n3host::check_launch("candidates_kernel"));

@@ -30,6 +30,7 @@ enum : uint32_t {
   kTagPropose = 0x50000000u,   // proposal slots u, v and the Metropolis uniform
   kTagExchange = 0xE0000000u,  // neighbour temperature exchanges
   kTagCandidate = 0xC0000000u, // learned-proposal candidate slots and sampling
+  kTagBias = 0xB0000000u,      // badness-weighted slot draw of a walk proposal
 };
 
 }  // namespace n3

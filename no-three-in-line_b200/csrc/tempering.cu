@@ -10,8 +10,11 @@
 //   barrier or the cluster barrier and distributed shared memory, never a
 //   global spin-wait.
 // * Every chain keeps its columns and badness in shared memory and proposes
-//   uniform row-pair column swaps (slots u, v from Philox4x32-10 with counter
-//   (proposal index, chain), key = seed).  The exact dE uses the maintained
+//   row-pair column swaps (slots u, v from Philox4x32-10 with counter
+//   (proposal index, chain), key = seed; u badness-weighted for bad_bias
+//   percent of proposals, tempering.py:50-55).  An optional umbrella restraint
+//   on the distance to a reference state enters the acceptance energy in
+//   2^-24 fixed point (tempering.py:59-63, 93-94).  The exact dE uses the maintained
 //   badness for the old side (the reference identity bad[u]+bad[v]-joint,
 //   accelerated.py:78) and two direction histograms for the new side; an
 //   accepted move rebuilds the old-side histograms to update every point's
@@ -83,6 +86,7 @@ __device__ void exchange_ladder(int* tmp_chain, int* tmp_temp, const int* e, int
   }
 }
 
+template <bool BIAS, bool UMB>
 __global__ void __launch_bounds__(512, 1) temper_kernel(const TemperArgs A) {
   extern __shared__ __align__(16) unsigned char smem[];
   const n3_chains& ch = A.ch;
@@ -128,6 +132,7 @@ __global__ void __launch_bounds__(512, 1) temper_kernel(const TemperArgs A) {
     bs[s] = ch.badness[(size_t)c * kMaxM + s];
   }
   int E = ch.energy[c], bestE = ch.best_energy[c];
+  int removed = UMB ? ch.removed[c] : 0;
   uint64_t counter = ch.counter[c];
   uint32_t accepted = ch.accepted[c];
   uint32_t err = 0;
@@ -157,14 +162,30 @@ __global__ void __launch_bounds__(512, 1) temper_kernel(const TemperArgs A) {
   const int per_round = cfg.round_proposals > 0 ? cfg.round_proposals : cfg.round_sweeps * m;
   const uint32_t k0 = (uint32_t)cfg.seed, k1 = (uint32_t)(cfg.seed >> 32);
   const int W = ch.acc_width;
+  WalkParams wp;
+  wp.bad_bias = cfg.bad_bias;
+  wp.k0 = k0;
+  wp.k1 = k1;
+  wp.ref = ch.reference;
+  wp.frac = nullptr;
+  wp.s_q = 0;
+  wp.c2s_q = 0;
   for (int r = 0; r < rounds; ++r) {
     const int temp = L_temp[lidx];
     const uint32_t* thr = ch.acc_thresh + (size_t)temp * W;
+    if (UMB) {
+      const size_t pos = (size_t)lad * L + temp;  // the replica position (temperature slot) of this chain
+      wp.frac = ch.acc_frac + (size_t)temp * 768;
+      wp.s_q = ch.umbrella[2 * pos];
+      wp.c2s_q = ch.umbrella[2 * pos + 1];
+    }
     for (int p = 0; p < per_round; ++p) {
       const U4 rnd = philox4x32_10(U4{(uint32_t)counter, (uint32_t)(counter >> 32), (uint32_t)c, kTagPropose},
                                    k0, k1);
+      const int acc = propose_walk<BIAS, UMB>(cs, bs, m, lut, hist, lane, rnd, counter, c, thr, W, E, err, wp,
+                                              removed);
       ++counter;
-      if (propose(cs, bs, m, lut, hist, lane, rnd, thr, W, E, err)) {
+      if (acc) {
         ++accepted;
         if (E < bestE) {
           bestE = E;
@@ -205,6 +226,7 @@ __global__ void __launch_bounds__(512, 1) temper_kernel(const TemperArgs A) {
     ch.best_energy[c] = bestE;
     ch.counter[c] = counter;
     ch.accepted[c] = accepted;
+    if (UMB) ch.removed[c] = removed;
     if (err && ch.error_word) atomicOr(ch.error_word, err);
     if (ch.global_best) atomicMin(ch.global_best, bestE);
   }
@@ -296,6 +318,14 @@ int temper_launch(const n3_chains* ch, const n3_temper_config* cfg, cudaStream_t
     return set_error(N3_ERR_ARG, "negative round count or length");
   if (!cfg->exchange && cfg->round_proposals == 0 && cfg->round_sweeps == 0)
     return set_error(N3_ERR_ARG, "a round without exchange needs proposals");
+  if (cfg->bad_bias < 0 || cfg->bad_bias > 100) return set_error(N3_ERR_ARG, "bad_bias %d outside [0, 100]", cfg->bad_bias);
+  const bool umb = ch->umbrella != nullptr;
+  if (umb) {
+    if (!ch->reference || !ch->removed || !ch->acc_frac)
+      return set_error(N3_ERR_ARG, "umbrella needs reference, removed and acc_frac");
+    if (cfg->exchange)
+      return set_error(N3_ERR_ARG, "temperature-only exchange is disabled with umbrella potentials");
+  }
   N3_TRY(ensure_device_tables());
   n3::TemperArgs args;
   args.ch = *ch;
@@ -303,7 +333,10 @@ int temper_launch(const n3_chains* ch, const n3_temper_config* cfg, cudaStream_t
   args.cfg = *cfg;
   args.cluster = cluster;
   const size_t smem = n3::TemperSmem::bytes(cpb);
-  N3_TRY(allow_smem(reinterpret_cast<const void*>(n3::temper_kernel), n3::TemperSmem::bytes(16)));
+  const bool bias = cfg->bad_bias > 0;
+  void (*kern)(const n3::TemperArgs) = umb ? (bias ? n3::temper_kernel<true, true> : n3::temper_kernel<false, true>)
+                                           : (bias ? n3::temper_kernel<true, false> : n3::temper_kernel<false, false>);
+  N3_TRY(allow_smem(reinterpret_cast<const void*>(kern), n3::TemperSmem::bytes(16)));
   cudaLaunchConfig_t lc = {};
   lc.gridDim = dim3(ch->n_chains / cpb);
   lc.blockDim = dim3(cpb * 32);
@@ -316,7 +349,7 @@ int temper_launch(const n3_chains* ch, const n3_temper_config* cfg, cudaStream_t
   attr[0].val.clusterDim.z = 1;
   lc.attrs = attr;
   lc.numAttrs = 1;
-  const cudaError_t e = cudaLaunchKernelEx(&lc, n3::temper_kernel, args);
+  const cudaError_t e = cudaLaunchKernelEx(&lc, kern, args);
   if (e != cudaSuccess) return set_error(N3_ERR_CUDA, "temper_kernel launch: %s", cudaGetErrorString(e));
   return check_launch("temper_kernel");
 }
@@ -325,7 +358,10 @@ int temper_launch(const n3_chains* ch, const n3_temper_config* cfg, cudaStream_t
 
 namespace n3host {
 int prepare_tempering() {
-  N3_TRY(allow_smem(reinterpret_cast<const void*>(n3::temper_kernel), n3::TemperSmem::bytes(16)));
+  N3_TRY(allow_smem(reinterpret_cast<const void*>(n3::temper_kernel<false, false>), n3::TemperSmem::bytes(16)));
+  N3_TRY(allow_smem(reinterpret_cast<const void*>(n3::temper_kernel<true, false>), n3::TemperSmem::bytes(16)));
+  N3_TRY(allow_smem(reinterpret_cast<const void*>(n3::temper_kernel<false, true>), n3::TemperSmem::bytes(16)));
+  N3_TRY(allow_smem(reinterpret_cast<const void*>(n3::temper_kernel<true, true>), n3::TemperSmem::bytes(16)));
   return allow_smem(reinterpret_cast<const void*>(n3::audit_kernel), n3::kAuditSmem);
 }
 }  // namespace n3host

@@ -42,7 +42,8 @@ _P = ctypes.c_void_p
 _lib.register("n3_mlp_param_count", [])
 _lib.register("n3_mlp_scratch_floats", [ctypes.c_int])
 _lib.register("n3_mlp_pack", [ctypes.POINTER(N3Mlp), _P])
-_lib.register("n3_mlp_candidates", [ctypes.POINTER(N3Chains), ctypes.POINTER(N3Mlp), ctypes.c_uint64, _P])
+_lib.register("n3_mlp_candidates", [ctypes.POINTER(N3Chains), ctypes.POINTER(N3Mlp), ctypes.c_uint64, ctypes.c_int,
+                                     _P])
 _lib.register("n3_mlp_infer", [ctypes.POINTER(N3Mlp), ctypes.c_int, _P])
 _lib.register("n3_mlp_step", [ctypes.POINTER(N3Chains), ctypes.POINTER(N3Mlp), _P, ctypes.c_uint64, ctypes.c_int,
                               _P])
@@ -85,8 +86,12 @@ class LearnedProposal:
     """Learned proposals driving a TemperingChains object's chains."""
 
     def __init__(self, chains: TemperingChains, *, seed: int = 1, ring_capacity: int = 1 << 21,
-                 batch: int = 4096, lr: float = 1e-3, params: np.ndarray | None = None, moves: int = 1):
+                 batch: int = 4096, lr: float = 1e-3, params: np.ndarray | None = None, moves: int = 1,
+                 bad_bias: int = 0):
         t = _lib.torch()
+        if not 0 <= bad_bias <= 100:
+            raise ValueError("bad_bias must lie in [0,100]")
+        self.bad_bias = int(bad_bias)
         self.ch = chains
         dev = chains.device
         C = chains.cols.shape[0]
@@ -138,7 +143,8 @@ class LearnedProposal:
         L = _lib.lib()
         cd = self.ch._descriptor()
         s = _lib.stream_ptr(stream)
-        _lib.check(L.n3_mlp_candidates(ctypes.byref(cd), ctypes.byref(self._desc), self.seed, s), "n3_mlp_candidates")
+        _lib.check(L.n3_mlp_candidates(ctypes.byref(cd), ctypes.byref(self._desc), self.seed, self.bad_bias, s),
+                   "n3_mlp_candidates")
         _lib.check(L.n3_mlp_infer(ctypes.byref(self._desc), self.ch.cols.shape[0], s), "n3_mlp_infer")
 
     def step(self, stream=None):
@@ -147,6 +153,7 @@ class LearnedProposal:
         cd = self.ch._descriptor()
         _lib.check(_lib.lib().n3_mlp_step(ctypes.byref(cd), ctypes.byref(self._desc), self.temps.data_ptr(),
                                           self.seed, self.moves, _lib.stream_ptr(stream)), "n3_mlp_step")
+        self.ch._moved(False)
 
     def train(self, stream=None):
         """One Adam step on a batch from the ring buffer."""

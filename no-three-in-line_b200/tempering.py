@@ -42,13 +42,16 @@ class N3Chains(ctypes.Structure):
                 ("ladder_n", ctypes.c_void_p), ("ladder_round", ctypes.c_void_p),
                 ("ladder_exchanges", ctypes.c_void_p), ("acc_thresh", ctypes.c_void_p), ("acc_width", ctypes.c_int),
                 ("exch_thresh", ctypes.c_void_p), ("exch_width", ctypes.c_int), ("global_best", ctypes.c_void_p),
-                ("hit", ctypes.c_void_p), ("stop", ctypes.c_void_p), ("error_word", ctypes.c_void_p)]
+                ("hit", ctypes.c_void_p), ("stop", ctypes.c_void_p), ("error_word", ctypes.c_void_p),
+                ("reference", ctypes.c_void_p), ("removed", ctypes.c_void_p), ("umbrella", ctypes.c_void_p),
+                ("acc_frac", ctypes.c_void_p)]
 
 
 class N3TemperConfig(ctypes.Structure):
     _fields_ = [("seed", ctypes.c_uint64), ("chains_per_block", ctypes.c_int), ("rounds", ctypes.c_int),
                 ("ladder_rounds", ctypes.c_void_p), ("round_sweeps", ctypes.c_int),
-                ("round_proposals", ctypes.c_int), ("exchange", ctypes.c_int), ("target_energy", ctypes.c_int)]
+                ("round_proposals", ctypes.c_int), ("exchange", ctypes.c_int), ("target_energy", ctypes.c_int),
+                ("bad_bias", ctypes.c_int)]
 
 
 _lib.register("n3_temper_run", [ctypes.POINTER(N3Chains), ctypes.POINTER(N3TemperConfig), ctypes.c_void_p])
@@ -83,6 +86,41 @@ def exchange_table(temperatures) -> np.ndarray:
     tab = np.minimum(np.floor(p * _TWO32), _TWO32 - 1).astype(np.uint64).astype(np.uint32)
     tab[:, 0] = 0xFFFFFFFF
     return tab
+
+
+def fraction_table(temperatures) -> np.ndarray:
+    """uint32 [L, 768]: the fraction factors of the umbrella acceptance test,
+    floor(2^32 exp(-k / (2^j T))) for j = 8, 16, 24 and k < 256.  An acceptance
+    energy e = a + b / 2^24 (a, b integers, 0 <= b < 2^24) is accepted iff a
+    32-bit uniform lies below acc[a] x f8[b >> 16] x f16[(b >> 8) & 255] x
+    f24[b & 255] in 32-bit fixed point (a factor with index 0 is skipped)."""
+    T = np.asarray(temperatures, dtype=np.float64)
+    k = np.arange(256, dtype=np.float64)
+    parts = [np.exp(-k[None, :] / (float(2 ** j) * T[:, None])) for j in (8, 16, 24)]
+    tab = np.minimum(np.floor(np.concatenate(parts, 1) * _TWO32), _TWO32 - 1)
+    return tab.astype(np.uint64).astype(np.uint32)
+
+
+def umbrella_coefficients(strengths, centers) -> np.ndarray:
+    """int64 [R, 2]: round(2^24 s) and round(2^24 * 2 s c) of each replica
+    position's float32 strength s and centre c.  The acceptance energy of a
+    move that changes the distance by dd at distance `removed` is then
+    dE + (s_q (2 removed dd + dd^2) - c2s_q dd) / 2^24, the reference's
+    dE + s (2 (removed - c) dd + dd^2) (tempering.py:93-94) in 2^-24 units."""
+    s = np.asarray(strengths, dtype=np.float32).astype(np.float64)
+    c = np.asarray(centers, dtype=np.float32).astype(np.float64)
+    q = float(1 << 24)
+    return np.stack([np.rint(q * s), np.rint(q * 2.0 * s * c)], 1).astype(np.int64)
+
+
+def reference_distance(reference, rows) -> np.ndarray:
+    """Points of the reference state missing from each slot-column row (the
+    reference's removed_points, tempering.py:148-150)."""
+    ref = np.asarray(reference).reshape(-1)
+    rows = np.atleast_2d(np.asarray(rows))
+    m = len(ref)
+    r_pts = set((i // 2, int(c)) for i, c in enumerate(ref))
+    return np.asarray([len(r_pts - set((i // 2, int(c)) for i, c in enumerate(row[:m]))) for row in rows], np.int32)
 
 
 def geometric_ladder(tmin: float, tmax: float, size: int) -> np.ndarray:
@@ -156,6 +194,22 @@ class TemperingChains:
         self.error_word = t.zeros(1, dtype=t.int32, device=dev)
         self.round = 0
         self._graphs = {}
+        # Umbrella restraint (tempering.py:148-152): the reference state is
+        # replica 0's initial state; centres and strengths are per replica
+        # position (host float32 arrays, like the reference's, which callers
+        # assign or fill); `removed` is kept exact on the device while an
+        # umbrella is active and recounted from the states before one starts.
+        m0 = 2 * int(self.ladder_n_host[0])
+        self.reference_host = np.asarray(cols[0, :m0], np.int32)
+        ref = np.zeros(STRIDE, np.int16)
+        ref[:m0] = self.reference_host
+        self.reference_dev = t.from_numpy(ref).to(dev)
+        self.removed_dev = t.from_numpy(reference_distance(self.reference_host, padded)).to(dev)
+        self._removed_exact = True
+        self.centers = np.zeros(R, np.float32)
+        self.strengths = np.zeros(R, np.float32)
+        self.umbrella_dev = t.zeros((R, 2), dtype=t.int64, device=dev)
+        self.frac_table = t.from_numpy(fraction_table(ladder).view(np.int32)).to(dev)
 
     @classmethod
     def mixed(cls, groups, ladder_temperatures, seed: int, device=None):
@@ -213,7 +267,45 @@ class TemperingChains:
         d.exch_thresh, d.exch_width = self.exch_table.data_ptr(), self.exch_table.shape[1]
         d.global_best, d.hit, d.stop = self.global_best.data_ptr(), self.hit.data_ptr(), self.stop.data_ptr()
         d.error_word = self.error_word.data_ptr()
+        d.reference, d.removed = self.reference_dev.data_ptr(), self.removed_dev.data_ptr()
+        d.acc_frac = self.frac_table.data_ptr()
+        d.umbrella = self.umbrella_dev.data_ptr() if self.umbrella_active() else None
         return d
+
+    # -- umbrella restraint ------------------------------------------------------------
+    def umbrella_active(self) -> bool:
+        return bool(np.any(np.asarray(self.strengths) != 0))
+
+    def _prepare_umbrella(self) -> None:
+        """Uploads the fixed-point coefficients of the current centres and
+        strengths and, if the distance counts went stale under launches without
+        an umbrella, recounts them (called outside any graph capture)."""
+        t = _lib.torch()
+        R = self.cols.shape[0]
+        s, c = np.asarray(self.strengths, np.float32), np.asarray(self.centers, np.float32)
+        if s.shape != (R,) or c.shape != (R,):
+            raise ValueError("one umbrella centre and strength is required per replica")
+        if not np.all(np.isfinite(s)) or not np.all(np.isfinite(c)):
+            raise ValueError("umbrella centres and strengths must be finite")
+        if not self.umbrella_active():
+            return
+        if len(np.unique(self.ladder_n_host)) != 1:
+            raise ValueError("an umbrella needs chains of one grid size")
+        self.umbrella_dev.copy_(t.from_numpy(umbrella_coefficients(s, c)))
+        self._refresh_removed()
+
+    def _refresh_removed(self) -> None:
+        if self._removed_exact:
+            return
+        t = _lib.torch()
+        cols = self.cols.cpu().numpy()
+        self.removed_dev.copy_(t.from_numpy(reference_distance(self.reference_host, cols)))
+        self._removed_exact = True
+
+    def _moved(self, umbrella: bool) -> None:
+        """Bookkeeping after a launch that may have moved states."""
+        if not umbrella:
+            self._removed_exact = False
 
     def default_chains_per_block(self) -> int:
         """Chains (warps) per CTA: whole ladders per CTA when L <= 16 (as many as
@@ -229,7 +321,7 @@ class TemperingChains:
         raise ValueError(f"ladder size {L} cannot be split over at most 8 CTAs of at most 16 chains")
 
     def _config(self, *, rounds, round_sweeps=0, round_proposals=0, exchange=True, chains_per_block=None,
-                target=-1, ladder_rounds=None) -> N3TemperConfig:
+                target=-1, ladder_rounds=None, bad_bias=0) -> N3TemperConfig:
         c = N3TemperConfig()
         c.seed = self.seed
         c.chains_per_block = chains_per_block or self.default_chains_per_block()
@@ -239,6 +331,7 @@ class TemperingChains:
         c.round_proposals = round_proposals
         c.exchange = int(exchange)
         c.target_energy = target
+        c.bad_bias = int(bad_bias)
         return c
 
     def _launch(self, cfg: N3TemperConfig, stream=None):
@@ -248,12 +341,16 @@ class TemperingChains:
 
     # -- reference API ---------------------------------------------------------
     def advance(self, steps: int, bad_bias: int = 0) -> None:
-        """``steps`` proposals per replica, no exchange (tempering.py:158-167)."""
+        """``steps`` proposals per replica, no exchange (tempering.py:158-167).
+        With ``bad_bias`` > 0 that percentage of proposals draws slot u in
+        proportion to badness (tempering.py:51-55); active umbrella centres and
+        strengths restrain the distance to the reference state (:59-63, 93-94)."""
         if steps < 1 or not 0 <= bad_bias <= 100:
             raise ValueError("steps must be positive and bad_bias in [0,100]")
-        if bad_bias:
-            raise ValueError("badness-biased slot selection is not provided by this engine; use bad_bias=0")
-        self._launch(self._config(rounds=1, round_proposals=int(steps), exchange=False))
+        self._prepare_umbrella()
+        umb = self.umbrella_active()
+        self._launch(self._config(rounds=1, round_proposals=int(steps), exchange=False, bad_bias=bad_bias))
+        self._moved(umb)
         _lib.torch().cuda.current_stream().synchronize()
 
     def exchange(self, ladder_size: int | None = None) -> int:
@@ -261,6 +358,8 @@ class TemperingChains:
         returns the number of accepted exchanges."""
         if ladder_size is not None and ladder_size != self.L:
             raise ValueError("ladder_size must divide replica count and match the chains' ladders")
+        if self.umbrella_active():
+            raise ValueError("temperature-only exchange is disabled with umbrella potentials")
         before = int(self.ladder_exchanges.sum().item())
         cfg = self._config(rounds=1, round_sweeps=0, round_proposals=0, exchange=True)
         cfg.round_proposals = 0
@@ -271,14 +370,23 @@ class TemperingChains:
 
     def run(self, sweeps: int, *, exchange_every: int = 10, chains_per_block: int | None = None,
             sweeps_per_launch: int | None = None, target: int | None = None, ladder_sweeps=None,
-            max_seconds: float | None = None, graph: bool = True) -> RunResult:
+            max_seconds: float | None = None, graph: bool = True, bad_bias: int = 0,
+            exchange: bool = True) -> RunResult:
         """Native path: ``sweeps`` sweeps (one sweep = 2n proposals per chain)
         with a neighbour exchange every ``exchange_every`` sweeps, all on the
         device.  With ``target`` the run stops at the first exchange boundary
-        after some chain reaches E <= target; ``hit`` then reports when."""
+        after some chain reaches E <= target; ``hit`` then reports when.
+        ``bad_bias`` as in ``advance``; ``exchange=False`` runs the rounds
+        without exchanges (required while an umbrella is active)."""
         t = _lib.torch()
         if sweeps % exchange_every:
             raise ValueError("sweeps must be a multiple of exchange_every")
+        if not 0 <= bad_bias <= 100:
+            raise ValueError("bad_bias must lie in [0,100]")
+        self._prepare_umbrella()
+        umb = self.umbrella_active()
+        if umb and exchange:
+            raise ValueError("temperature-only exchange is disabled with umbrella potentials")
         per_launch = sweeps_per_launch or sweeps
         per_launch = max(exchange_every, per_launch - per_launch % exchange_every)
         launches = -(-sweeps // per_launch)
@@ -295,12 +403,14 @@ class TemperingChains:
         tgt = -1 if target is None else int(target)
         self.stop.zero_()
         self.hit.fill_(-1)
-        cfg = self._config(rounds=rounds_per_launch, round_sweeps=exchange_every, exchange=True,
-                           chains_per_block=chains_per_block, target=tgt, ladder_rounds=ladder_rounds)
+        cfg = self._config(rounds=rounds_per_launch, round_sweeps=exchange_every, exchange=exchange,
+                           chains_per_block=chains_per_block, target=tgt, ladder_rounds=ladder_rounds,
+                           bad_bias=bad_bias)
         stream = t.cuda.current_stream()
         if graph:
             key = (rounds_per_launch, exchange_every, cfg.chains_per_block, tgt,
-                   None if ladder_sweeps is None else tuple(int(x) for x in np.asarray(ladder_sweeps)))
+                   None if ladder_sweeps is None else tuple(int(x) for x in np.asarray(ladder_sweeps)),
+                   int(bad_bias), bool(exchange), umb)
             if key not in self._graphs:
                 self._graphs[key] = (self._capture(cfg), ladder_rounds)
             exec_handle = self._graphs[key][0]
@@ -327,6 +437,7 @@ class TemperingChains:
         end_ev.synchronize()
         seconds = start_ev.elapsed_time(end_ev) / 1e3
         self.round += done
+        self._moved(umb)
         hit = None
         h = self.hit.cpu().numpy().astype(np.int64)
         if h[0] >= 0:
@@ -385,6 +496,21 @@ class TemperingChains:
         if bad or err:
             raise AssertionError(f"{bad} chain(s): incremental score/badness differs from full determinant check "
                                  f"(device error bits {err:#x})")
+        if self._removed_exact and len(np.unique(self.ladder_n_host)) == 1:
+            # the distance to the reference state (tempering.py:202-204)
+            if not np.array_equal(reference_distance(self.reference_host, self.cols.cpu().numpy()),
+                                  self.removed_dev.cpu().numpy()):
+                raise AssertionError("incremental distance mismatch")
+
+    @property
+    def removed_points(self):
+        """Reference points missing from each state, in replica order."""
+        self._refresh_removed()
+        return self.removed_dev[self._replica_index()]
+
+    @property
+    def reference(self):
+        return self.reference_host
 
     # -- replica-order views -------------------------------------------------------
     def _replica_index(self):
@@ -434,21 +560,36 @@ class TemperingChains:
              "accepted_dev", "ladder_n", "ladder_round", "ladder_exchanges")
 
     def save(self, path) -> None:
-        """npz checkpoint; carries the reference's keys (tempering.py:206-212)
-        plus the Philox counters and temperature labels."""
+        """npz checkpoint with every key the reference writes (tempering.py:206-212:
+        columns, badness, scores, rngs, best_*, accepted, reference,
+        removed_points, centers, strengths, temperatures, round, host_rng) plus
+        this engine's own: the chain-order arrays, the Philox counters (also
+        stored as ``rngs``), the temperature labels and the key."""
+        self._refresh_removed()
         arrays = {k: getattr(self, k).cpu().numpy() for k in self._SAVE}
         arrays.update(columns=self.columns.cpu().numpy(), badness=self.badness.cpu().numpy(),
                       scores=self.scores.cpu().numpy(), best_columns=self.best_columns.cpu().numpy(),
                       best_scores=self.best_energy.cpu().numpy(), accepted=self.accepted_dev.cpu().numpy(),
-                      rngs=self.counter.cpu().numpy().astype(np.uint64))
+                      rngs=self.counter.cpu().numpy().astype(np.uint64), reference=self.reference_host,
+                      removed_points=self.removed_points.cpu().numpy(), removed=self.removed_dev.cpu().numpy(),
+                      centers=np.asarray(self.centers, np.float32), strengths=np.asarray(self.strengths, np.float32))
         np.savez_compressed(path, **arrays, temperatures=self.temperatures_host, ladder_size=np.asarray(self.L),
                             seed=np.asarray(self.seed, dtype=np.uint64), round=np.asarray(self.round),
                             host_rng=np.asarray(json.dumps({"philox_key": self.seed})))
 
     @classmethod
     def restore(cls, path):
+        """Restores a checkpoint written by ``save`` or by the reference's
+        ``TemperingChains.save`` (tempering.py:206-225).  A reference checkpoint
+        carries xorshift states rather than Philox counters: its chains restart
+        their counters at 0 under the key ``rngs[0]``, at the temperatures and
+        round parity it records.  Either way every energy and badness is then
+        recomputed and compared (AssertionError on a difference, as the
+        reference's restore does through validate)."""
         t = _lib.torch()
         with np.load(path, allow_pickle=False) as z:
+            if "ladder_size" not in z:
+                return cls._restore_reference(z)
             L = int(z["ladder_size"])
             ladder_n = z["ladder_n"]
             cols = z["cols"]
@@ -460,6 +601,52 @@ class TemperingChains:
                 setattr(obj, k, t.from_numpy(np.ascontiguousarray(z[k])).to(obj.device))
             obj.round = int(z["round"])
             assert obj.cols.shape[0] == R
+            obj._restore_umbrella(z, chain_order=True)
+        obj.validate()
+        return obj
+
+    def _restore_umbrella(self, z, *, chain_order: bool) -> None:
+        t = _lib.torch()
+        if "reference" in z:
+            m0 = len(self.reference_host)
+            self.reference_host = np.asarray(z["reference"], np.int32).reshape(-1)[:m0]
+            ref = np.zeros(STRIDE, np.int16)
+            ref[:m0] = self.reference_host
+            self.reference_dev.copy_(t.from_numpy(ref))
+        for k in ("centers", "strengths"):
+            if k in z:
+                setattr(self, k, np.asarray(z[k], np.float32).copy())
+        key = "removed" if chain_order else "removed_points"
+        if key in z:
+            self.removed_dev.copy_(t.from_numpy(np.ascontiguousarray(z[key], dtype=np.int32)))
+            self._removed_exact = True
+        else:
+            self._removed_exact = False
+            self._refresh_removed()
+
+    @classmethod
+    def _restore_reference(cls, z):
+        t = _lib.torch()
+        cols = np.asarray(z["columns"])
+        rngs = np.asarray(z["rngs"], np.uint64) if "rngs" in z else np.zeros(1, np.uint64)
+        obj = cls(cols, np.asarray(z["temperatures"]), int(rngs[0]))
+        # the reference's chains sit at their replica positions: identity labels
+        scores, bad = obj.energy.cpu().numpy(), obj.badness_dev.cpu().numpy()[:, :cols.shape[1]]
+        if "scores" in z and not np.array_equal(np.asarray(z["scores"], np.int64), scores.astype(np.int64)):
+            raise AssertionError("checkpoint scores differ from the full determinant check")
+        if "badness" in z and not np.array_equal(np.asarray(z["badness"], np.int64), bad.astype(np.int64)):
+            raise AssertionError("checkpoint badness differs from the full determinant check")
+        R, m = cols.shape
+        if "best_scores" in z and "best_columns" in z:
+            obj.best_energy.copy_(t.from_numpy(np.asarray(z["best_scores"], np.int32)))
+            best = np.zeros((R, STRIDE), np.int16)
+            best[:, :m] = np.asarray(z["best_columns"])
+            obj.best_cols.copy_(t.from_numpy(best))
+        if "accepted" in z:
+            obj.accepted_dev.copy_(t.from_numpy(np.asarray(z["accepted"], np.int32)))
+        obj.round = int(z["round"]) if "round" in z else 0
+        obj.ladder_round.fill_(obj.round)
+        obj._restore_umbrella(z, chain_order=False)
         obj.validate()
         return obj
 

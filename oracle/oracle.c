@@ -396,7 +396,13 @@ int64_t n3o_det_score_points(const int32_t* rows, const int32_t* cols, int m, in
  * u = floor(r0*m/2^32), v = floor(r1*m/2^32) of the Philox block with counter
  * (proposal index lo, hi, chain, 0x50000000) and key = seed), each scored by
  * the reference's pair formulation (n3o_walk_delta, tempering.py:68-89) and
- * accepted iff dE <= 0 or (dE < W and r2 < acc[temp][dE]); then each ladder
+ * accepted iff dE <= 0 or (dE < W and r2 < acc[temp][dE]).  With bad_bias,
+ * when floor(r3*100/2^32) < bad_bias, u is instead the reference's
+ * badness-weighted slot (tempering.py:51-55) for the target floor(r*3E/2^32),
+ * r the first word of the Philox block (proposal index lo, hi, chain,
+ * 0xB0000000).  No proposal moves a chain at E = 0 (tempering.py:58).  An
+ * umbrella adds s_q (2 removed dd + dd^2) - c2s_q dd (units of 2^-24) to the
+ * acceptance energy (tempering.py:59-63, 93-94).  Then each ladder
  * exchanges neighbours (t, t+1) for t = round%2, round%2+2, ... with the
  * reference's rule (tempering.py:178-184): swap when E(lower T) >= E(higher T),
  * else iff the Philox word for (round, t, ladder, 0xE0000000) is below
@@ -438,7 +444,47 @@ typedef struct {
     int rounds, round_sweeps, round_proposals, exchange;
     const int32_t* ladder_rounds;
     int round;
+    int bad_bias;
+    const int32_t* reference; /* umbrella: reference slot columns, or NULL */
+    int32_t* removed;
+    const int64_t* umbrella;  /* [C][2] per replica position */
+    const uint32_t* frac;     /* [L][768] */
 } n3o_temper_ctx;
+
+static uint32_t n3o_mulhi(uint32_t a, uint32_t b) { return (uint32_t)(((uint64_t)a * b) >> 32); }
+
+/* The reference's badness-weighted slot (tempering.py:52-54), literally. */
+static int n3o_bias_slot(const int32_t* bad, int m, int32_t target) {
+    int u = 0;
+    while (u < m - 1 && target >= bad[u]) {
+        target -= bad[u];
+        ++u;
+    }
+    return u;
+}
+
+/* distance_delta of tempering.py:59-63. */
+static int n3o_distance_delta(const int32_t* ref, int u, int v, int cu, int cv) {
+    const int ur = (u >> 1) * 2, vr = (v >> 1) * 2;
+    return (cu == ref[ur] || cu == ref[ur + 1]) + (cv == ref[vr] || cv == ref[vr + 1]) -
+           (cv == ref[ur] || cv == ref[ur + 1]) - (cu == ref[vr] || cu == ref[vr + 1]);
+}
+
+/* Acceptance with the umbrella term in units of 2^-24 (see the device's
+ * umbrella_accept): thresholds thr[a] x three 8-bit fraction factors. */
+static int n3o_umbrella_accept(int32_t dE, int64_t umb, uint32_t z, const uint32_t* thr, int W,
+                               const uint32_t* frac) {
+    const int64_t e = ((int64_t)dE << 24) + umb;
+    if (e <= 0) return 1;
+    const int64_t a = e >> 24;
+    if (a >= W) return 0;
+    uint32_t t = thr[a];
+    const int b = (int)(e & 0xFFFFFF);
+    if (b >> 16) t = n3o_mulhi(t, frac[b >> 16]);
+    if ((b >> 8) & 255) t = n3o_mulhi(t, frac[256 + ((b >> 8) & 255)]);
+    if (b & 255) t = n3o_mulhi(t, frac[512 + (b & 255)]);
+    return z < t;
+}
 
 static void n3o_temper_chain_round(int c, void* arg) {
     n3o_temper_ctx* T = (n3o_temper_ctx*)arg;
@@ -447,22 +493,39 @@ static void n3o_temper_chain_round(int c, void* arg) {
     int32_t* cols = T->cols + (size_t)c * T->stride;
     int32_t* bad = T->bad + (size_t)c * T->stride;
     const int per = T->round_proposals > 0 ? T->round_proposals : T->round_sweeps * m;
-    const uint32_t* thr = T->acc + (size_t)T->temp_of[c] * T->W;
+    const int temp = T->temp_of[c];
+    const uint32_t* thr = T->acc + (size_t)temp * T->W;
+    const size_t pos = (size_t)(c / T->L) * T->L + temp;
     int32_t dbad[512];
     for (int p = 0; p < per; ++p) {
         const uint64_t k = T->counter[c]++;
+        if (T->E[c] <= 0) continue; /* tempering.py:58: no move once score == 0 */
         uint32_t r[4] = {(uint32_t)k, (uint32_t)(k >> 32), (uint32_t)c, 0x50000000u};
         n3o_philox(r, (uint32_t)T->seed, (uint32_t)(T->seed >> 32));
-        const int u = (int)(((uint64_t)r[0] * (uint32_t)m) >> 32);
-        const int v = (int)(((uint64_t)r[1] * (uint32_t)m) >> 32);
+        int u = (int)n3o_mulhi(r[0], (uint32_t)m);
+        const int v = (int)n3o_mulhi(r[1], (uint32_t)m);
+        if (T->bad_bias > 0 && (int)n3o_mulhi(r[3], 100u) < T->bad_bias) {
+            uint32_t r2[4] = {(uint32_t)k, (uint32_t)(k >> 32), (uint32_t)c, 0xB0000000u};
+            n3o_philox(r2, (uint32_t)T->seed, (uint32_t)(T->seed >> 32));
+            u = n3o_bias_slot(bad, m, (int32_t)n3o_mulhi(r2[0], 3u * (uint32_t)T->E[c]));
+        }
         int32_t dE = 0;
         if (!n3o_walk_delta(cols, n, u, v, &dE, dbad)) continue;
-        if (!(dE <= 0 || (dE < T->W && r[2] < thr[dE]))) continue;
+        int dd = 0;
+        if (T->umbrella) {
+            dd = n3o_distance_delta(T->reference, u, v, cols[u], cols[v]);
+            const int64_t sq = T->umbrella[2 * pos], c2 = T->umbrella[2 * pos + 1];
+            const int64_t umb = sq * (int64_t)(2 * T->removed[c] * dd + dd * dd) - c2 * (int64_t)dd;
+            if (!n3o_umbrella_accept(dE, umb, r[2], thr, T->W, T->frac + (size_t)temp * 768)) continue;
+        } else if (!(dE <= 0 || (dE < T->W && r[2] < thr[dE]))) {
+            continue;
+        }
         const int32_t t = cols[u];
         cols[u] = cols[v];
         cols[v] = t;
         for (int s = 0; s < m; ++s) bad[s] += dbad[s];
         T->E[c] += dE;
+        if (T->umbrella) T->removed[c] += dd;
         T->accepted[c] += 1;
         if (T->E[c] < T->bestE[c]) {
             T->bestE[c] = T->E[c];
@@ -498,15 +561,18 @@ static void n3o_temper_exchange(n3o_temper_ctx* T, int lad) {
 }
 
 /* Replays `rounds` rounds of the device tempering kernel on the CPU.  Arrays
- * follow the n3_chains layout (columns widened to int32, row stride `stride`). */
+ * follow the n3_chains layout (columns widened to int32, row stride `stride`).
+ * bad_bias, reference/removed/umbrella/frac: see n3o_temper_chain_round
+ * (umbrella NULL: no restraint). */
 void n3o_temper_run(int C, int L, int stride, int32_t* cols, int32_t* bad, int32_t* E, int32_t* bestE,
                     int32_t* best_cols, int32_t* temp_of, int32_t* chain_at, uint64_t* counter, uint32_t* accepted,
                     const int32_t* ladder_n, uint32_t* ladder_round, uint32_t* ladder_exch, const uint32_t* acc,
                     int W, const uint32_t* exch, int XW, uint64_t seed, int rounds, int round_sweeps,
-                    int round_proposals, int exchange, const int32_t* ladder_rounds, int threads) {
+                    int round_proposals, int exchange, const int32_t* ladder_rounds, int threads, int bad_bias,
+                    const int32_t* reference, int32_t* removed, const int64_t* umbrella, const uint32_t* frac) {
     n3o_temper_ctx T = {C, L, stride, cols, bad, E, bestE, best_cols, temp_of, chain_at, counter, accepted,
                         ladder_n, ladder_round, ladder_exch, acc, W, exch, XW, seed, rounds, round_sweeps,
-                        round_proposals, exchange, ladder_rounds, 0};
+                        round_proposals, exchange, ladder_rounds, 0, bad_bias, reference, removed, umbrella, frac};
     int max_rounds = rounds;
     if (ladder_rounds)
         for (int lad = 0; lad < C / L; ++lad)

@@ -141,6 +141,84 @@ def walk_delta(cols, u: int, v: int):
     return bool(ok), int(dE.value), dbad
 
 
+_MASK64 = (1 << 64) - 1
+
+
+def next_u64(state: int) -> tuple[int, int]:
+    """xorshift64* (Vigna) as the reference's next_u64 (gpu_device_search.py:18-25):
+    returns (new state, output)."""
+    x = state
+    x ^= x >> 12
+    x ^= (x << 25) & _MASK64
+    x ^= x >> 27
+    return x, (x * 2685821657736338717) & _MASK64
+
+
+def bias_slot(badness, m: int, target: int) -> int:
+    """The reference's badness-weighted slot (tempering.py:52-54)."""
+    u = 0
+    while u < m - 1 and target >= int(badness[u]):
+        target -= int(badness[u])
+        u += 1
+    return u
+
+
+def distance_delta(reference, u: int, v: int, cu: int, cv: int) -> int:
+    """Change of the distance to the reference state (tempering.py:59-63)."""
+    ur, vr = (u >> 1) * 2, (v >> 1) * 2
+    return (int(cu in (reference[ur], reference[ur + 1])) + int(cv in (reference[vr], reference[vr + 1]))
+            - int(cv in (reference[ur], reference[ur + 1])) - int(cu in (reference[vr], reference[vr + 1])))
+
+
+def walk_with_reference_rng(cols, bad, score: int, rng: int, best_cols, best_score: int, temperature: float,
+                            accepted: int, reference, removed: int, center: float, strength: float, steps: int,
+                            bad_bias: int) -> dict:
+    """One replica of the reference's walk kernel (tempering.py:29-115) with
+    its own xorshift64* draws and double-precision acceptance, restated from
+    this oracle's pieces: ``bias_slot``, ``distance_delta`` and the pair-form
+    delta ``walk_delta``.  Used to pin those pieces against the reference's
+    kernel; the device engine draws with Philox instead (``temper_run``)."""
+    import math
+
+    cols = np.array(cols, np.int32)
+    bad = np.array(bad, np.int32)
+    best_cols = np.array(best_cols, np.int32)
+    m = len(cols)
+    T = float(np.float32(temperature))
+    c32, s32 = float(np.float32(center)), float(np.float32(strength))
+    for _ in range(steps):
+        rng, x = next_u64(rng)
+        u = x % m
+        if bad_bias > 0 and score > 0:
+            rng, x = next_u64(rng)
+            if x % 100 < bad_bias:
+                rng, x = next_u64(rng)
+                u = bias_slot(bad, m, x % (3 * score))
+        rng, x = next_u64(rng)
+        v = x % m
+        cu, cv = int(cols[u]), int(cols[v])
+        valid = score > 0 and (u >> 1) != (v >> 1) and cu != cv and cols[u ^ 1] != cv and cols[v ^ 1] != cu
+        if not valid:
+            continue
+        dd = distance_delta(reference, u, v, cu, cv)
+        _, delta, dbad = walk_delta(cols, u, v)
+        rng, x = next_u64(rng)
+        uniform = ((x >> 11) + 0.5) / 9007199254740992.0
+        offset = removed - c32
+        energy = delta + s32 * (2 * offset * dd + dd * dd)
+        if energy <= 0 or math.log(uniform) < -energy / T:
+            cols[u], cols[v] = cv, cu
+            bad += dbad
+            score += delta
+            removed += dd
+            accepted += 1
+            if score < best_score:
+                best_score = score
+                best_cols = cols.copy()
+    return {"columns": cols, "badness": bad, "scores": score, "rngs": rng, "best_columns": best_cols,
+            "best_scores": best_score, "accepted": accepted, "removed": removed}
+
+
 def score_columns(cols) -> tuple[int, np.ndarray]:
     c = _c32(cols)
     bad = np.zeros(len(c), np.int32)
@@ -160,17 +238,21 @@ def philox4x32_10(ctr, key0: int, key1: int) -> list[int]:
 
 
 def temper_run(state: dict, *, ladder_size: int, acc, exch, seed: int, rounds: int = 0, round_sweeps: int = 0,
-               round_proposals: int = 0, exchange: bool = True, ladder_rounds=None, threads: int = 0) -> dict:
+               round_proposals: int = 0, exchange: bool = True, ladder_rounds=None, threads: int = 0,
+               bad_bias: int = 0, reference=None, umbrella=None, frac=None) -> dict:
     """CPU replay of the device tempering kernel (see n3o_temper_run in oracle.c).
 
     ``state`` holds numpy arrays in the layout of the device chains (columns
-    [C, stride]); a replayed copy is returned."""
+    [C, stride]); a replayed copy is returned.  With ``umbrella`` ([C, 2] int64
+    per replica position) the state also needs ``removed`` [C]; ``reference``
+    is the reference state's slot columns and ``frac`` the [L, 768] factors."""
     L = lib()
     f = L.n3o_temper_run
     f.restype = None
     P = ctypes.c_void_p
-    f.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_int] + [P] * 13 + [ctypes.c_int, P, ctypes.c_int,
-                                                                         ctypes.c_uint64] + [ctypes.c_int] * 4 + [P, ctypes.c_int]
+    f.argtypes = ([ctypes.c_int, ctypes.c_int, ctypes.c_int] + [P] * 13 + [ctypes.c_int, P, ctypes.c_int,
+                                                                          ctypes.c_uint64] + [ctypes.c_int] * 4 +
+                  [P, ctypes.c_int, ctypes.c_int, P, P, P, P])
     s = {k: np.array(v, copy=True) for k, v in state.items()}
     conv = {"cols": np.int32, "bad": np.int32, "E": np.int32, "bestE": np.int32, "best_cols": np.int32,
             "temp_of": np.int32, "chain_at": np.int32, "counter": np.uint64, "accepted": np.uint32,
@@ -181,11 +263,20 @@ def temper_run(state: dict, *, ladder_size: int, acc, exch, seed: int, rounds: i
     exch = np.ascontiguousarray(exch, dtype=np.uint32)
     lr = None if ladder_rounds is None else np.ascontiguousarray(ladder_rounds, dtype=np.int32)
     C, stride = s["cols"].shape
+    ref = umb = fr = None
+    if umbrella is not None:
+        s["removed"] = np.ascontiguousarray(s["removed"], dtype=np.int32)
+        ref = np.ascontiguousarray(reference, dtype=np.int32)
+        umb = np.ascontiguousarray(umbrella, dtype=np.int64)
+        fr = np.ascontiguousarray(frac, dtype=np.uint32)
     f(C, ladder_size, stride, *(s[k].ctypes.data for k in ["cols", "bad", "E", "bestE", "best_cols", "temp_of",
                                                             "chain_at", "counter", "accepted", "ladder_n",
                                                             "ladder_round", "ladder_exch"]),
       acc.ctypes.data, acc.shape[1], exch.ctypes.data, exch.shape[1], seed & 0xFFFFFFFFFFFFFFFF, rounds,
-      round_sweeps, round_proposals, int(exchange), lr.ctypes.data if lr is not None else None, threads)
+      round_sweeps, round_proposals, int(exchange), lr.ctypes.data if lr is not None else None, threads,
+      int(bad_bias), None if ref is None else ref.ctypes.data,
+      None if umb is None else s["removed"].ctypes.data, None if umb is None else umb.ctypes.data,
+      None if fr is None else fr.ctypes.data)
     return s
 
 
