@@ -368,6 +368,22 @@ class TemperingChains:
         self.round += 1
         return int(self.ladder_exchanges.sum().item()) - before
 
+    def epoch(self, steps: int, bad_bias: int = 0) -> int:
+        """One epoch of the reference's driver loop (tempering.py:276-278):
+        ``steps`` proposals per replica, then one neighbour-exchange round
+        unless an umbrella is active, in a single launch.  Returns the number
+        of accepted exchanges."""
+        if steps < 1 or not 0 <= bad_bias <= 100:
+            raise ValueError("steps must be positive and bad_bias in [0,100]")
+        self._prepare_umbrella()
+        umb = self.umbrella_active()
+        before = int(self.ladder_exchanges.sum().item())
+        self._launch(self._config(rounds=1, round_proposals=int(steps), exchange=not umb, bad_bias=bad_bias))
+        self._moved(umb)
+        if not umb:
+            self.round += 1
+        return int(self.ladder_exchanges.sum().item()) - before
+
     def run(self, sweeps: int, *, exchange_every: int = 10, chains_per_block: int | None = None,
             sweeps_per_launch: int | None = None, target: int | None = None, ladder_sweeps=None,
             max_seconds: float | None = None, graph: bool = True, bad_bias: int = 0,
@@ -660,3 +676,119 @@ def _device_now_ns(device) -> int:
 
 
 _lib.register("n3_device_clock_ns", [ctypes.c_void_p, ctypes.c_void_p])
+
+
+def _state_columns(state) -> np.ndarray:
+    """Slot-column row of a P/Q state (the reference's column_stack((P, Q)).flatten())."""
+    return np.column_stack((state.P, state.Q)).flatten().astype(np.int32)
+
+
+def _symmetric_distance(reference: set, row) -> int:
+    return len(reference.symmetric_difference((i // 2, int(c)) for i, c in enumerate(row)))
+
+
+def main(argv=None) -> int:
+    """The reference's tempering driver (tempering.py:228-319) on this engine:
+    same arguments and the same output directory layout (parameters.json,
+    best-E<k>.json records, history.jsonl every 10 epochs with an audit,
+    frontier-bin<k>.json under an umbrella, checkpoint.npz every 50 epochs and
+    at the end, summary.json).  An epoch is one launch: ``steps`` proposals
+    per replica then an exchange round.  A new record is rescored by both
+    device counts (determinant and slope) before it is written, as the
+    reference rescores it with score_and_badness; a record of E = 0 must pass
+    both counts with zero, as it must pass both verifiers there."""
+    import argparse
+
+    from . import gpu
+    from .io import load_candidate, write_candidate
+
+    parser = argparse.ArgumentParser(description="Persistent replica-exchange tempering with exact integer deltas.")
+    parser.add_argument("--initial", nargs="+", required=True)
+    parser.add_argument("--output", required=True)
+    parser.add_argument("--seed", type=int, required=True)
+    parser.add_argument("--replicas", type=int, default=128)
+    parser.add_argument("--ladder-size", type=int, default=16)
+    parser.add_argument("--tmin", type=float, default=0.2)
+    parser.add_argument("--tmax", type=float, default=4)
+    parser.add_argument("--rounds", type=int, default=200)
+    parser.add_argument("--steps", type=int, default=100)
+    parser.add_argument("--bad-bias", type=int, default=0)
+    parser.add_argument("--resume")
+    parser.add_argument("--umbrella-max", type=float, default=0)
+    parser.add_argument("--umbrella-strength", type=float, default=0.2)
+    args = parser.parse_args(argv)
+    output = Path(args.output)
+    output.mkdir(parents=True, exist_ok=True)
+    rows, n = [], None
+    for path in args.initial:
+        size, points, _ = load_candidate(path)
+        if n is not None and n != size:
+            raise ValueError("all initial sizes must agree")
+        n = size
+        rows.append(_state_columns(points_to_permutations(points, n)))
+    if args.replicas % args.ladder_size or args.ladder_size < 2:
+        raise ValueError("replicas must be a multiple of ladder-size >=2")
+    if args.resume:
+        chains = TemperingChains.restore(Path(args.resume))
+        if chains.cols.shape[0] != args.replicas or chains.n != n:
+            raise ValueError("checkpoint dimensions differ from arguments")
+    else:
+        columns = np.asarray([rows[(i // args.ladder_size) % len(rows)] for i in range(args.replicas)], np.int32)
+        temperatures = np.tile(geometric_ladder(args.tmin, args.tmax, args.ladder_size),
+                               args.replicas // args.ladder_size)
+        chains = TemperingChains(columns, temperatures, args.seed, ladder_size=args.ladder_size)
+    if args.umbrella_max:
+        chains.centers = np.repeat(np.linspace(0, args.umbrella_max, args.replicas // args.ladder_size),
+                                   args.ladder_size).astype(np.float32)
+        chains.strengths.fill(args.umbrella_strength)
+    reference = set((i // 2, int(c)) for i, c in enumerate(rows[0]))
+    start = time.perf_counter()
+    best, proposals, archive = 10 ** 9, 0, {}
+    (output / "parameters.json").write_text(json.dumps(vars(args), indent=2) + "\n", encoding="utf-8")
+    for epoch in range(1, args.rounds + 1):
+        exchanges = chains.epoch(args.steps, args.bad_bias)
+        proposals += args.steps * args.replicas
+        best_scores = chains.best_scores.cpu().numpy()
+        index = int(np.argmin(best_scores))
+        if int(best_scores[index]) < best:
+            best = int(best_scores[index])
+            row = chains.best_columns[index].cpu().numpy()
+            state = chains.to_state(row)
+            exact = gpu.score_checked_gpu(_state_columns(state)[None])
+            if int(exact.scores[0]) != best:
+                raise AssertionError("record differs from independent full score")
+            write_candidate(output / f"best-E{best}.json", n, state.points(), conflicts=best, seed=args.seed,
+                            epoch=epoch, proposals=proposals, method="persistent CUDA replica exchange")
+            print(f"epoch={epoch} best={best} proposals={proposals} seconds={time.perf_counter() - start:.2f}",
+                  flush=True)
+            if best == 0:
+                break
+        if epoch % 10 == 0 or epoch == args.rounds:
+            chains.validate()
+            columns = chains.columns.cpu().numpy()
+            scores = chains.scores.cpu().numpy()
+            distances = [_symmetric_distance(reference, r) for r in columns]
+            if args.umbrella_max:
+                for i, (score, distance) in enumerate(zip(scores, distances)):
+                    bucket = distance // 8
+                    if int(score) < archive.get(bucket, 10 ** 9):
+                        archive[bucket] = int(score)
+                        candidate = chains.to_state(columns[i])
+                        write_candidate(output / f"frontier-bin{bucket:02d}.json", n, candidate.points(),
+                                        conflicts=int(score), symmetric_difference=distance, epoch=epoch,
+                                        seed=args.seed)
+            payload = {"epoch": epoch, "proposals": proposals, "elapsed_seconds": time.perf_counter() - start,
+                       "best": best, "scores": scores.tolist(), "distances": distances, "exchanges": exchanges,
+                       "accepted": int(chains.accepted.cpu().numpy().astype(np.int64).sum())}
+            with (output / "history.jsonl").open("a", encoding="utf-8") as stream:
+                stream.write(json.dumps(payload) + "\n")
+        if epoch % 50 == 0:
+            chains.save(output / "checkpoint.npz")
+    chains.validate()
+    chains.save(output / "checkpoint.npz")
+    result = {"best": best, "proposals": proposals, "elapsed_seconds": time.perf_counter() - start,
+              "accepted": int(chains.accepted.cpu().numpy().astype(np.int64).sum()), "distance_frontier": archive}
+    (output / "summary.json").write_text(json.dumps(result, indent=2) + "\n", encoding="utf-8")
+    print(json.dumps(result), flush=True)
+    return 0
+
