@@ -283,6 +283,26 @@ int n3_mlp_train_noalloc(const n3_mlp* mlp, int n_chains, int batch, float lr, u
                          float* adam_v, void* stream);
 
 /* ---------------------------------------------------------------------------
+ * Conflict analysis: the lines behind a score.
+ * ------------------------------------------------------------------------- */
+
+/* Every line holding three or more points of each of B point sets (m points
+ * each, coordinates (row, col) in [0, N3_MAX_N), m <= 160), with each point's
+ * badness.  Replaces conflicts.analyze_points (src/no_three_75/conflicts.py:36-72)
+ * and its per-pair geometry.canonical_line (src/no_three_75/geometry.py:14-28).
+ *   points     int16 [B][m][2]
+ *   badness    int32 [B][m]: sum over lines through the point of C(k-1, 2)
+ *   line_count int32 [B]: lines found, or -1 for a set with a point outside the
+ *              grid, two equal points (the reference raises ValueError) or more
+ *              lines than `capacity` (error bits 1, 2 and 32 of *error_word)
+ *   lines      int32 [B][capacity][9]: A, B, C (the reference's canonical line:
+ *              A x + B y + C = 0 over (row, col), gcd 1, A > 0 or A = 0 < B),
+ *              occupancy k, then a 160-bit member mask (bit t of word w is
+ *              point 32 w + t); lines in no particular order */
+int n3_analyze_lines(const int16_t* points, int B, int m, int32_t* badness, int32_t* line_count,
+                     int32_t* lines, int capacity, uint32_t* error_word, void* stream);
+
+/* ---------------------------------------------------------------------------
  * Multi-point moves.
  * ------------------------------------------------------------------------- */
 

@@ -25,6 +25,7 @@ enum : uint32_t {
   kErrMismatch = 1u << 2,      // determinant and slope counts disagree
   kErrTimeout = 1u << 3,       // a bounded wait gave up
   kErrAudit = 1u << 4,         // incremental energy differs from a full recompute
+  kErrCapacity = 1u << 5,      // an output list was longer than the caller's capacity
 };
 
 __device__ __forceinline__ int warp_sum(int v) { return __reduce_add_sync(0xffffffffu, v); }

@@ -597,3 +597,68 @@ def score_csr(points, tables: dict) -> int:
     counts = np.add.reduceat(occupied[tables["indices"]], tables["offsets"][:-1]).astype(np.int64)
     counts = counts[counts >= 3]
     return int(np.sum(counts * (counts - 1) * (counts - 2) // 6))
+
+
+# --------------------------------------------------------------------------
+# Conflict analysis (conflicts.py:36-72 over geometry.py:14-40), restated.
+# --------------------------------------------------------------------------
+def canonical_line(a, b) -> tuple[int, int, int]:
+    """geometry.py:14-28: primitive (A, B, C) with A*row + B*col + C = 0."""
+    from math import gcd
+
+    if tuple(a) == tuple(b):
+        raise ValueError("two distinct points are required")
+    A, B = int(b[1]) - int(a[1]), int(a[0]) - int(b[0])
+    C = -(A * int(a[0]) + B * int(a[1]))
+    g = gcd(gcd(abs(A), abs(B)), abs(C))
+    A, B, C = A // g, B // g, C // g
+    if A < 0 or (A == 0 and B < 0):
+        A, B, C = -A, -B, -C
+    return A, B, C
+
+
+def primitive_slope(key) -> tuple[int, int]:
+    """geometry.py:31-40."""
+    from math import gcd
+
+    dx, dy = int(key[1]), -int(key[0])
+    g = gcd(abs(dx), abs(dy))
+    dx, dy = dx // g, dy // g
+    if dx < 0 or (dx == 0 and dy < 0):
+        dx, dy = -dx, -dy
+    return dx, dy
+
+
+def analyze_points(points, line_weights=None) -> dict:
+    """conflicts.py:36-72: lines of three or more points (key, sorted points,
+    C(k,3)) sorted by (-triples, key), per-point badness, slope histogram and
+    the summary counts, as plain Python values."""
+    from itertools import combinations
+    from math import comb
+
+    pts = [(int(r), int(c)) for r, c in points]
+    members: dict = {}
+    for i, j in combinations(range(len(pts)), 2):
+        s = members.setdefault(canonical_line(pts[i], pts[j]), set())
+        s.add(i)
+        s.add(j)
+    badness = [0] * len(pts)
+    lines, hist = [], {}
+    triples = weighted = 0
+    for key, idx in members.items():
+        k = len(idx)
+        if k < 3:
+            continue
+        t = comb(k, 3)
+        triples += t
+        weighted += (line_weights.get(key, 1) if line_weights else 1) * t
+        for i in idx:
+            badness[i] += comb(k - 1, 2)
+        lines.append((key, tuple(sorted(pts[i] for i in idx)), t))
+        s = primitive_slope(key)
+        hist[s] = hist.get(s, 0) + t
+    lines.sort(key=lambda x: (-x[2], x[0]))
+    return {"triples": triples, "violating_lines": len(lines),
+            "max_line_occupancy": max((len(x[1]) for x in lines), default=2),
+            "max_point_badness": max(badness, default=0), "weighted_score": weighted, "badness": badness,
+            "lines": lines, "slope_histogram": hist}
