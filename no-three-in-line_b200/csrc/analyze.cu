@@ -169,7 +169,7 @@ extern "C" int n3_analyze_lines(const int16_t* points, int B, int m, int32_t* ba
   if (B < 0 || m < 0 || capacity < 0) return n3host::set_error(N3_ERR_ARG, "negative size");
   if (m > n3::kAnaMaxM) return n3host::set_error(N3_ERR_RANGE, "point sets of %d points exceed %d", m, n3::kAnaMaxM);
   if (B == 0) return N3_OK;
-  if (!points || !badness || !line_count || (!lines && capacity > 0))
+  if (!line_count || (m > 0 && (!points || !badness)) || (!lines && capacity > 0))
     return n3host::set_error(N3_ERR_ARG, "null device pointer");
   N3_TRY(n3host::ensure_device_tables());
   N3_TRY(n3host::allow_smem(reinterpret_cast<const void*>(n3::analyze_kernel), n3::kAnaSmem));
