@@ -40,7 +40,12 @@ UNIT = "states/s"
 N = 75
 STATES = 4096
 TESTS_PER_STATE = math.comb(2 * N, 3)  # 551,300
-OPS_PER_TEST = 4                       # multiply, multiply-add, compare, count
+# the determinant kernel tests every triple except those holding two points of
+# one row (never collinear with a third point in another row): 75 rows x 148
+KERNEL_TESTS_PER_STATE = TESTS_PER_STATE - N * (2 * N - 2)  # 540,200
+# per test: one product on the FMA pipe (2 multiplies + 2 multiply-adds serve
+# 4 tests) and one compare on the ALU pipe
+OPS_PER_TEST = 2
 L2_FLUSH_BYTES = 256 << 20             # > 126 MB L2
 WORKLOAD = "n=75 population scoring, 4096 states, determinant + slope cross-check + badness"
 # dram__bytes_read.sum + dram__bytes_write.sum of one det_kernel launch over the
@@ -67,6 +72,9 @@ def parse():
     ap.add_argument("--seeds", type=int, default=3, help="time-to-target: seeds per method")
     ap.add_argument("--budget", type=float, default=30.0, help="time-to-target: device seconds per run")
     ap.add_argument("--target", type=int, default=12, help="time-to-target: energy target")
+    ap.add_argument("--methods", type=str, default="plain,plain:b85,learned:x16:b85",
+                    help="time-to-target: comma-separated methods: plain, plain:b<bias>, learned, "
+                         "learned:x<moves>, learned:x<moves>:b<bias> (b = the walk's badness-biased share)")
     ap.add_argument("--learned-moves", type=str, default="1",
                     help="time-to-target: comma-separated moves per learned step to compare (1 = one move per "
                          "step); learned: the first value is the moves per step")
@@ -500,8 +508,8 @@ def run_lines_mode(args):
 def run_time_to_target(args):
     from no_three_in_line_b200 import compare
 
-    moves = tuple(int(x) for x in args.learned_moves.split(","))
-    res = compare.compare(list(range(1, args.seeds + 1)), args.target, args.budget, learned_moves=moves)
+    methods = tuple(m.strip() for m in args.methods.split(",") if m.strip())
+    res = compare.compare(list(range(1, args.seeds + 1)), args.target, args.budget, methods=methods)
     line = {"metric": "time-to-E<=target, learned vs plain proposal (n=75, 2048 chains, 64-temperature ladders)",
             "unit": "s", "higher_is_better": False, "target": args.target, "budget_s": args.budget,
             **{k: v for k, v in res.items() if k.startswith("plain") or k.startswith("learned")},
@@ -665,28 +673,40 @@ def run_b200(args):
     det_ms = [a.elapsed_time(b) for a, b in det_ms[2:]]
     det_launch_s = statistics.mean(det_ms) / 1e3
 
-    # integer-pipe ceiling of the same test expression
+    # integer-pipe ceilings: each pipe alone (multiply-add chains, logic-op
+    # chains), and the scorer's own expression on registers
     scratch = torch.zeros(2, dtype=torch.int64, device=dev)
     sms = torch.cuda.get_device_properties(dev).multi_processor_count
+
+    def timed_rate(launch, ops_per_launch, reps=5):
+        launch()
+        c0, c1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        c0.record(stream)
+        for _ in range(reps):
+            launch()
+        c1.record(stream)
+        torch.cuda.synchronize()
+        return ops_per_launch * reps / (c0.elapsed_time(c1) / 1e3)
+
     blocks, iters = sms * 8, 4096
-    _lib.check(L.n3_calibrate_det_ceiling(blocks, iters, scratch.data_ptr(), sptr), "calibrate")
-    c0, c1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    c0.record(stream)
-    for _ in range(5):
-        _lib.check(L.n3_calibrate_det_ceiling(blocks, iters, scratch.data_ptr(), sptr), "calibrate")
-    c1.record(stream)
-    torch.cuda.synchronize()
-    ceiling_tests = blocks * 256 * iters * 16 * 5 / (c0.elapsed_time(c1) / 1e3)
+    pipe_rate = {}
+    for kind, name in ((0, "imad"), (1, "alu")):
+        pipe_rate[name] = timed_rate(
+            lambda k=kind: _lib.check(L.n3_calibrate_int_pipe(k, blocks, iters, scratch.data_ptr(), sptr), "pipe"),
+            blocks * 256 * iters * 8)
+    ceiling_tests = timed_rate(
+        lambda: _lib.check(L.n3_calibrate_det_ceiling(blocks, iters, scratch.data_ptr(), sptr), "calibrate"),
+        blocks * 256 * iters * 16)
 
     line = None
     if rank == 0:
         ms_per_step = total_ms / args.steps
         tests_per_s = value * TESTS_PER_STATE
-        if args.mode == "slope":
-            achieved = tests_per_s / world * OPS_PER_TEST / 1e9
-        else:  # the determinant kernel's own launches: 4096 states x 551,300 tests x 4 ops
-            achieved = B * TESTS_PER_STATE * OPS_PER_TEST / det_launch_s / 1e9
-        peak = ceiling_tests * OPS_PER_TEST / 1e9
+        # the determinant kernel's own launches: 4096 states x 540,200 tested triples
+        kernel_tests = B * KERNEL_TESTS_PER_STATE / det_launch_s
+        pipe_tests = min(pipe_rate["imad"], pipe_rate["alu"])  # one op of each pipe per test
+        achieved = kernel_tests * OPS_PER_TEST / 1e9
+        peak = pipe_tests * OPS_PER_TEST / 1e9
         peaks, peak_kind = measured_peaks()
         line = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
@@ -701,16 +721,22 @@ def run_b200(args):
                     "d2h_bytes_per_step": int(h_scores.numel() * 4 + h_flags.numel() * 4),
                     "copies": "pinned host buffers; H2D of step k+1 on a second stream beside step k"},
             "gpu_launches": args.steps * (2 if args.mode == "checked" else 1),
-            "roofline": {"bound": "int32-alu",
-                         "kernel": {"checked": "n3::det_kernel<ColSource,false> (the larger of the step's two "
-                                               "launches; the other is n3::slope_kernel<2>)",
-                                    "det": "n3::det_kernel<ColSource,false>",
-                                    "slope": "n3::slope_kernel<0>"}[args.mode],
-                         "kernel_launch_us": det_launch_s * 1e6 if args.mode != "slope" else None,
+            "roofline": {"bound": "int32 pipes (FMA pipe for products, ALU pipe for compares)",
+                         "kernel": "n3::det_kernel<ColSource,false> (the larger of the checked step's two "
+                                   "launches; the other is n3::slope_kernel<2>), timed alone",
+                         "kernel_launch_us": det_launch_s * 1e6,
+                         "kernel_tests_per_s": kernel_tests,
                          "achieved": achieved, "peak": peak, "unit": "Gop/s", "frac": achieved / peak,
-                         "peak_source": "measured on this GPU: n3_calibrate_det_ceiling, the scorer's own "
-                                        "test expression on registers (4 int32 ops per triple test)",
-                         "traffic": DET_TRAFFIC_BYTES if args.mode != "slope" else None,
+                         "peak_source": "measured on this GPU: n3_calibrate_int_pipe, multiply-add chains "
+                                        f"{pipe_rate['imad'] / 1e12:.2f} Top/s and logic-op chains "
+                                        f"{pipe_rate['alu'] / 1e12:.2f} Top/s; 2 ops per tested triple (one "
+                                        "product share on the FMA pipe, one compare on the ALU pipe), "
+                                        f"{KERNEL_TESTS_PER_STATE} tested triples per state",
+                         "expression_ceiling": {"tests_per_s": ceiling_tests,
+                                                "frac": kernel_tests / ceiling_tests,
+                                                "source": "n3_calibrate_det_ceiling: the scorer's test "
+                                                          "expression with per-test counting, on registers"},
+                         "traffic": DET_TRAFFIC_BYTES,
                          "hbm_context": {"bytes_per_step": int(cols_host.nbytes + B * 4 + B * 2 * N * 4),
                                          "hbm_gbs_peak": peaks.get("hbm_gbs"), "peak_kind": peak_kind}},
             "wall_s_timed": wall,

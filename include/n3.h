@@ -276,6 +276,9 @@ int n3_mlp_train(const n3_mlp* mlp, int n_chains, int batch, float lr, uint64_t 
  * exits), so this call allocates nothing.  batch must lie in [64, 512]; larger
  * batches are rejected with N3_ERR_RANGE.  The first call on a device looks up
  * the array's device address; make that first call before any stream capture.
+ * The address is looked up again after the device's context has changed (a
+ * cudaDeviceReset), so make the first call after such a reset outside any
+ * capture as well.
  * All calls share the array, which keeps the last call's contents (the call
  * clears what must start at zero): calls that overlap on the GPU, from several
  * streams or threads, race on it and must be serialised by the caller. */
@@ -488,6 +491,20 @@ int n3_graph_destroy(void* graph_exec);
  * event-timed rate is the integer-pipe ceiling that bench.py reports the
  * scorer's rate against.  scratch2: device uint64[2]. */
 int n3_calibrate_det_ceiling(int blocks, int iters, unsigned long long* scratch2, void* stream);
+
+/* Throughput of one integer pipe on its own: blocks x 256 threads x iters x 8
+ * dependent-chain operations, kind 0 an integer multiply-add (the FMA pipe,
+ * which the scorer's products use), kind 1 a three-input logic operation (the
+ * ALU pipe, which its compares use).  Event-timed, these are the pipe ceilings
+ * bench.py states the scorer's roofline against.  scratch2: device uint64[2]. */
+int n3_calibrate_int_pipe(int kind, int blocks, int iters, unsigned long long* scratch2, void* stream);
+
+/* Makes one bounded device wait expire, safely: an mbarrier that nothing
+ * arrives on is waited for at most `tries` times (1 .. 2^20) with the wait
+ * the tensor-core pipeline uses, which then ORs error bit 8 (a bounded wait
+ * gave up) into *error_word and returns.  Lets callers and tests check the
+ * expiry path without hanging or faulting the GPU.  No reference counterpart. */
+int n3_check_bounded_wait(uint32_t tries, uint32_t* error_word, void* stream);
 
 #ifdef __cplusplus
 }

@@ -38,36 +38,16 @@ def seeded_chains(n: int, chains: int, ladder: int, seed: int, tmin: float = 0.0
     return tempering.TemperingChains(state.pq_to_columns(p, q), temps, seed, ladder_size=ladder)
 
 
-def run_plain(seed: int, target: int, budget: float, *, n=75, chains=2048, ladder=64, block_sweeps=100):
+def run_plain(seed: int, target: int, budget: float, *, n=75, chains=2048, ladder=64, block_sweeps=100,
+              bad_bias=0, name=None):
+    """Uniform-proposal tempering (config 3); with ``bad_bias`` that share of
+    proposals draws slot u by badness, the reference walk's option."""
+    name = name or ("plain" if not bad_bias else f"plain:b{bad_bias}")
     ch = seeded_chains(n, chains, ladder, seed)
     traj, spent = [], 0.0
     while spent < budget:
-        res = ch.run(block_sweeps, exchange_every=10, target=target, sweeps_per_launch=block_sweeps)
-        if res.hit is not None:
-            spent += res.hit[2]
-            traj.append((spent, res.best))
-            return TargetRun("plain", seed, target, True, spent, res.best, traj)
-        spent += res.seconds
-        traj.append((spent, res.best))
-    return TargetRun("plain", seed, target, False, spent, int(ch.best_energy.min().item()), traj)
-
-
-def run_learned(seed: int, target: int, budget: float, *, n=75, chains=2048, ladder=64, block=50,
-                train_every=10, moves=1, exchange_steps=None):
-    """Learned-proposal tempering; `moves` > 1 draws that many moves per step
-    (without replacement) from each step's scored candidates."""
-    from .learned import LearnedProposal
-
-    ch = seeded_chains(n, chains, ladder, seed)
-    lp = LearnedProposal(ch, seed=seed, moves=moves)
-    name = "learned" if moves == 1 else f"learned-x{moves}"
-    # exchange every 10 sweeps, a sweep being 2n learned steps (scoring passes);
-    # with moves > 1 each step makes up to `moves` proposals
-    every = exchange_steps if exchange_steps else 10 * 2 * n
-    traj, spent, first = [], 0.0, True
-    while spent < budget:
-        res = lp.run(every, exchange_every=every, train_every=train_every, block=block, target=target, warm=first)
-        first = False
+        res = ch.run(block_sweeps, exchange_every=10, target=target, sweeps_per_launch=block_sweeps,
+                     bad_bias=bad_bias)
         if res.hit is not None:
             spent += res.hit[2]
             traj.append((spent, res.best))
@@ -75,6 +55,60 @@ def run_learned(seed: int, target: int, budget: float, *, n=75, chains=2048, lad
         spent += res.seconds
         traj.append((spent, res.best))
     return TargetRun(name, seed, target, False, spent, int(ch.best_energy.min().item()), traj)
+
+
+def run_learned(seed: int, target: int, budget: float, *, n=75, chains=2048, ladder=64, block=50,
+                train_every=10, moves=1, exchange_steps=None, bad_bias=0, name=None):
+    """Learned-proposal tempering; `moves` > 1 draws that many moves per step
+    (without replacement) from each step's scored candidates; ``bad_bias``
+    draws that share of the candidates' slot u by badness.  The run's
+    proposal MAE (|predicted - exact dE| over every learned proposal) is kept."""
+    from .learned import LearnedProposal
+
+    ch = seeded_chains(n, chains, ladder, seed)
+    lp = LearnedProposal(ch, seed=seed, moves=moves, bad_bias=bad_bias)
+    if name is None:
+        name = "learned" if moves == 1 else f"learned:x{moves}"
+        name += f":b{bad_bias}" if bad_bias else ""
+    # exchange every 10 sweeps, a sweep being 2n learned steps (scoring passes);
+    # with moves > 1 each step makes up to `moves` proposals
+    every = exchange_steps if exchange_steps else 10 * 2 * n
+    traj, spent, first = [], 0.0, True
+    abs_err = count = 0.0
+    reached = False
+    while spent < budget:
+        res = lp.run(every, exchange_every=every, train_every=train_every, block=block, target=target, warm=first)
+        first = False
+        st = lp.read_stats()
+        abs_err += st.mae * st.proposals
+        count += st.proposals
+        if res.hit is not None:
+            spent += res.hit[2]
+            traj.append((spent, res.best))
+            reached = True
+            break
+        spent += res.seconds
+        traj.append((spent, res.best))
+    best = traj[-1][1] if reached else int(ch.best_energy.min().item())
+    run = TargetRun(name, seed, target, reached, spent, best, traj)
+    run.mae = abs_err / max(1.0, count)
+    return run
+
+
+def parse_method(spec: str) -> dict:
+    """``plain``, ``plain:b85``, ``learned``, ``learned:x16``, ``learned:x16:b85``."""
+    parts = spec.split(":")
+    if parts[0] not in ("plain", "learned"):
+        raise ValueError(f"unknown method {spec!r}")
+    out = {"kind": parts[0], "moves": 1, "bad_bias": 0, "name": spec}
+    for p in parts[1:]:
+        if p.startswith("x") and parts[0] == "learned":
+            out["moves"] = int(p[1:])
+        elif p.startswith("b"):
+            out["bad_bias"] = int(p[1:])
+        else:
+            raise ValueError(f"unknown method option {p!r} in {spec!r}")
+    return out
 
 
 def time_to_reach(traj, level: int):
@@ -85,31 +119,40 @@ def time_to_reach(traj, level: int):
     return None
 
 
-def compare(seeds, target: int, budget: float, *, learned_moves=(1,), **kw) -> dict:
+def compare(seeds, target: int, budget: float, *, methods=("plain", "learned"), **kw) -> dict:
+    specs = [parse_method(m) for m in methods]
     runs = []
     for s in seeds:
-        runs.append(run_plain(s, target, budget, **kw))
-        for k in learned_moves:
-            runs.append(run_learned(s, target, budget, moves=k, **kw))
-    out = {"target": target, "budget_s": budget, "runs": [asdict(r) for r in runs]}
-    methods = ["plain"] + ["learned" if k == 1 else f"learned-x{k}" for k in learned_moves]
-    for method in methods:
+        for sp in specs:
+            if sp["kind"] == "plain":
+                runs.append(run_plain(s, target, budget, bad_bias=sp["bad_bias"], name=sp["name"], **kw))
+            else:
+                runs.append(run_learned(s, target, budget, moves=sp["moves"], bad_bias=sp["bad_bias"],
+                                        name=sp["name"], **kw))
+    out = {"target": target, "budget_s": budget, "runs": [dict(asdict(r), mae=getattr(r, "mae", None))
+                                                          for r in runs]}
+    names = [sp["name"] for sp in specs]
+    for method in names:
         rs = [r for r in runs if r.method == method]
         out[method] = {"median_s": statistics.median(r.seconds for r in rs),
                        "reached": sum(r.reached for r in rs), "seeds": len(rs),
-                       "median_best": statistics.median(r.best for r in rs)}
-    # the lowest level every run of both methods reached, and the time each took
+                       "median_best": statistics.median(r.best for r in rs),
+                       "best_per_seed": sorted(r.best for r in rs)}
+        maes = [r.mae for r in rs if getattr(r, "mae", None) is not None]
+        if maes:
+            out[method]["proposal_mae"] = statistics.mean(maes)
+    # the lowest level every run reached, and the time each method took to it
     common = max(r.best for r in runs)
     out["common_level"] = common
-    for method in methods:
+    for method in names:
         times = [time_to_reach(r.trajectory, common) for r in runs if r.method == method]
         out[method]["median_s_to_common_level"] = statistics.median(times)
     # time to each level of a ladder of energies, censored at the budget
-    levels = list(range(common, min(r.best for r in runs) - 1, -1))
+    levels = list(range(max(r.trajectory[0][1] for r in runs if r.trajectory), min(r.best for r in runs) - 1, -1))
     ladder = {}
     for level in levels:
         row = {}
-        for method in methods:
+        for method in names:
             ts = [time_to_reach(r.trajectory, level) for r in runs if r.method == method]
             row[method] = {"median_s": statistics.median(budget if t is None else t for t in ts),
                            "reached": sum(t is not None for t in ts)}

@@ -1,12 +1,11 @@
 // Instruction-throughput ceiling of the determinant test.
 //
 // The population scorer's inner step (score.cu, det_pivot_row) performs, per
-// four triple tests, two IMUL + two IMAD and four compare-and-count pairs.
-// This kernel runs that exact expression on register-resident operands with
-// no shared-memory traffic, loop-carried only through the counters, on every
-// SM.  Its tests/s is the roofline ceiling against which the scorer's
-// achieved tests/s is reported (the hot kernels are integer-ALU bound, and no
-// integer peak is published for B200).
+// four triple tests, two integer multiplies, two multiply-adds and four
+// compares.  det_ceiling_kernel runs the same expression on register-resident
+// operands with no shared-memory traffic, counting every hit, on every SM: a
+// ceiling of that expression.  int_pipe_kernel measures the two integer pipes
+// the expression uses on their own (no integer peak is published for B200).
 #include "n3_common.cuh"
 
 namespace n3 {
@@ -42,7 +41,41 @@ __global__ void __launch_bounds__(256) det_ceiling_kernel(int iters, int seed, u
   if (threadIdx.x == 0 && blockIdx.x == 0) out[1] = (unsigned long long)iters;
 }
 
+// Pipe ceilings independent of the scorer's expression.  Each thread runs 8
+// independent loop-carried chains of one instruction kind on runtime values
+// (so nothing folds): an integer multiply-add a = a * b + c (the FMA pipe's
+// integer work, as the scorer's products) or a three-input logic op
+// a = (a & b) | (a ^ c) (the ALU pipe, as the scorer's compares).  Ops per
+// launch = blocks * 256 * iters * 8.
+template <int KIND>
+__global__ void __launch_bounds__(256) int_pipe_kernel(int iters, int seed, unsigned long long* out) {
+  const int t = threadIdx.x + blockIdx.x * 7 + seed;
+  const int b = (t | 1) * 0x9E37, c = t * 0x85EB + 11;
+  int a[8];
+#pragma unroll
+  for (int i = 0; i < 8; ++i) a[i] = t + i * 0x632B;
+#pragma unroll 4
+  for (int it = 0; it < iters; ++it) {
+#pragma unroll
+    for (int i = 0; i < 8; ++i) a[i] = KIND == 0 ? a[i] * b + c : (a[i] & b) | (a[i] ^ c);
+  }
+  int x = 0;
+#pragma unroll
+  for (int i = 0; i < 8; ++i) x ^= a[i];
+  if (x == 0x7fffffff) out[0] = (unsigned long long)x;  // keeps the chains live
+}
+
 }  // namespace n3
+
+extern "C" int n3_calibrate_int_pipe(int kind, int blocks, int iters, unsigned long long* scratch2, void* stream) {
+  if (blocks < 1 || iters < 1 || scratch2 == nullptr || (kind != 0 && kind != 1))
+    return n3host::set_error(N3_ERR_ARG, "calibrate: bad arguments");
+  if (kind == 0)
+    n3::int_pipe_kernel<0><<<blocks, 256, 0, (cudaStream_t)stream>>>(iters, blocks, scratch2);
+  else
+    n3::int_pipe_kernel<1><<<blocks, 256, 0, (cudaStream_t)stream>>>(iters, blocks, scratch2);
+  return n3host::check_launch("int_pipe_kernel");
+}
 
 extern "C" int n3_calibrate_det_ceiling(int blocks, int iters, unsigned long long* scratch2, void* stream) {
   if (blocks < 1 || iters < 1 || scratch2 == nullptr)

@@ -21,6 +21,7 @@
 // both on tcgen05 with fp32 accumulators in tensor memory.
 // Training (SIMT fp32, hand-written GEMMs) uses MSE on dE / kTargetScale with
 // Adam; the packed bf16 images are rebuilt after each update.
+#include <cuda.h>
 #include <cuda_bf16.h>
 #include <mutex>
 #include <math.h>
@@ -948,6 +949,62 @@ int prepare_mlp() {
 
 }  // namespace n3host
 
+namespace n3host {
+
+// One training step: gather a batch from the ring buffer, forward, backward,
+// Adam, repack the tensor-core weight images.  `scratch` holds the batch
+// activations (n3_mlp_scratch_floats(batch) floats), `grads` the gradient
+// (kParams floats); both entry points below call this body.
+static int train_step(const n3_mlp* M, int n_chains, int B, float lr, uint64_t seed, float* scratch, float* grads,
+                      float* adam_m, float* adam_v, cudaStream_t st) {
+  using namespace n3::mlp;
+  float* X = scratch;
+  float* y = X + (size_t)B * kIn;
+  float* d = y + B;
+  float* Z1 = d + B;
+  float* H1 = Z1 + (size_t)B * kH;
+  float* Z2 = H1 + (size_t)B * kH;
+  float* H2 = Z2 + (size_t)B * kH;
+  float* dZ2 = H2 + (size_t)B * kH;
+  float* dZ1 = dZ2 + (size_t)B * kH;
+  float* loss = dZ1 + (size_t)B * kH;
+  float* P = M->params;
+  // the gradient and the loss are accumulated: clear them first
+  if (cudaMemsetAsync(grads, 0, sizeof(float) * kParams, st) != cudaSuccess ||
+      cudaMemsetAsync(loss, 0, sizeof(float), st) != cudaSuccess)
+    return check_launch("MLP training: clearing the gradient");
+  gather_kernel<<<B, 64, 0, st>>>(M->rb_feat, M->rb_bad, M->rb_dE, M->counters, M->rb_capacity, n_chains, B,
+                                  (uint32_t)seed, (uint32_t)(seed >> 32), X, y);
+  const dim3 g_fwd(kH / 64, (B + 63) / 64, 1);
+  // Z1 = X W1^T + b1 ; H1 = relu(Z1)     (W1 [256][192]: B(k, n) = W1[n*192 + k])
+  gemm_kernel<1><<<g_fwd, 256, 0, st>>>(B, kH, kIn, X, kIn, 1, P + oW1, 1, kIn, H1, kH, P + oB1, Z1);
+  gemm_kernel<1><<<g_fwd, 256, 0, st>>>(B, kH, kH, H1, kH, 1, P + oW2, 1, kH, H2, kH, P + oB2, Z2);
+  head_kernel<<<(B + 7) / 8, 256, 0, st>>>(B, H2, Z2, P, y, d, dZ2, loss);
+  // gradients of the head and layer 2
+  colsum_kernel<<<dim3((kH + 127) / 128, (B + kColRows - 1) / kColRows), 128, 0, st>>>(B, kH, H2, d, grads + oW3);
+  sum_kernel<<<1, 1024, 0, st>>>(B, d, grads + oB3);
+  const int splits = B >= 2048 ? 16 : 4;
+  // gW2[n][k] = sum_b dZ2[b][n] H1[b][k]
+  gemm_kernel<0><<<dim3(kH / 64, kH / 64, splits), 256, 0, st>>>(kH, kH, B, dZ2, 1, kH, H1, kH, 1, grads + oW2, kH,
+                                                                   nullptr, nullptr);
+  colsum_kernel<<<dim3((kH + 127) / 128, (B + kColRows - 1) / kColRows), 128, 0, st>>>(B, kH, dZ2, nullptr, grads + oB2);
+  // dZ1 = (dZ2 W2) * (Z1 > 0)            (B(k, n) = W2[k*256 + n])
+  gemm_kernel<2><<<g_fwd, 256, 0, st>>>(B, kH, kH, dZ2, kH, 1, P + oW2, kH, 1, dZ1, kH, nullptr, Z1);
+  // gW1[n][k] = sum_b dZ1[b][n] X[b][k]
+  gemm_kernel<0><<<dim3(kIn / 64, kH / 64, splits), 256, 0, st>>>(kH, kIn, B, dZ1, 1, kH, X, kIn, 1, grads + oW1,
+                                                                    kIn, nullptr, nullptr);
+  colsum_kernel<<<dim3((kH + 127) / 128, (B + kColRows - 1) / kColRows), 128, 0, st>>>(B, kH, dZ1, nullptr, grads + oB1);
+  adam_kernel<<<(kParams + 255) / 256, 256, 0, st>>>(kParams, P, grads, adam_m, adam_v, lr, 0.9f, 0.999f, 1e-8f,
+                                                     M->counters);
+  bump_kernel<<<1, 1, 0, st>>>(M->counters, 1);
+  if (M->loss_out && cudaMemcpyAsync(M->loss_out, loss, sizeof(float), cudaMemcpyDeviceToDevice, st) != cudaSuccess)
+    return check_launch("MLP training: loss copy");
+  N3_TRY(check_launch("mlp training kernels"));
+  return launch_pack(M, st);
+}
+
+}  // namespace n3host
+
 extern "C" {
 
 int n3_mlp_param_count(void) { return n3::mlp::kParams; }
@@ -1038,51 +1095,9 @@ int n3_mlp_step(const n3_chains* ch, const n3_mlp* M, const float* temps, uint64
 
 int n3_mlp_train(const n3_mlp* M, int n_chains, int batch, float lr, uint64_t seed, float* scratch, float* grads,
                  float* adam_m, float* adam_v, void* stream) {
-  using namespace n3::mlp;
-  cudaStream_t st = (cudaStream_t)stream;
   if (!M || !scratch || !grads || !adam_m || !adam_v || batch < 64 || n_chains < 1)
     return n3host::set_error(N3_ERR_ARG, "bad MLP training arguments");
-  const int B = batch;
-  float* X = scratch;
-  float* y = X + (size_t)B * kIn;
-  float* d = y + B;
-  float* Z1 = d + B;
-  float* H1 = Z1 + (size_t)B * kH;
-  float* Z2 = H1 + (size_t)B * kH;
-  float* H2 = Z2 + (size_t)B * kH;
-  float* dZ2 = H2 + (size_t)B * kH;
-  float* dZ1 = dZ2 + (size_t)B * kH;
-  float* loss = dZ1 + (size_t)B * kH;
-  float* P = M->params;
-  cudaMemsetAsync(grads, 0, sizeof(float) * kParams, st);
-  cudaMemsetAsync(loss, 0, sizeof(float), st);
-  gather_kernel<<<B, 64, 0, st>>>(M->rb_feat, M->rb_bad, M->rb_dE, M->counters, M->rb_capacity, n_chains, B,
-                                  (uint32_t)seed, (uint32_t)(seed >> 32), X, y);
-  const dim3 g_fwd(kH / 64, (B + 63) / 64, 1);
-  // Z1 = X W1^T + b1 ; H1 = relu(Z1)     (W1 [256][192]: B(k, n) = W1[n*192 + k])
-  gemm_kernel<1><<<g_fwd, 256, 0, st>>>(B, kH, kIn, X, kIn, 1, P + oW1, 1, kIn, H1, kH, P + oB1, Z1);
-  gemm_kernel<1><<<g_fwd, 256, 0, st>>>(B, kH, kH, H1, kH, 1, P + oW2, 1, kH, H2, kH, P + oB2, Z2);
-  head_kernel<<<(B + 7) / 8, 256, 0, st>>>(B, H2, Z2, P, y, d, dZ2, loss);
-  // gradients of the head and layer 2
-  colsum_kernel<<<dim3((kH + 127) / 128, (B + kColRows - 1) / kColRows), 128, 0, st>>>(B, kH, H2, d, grads + oW3);
-  sum_kernel<<<1, 1024, 0, st>>>(B, d, grads + oB3);
-  const int splits = B >= 2048 ? 16 : 4;
-  // gW2[n][k] = sum_b dZ2[b][n] H1[b][k]
-  gemm_kernel<0><<<dim3(kH / 64, kH / 64, splits), 256, 0, st>>>(kH, kH, B, dZ2, 1, kH, H1, kH, 1, grads + oW2, kH,
-                                                                   nullptr, nullptr);
-  colsum_kernel<<<dim3((kH + 127) / 128, (B + kColRows - 1) / kColRows), 128, 0, st>>>(B, kH, dZ2, nullptr, grads + oB2);
-  // dZ1 = (dZ2 W2) * (Z1 > 0)            (B(k, n) = W2[k*256 + n])
-  gemm_kernel<2><<<g_fwd, 256, 0, st>>>(B, kH, kH, dZ2, kH, 1, P + oW2, kH, 1, dZ1, kH, nullptr, Z1);
-  // gW1[n][k] = sum_b dZ1[b][n] X[b][k]
-  gemm_kernel<0><<<dim3(kIn / 64, kH / 64, splits), 256, 0, st>>>(kH, kIn, B, dZ1, 1, kH, X, kIn, 1, grads + oW1,
-                                                                    kIn, nullptr, nullptr);
-  colsum_kernel<<<dim3((kH + 127) / 128, (B + kColRows - 1) / kColRows), 128, 0, st>>>(B, kH, dZ1, nullptr, grads + oB1);
-  adam_kernel<<<(kParams + 255) / 256, 256, 0, st>>>(kParams, P, grads, adam_m, adam_v, lr, 0.9f, 0.999f, 1e-8f,
-                                                     M->counters);
-  bump_kernel<<<1, 1, 0, st>>>(M->counters, 1);
-  if (M->loss_out) cudaMemcpyAsync(M->loss_out, loss, sizeof(float), cudaMemcpyDeviceToDevice, st);
-  N3_TRY(n3host::check_launch("mlp training kernels"));
-  return n3host::launch_pack(M, st);
+  return n3host::train_step(M, n_chains, batch, lr, seed, scratch, grads, adam_m, adam_v, (cudaStream_t)stream);
 }
 
 }  // extern "C"
@@ -1111,21 +1126,53 @@ static __device__ __align__(256) float g_noalloc_work[kNoAllocFloats];
 
 namespace n3host {
 
-// Device address of g_noalloc_work on the current device, looked up once per
-// device (the symbol's host-side name is not a device address).
+// Device address of g_noalloc_work in the current context.  The symbol's
+// host-side name is not a device address, so the address is looked up with
+// cudaGetSymbolAddress: once per device, and again whenever the device's
+// context has changed since (cudaDeviceReset destroys the context and with it
+// the address).  Contexts are told apart by the driver's context id; while
+// no context is current yet, or where that query is unavailable, the address
+// is looked up on every call.
+using CtxGetCurrentFn = CUresult (*)(CUcontext*);
+using CtxGetIdFn = CUresult (*)(CUcontext, unsigned long long*);
+
+static bool current_context_id(unsigned long long* id) {
+  static CtxGetCurrentFn get_current = nullptr;
+  static CtxGetIdFn get_id = nullptr;
+  static std::once_flag once;
+  std::call_once(once, [] {
+    void* f = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuCtxGetCurrent", &f, cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      get_current = reinterpret_cast<CtxGetCurrentFn>(f);
+    f = nullptr;
+    if (cudaGetDriverEntryPoint("cuCtxGetId", &f, cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      get_id = reinterpret_cast<CtxGetIdFn>(f);
+  });
+  CUcontext ctx = nullptr;
+  return get_current && get_id && get_current(&ctx) == CUDA_SUCCESS && ctx != nullptr &&
+         get_id(ctx, id) == CUDA_SUCCESS;
+}
+
 static int noalloc_work_ptr(float** out) {
   static std::mutex mu;
   static float* ptrs[64];
+  static unsigned long long ctx_ids[64];
   int dev = 0;
   if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64)
     return set_error(N3_ERR_CUDA, "n3_mlp_train_noalloc: no usable current device");
+  unsigned long long id = 0;
+  const bool have_id = current_context_id(&id);
   std::lock_guard<std::mutex> lock(mu);
-  if (ptrs[dev] == nullptr) {
+  if (ptrs[dev] == nullptr || !have_id || ctx_ids[dev] != id) {
     float* p = nullptr;
     const cudaError_t e = cudaGetSymbolAddress((void**)&p, n3::mlp::g_noalloc_work);
     if (e != cudaSuccess || p == nullptr)
       return set_error(N3_ERR_CUDA, "n3_mlp_train_noalloc: cudaGetSymbolAddress failed: %s", cudaGetErrorString(e));
     ptrs[dev] = p;
+    ctx_ids[dev] = have_id ? id : 0;
   }
   *out = ptrs[dev];
   return N3_OK;
@@ -1136,50 +1183,44 @@ static int noalloc_work_ptr(float** out) {
 extern "C" int n3_mlp_train_noalloc(const n3_mlp* M, int n_chains, int batch, float lr, uint64_t seed,
                                     float* adam_m, float* adam_v, void* stream) {
   using namespace n3::mlp;
-  cudaStream_t st = (cudaStream_t)stream;
   if (!M || !adam_m || !adam_v || n_chains < 1) return n3host::set_error(N3_ERR_ARG, "bad MLP training arguments");
   if (batch < 64 || batch > kNoAllocMaxBatch)
     return n3host::set_error(N3_ERR_RANGE, "n3_mlp_train_noalloc: batch %d outside [64, %d] (its static working "
                              "memory holds at most %d tuples)", batch, kNoAllocMaxBatch, kNoAllocMaxBatch);
   float* work = nullptr;
   N3_TRY(n3host::noalloc_work_ptr(&work));
-  const int B = batch;
-  float* X = work;
-  float* y = X + (size_t)B * kIn;
-  float* d = y + B;
-  float* Z1 = d + B;
-  float* H1 = Z1 + (size_t)B * kH;
-  float* Z2 = H1 + (size_t)B * kH;
-  float* H2 = Z2 + (size_t)B * kH;
-  float* dZ2 = H2 + (size_t)B * kH;
-  float* dZ1 = dZ2 + (size_t)B * kH;
-  float* loss = dZ1 + (size_t)B * kH;
-  float* grads = work + kNoAllocScratchFloats;
-  float* P = M->params;
-  // The array keeps the previous call's contents: clear the accumulated parts.
-  if (cudaMemsetAsync(grads, 0, sizeof(float) * kParams, st) != cudaSuccess ||
-      cudaMemsetAsync(loss, 0, sizeof(float), st) != cudaSuccess)
-    return n3host::check_launch("n3_mlp_train_noalloc: clearing the gradient");
-  gather_kernel<<<B, 64, 0, st>>>(M->rb_feat, M->rb_bad, M->rb_dE, M->counters, M->rb_capacity, n_chains, B,
-                                  (uint32_t)seed, (uint32_t)(seed >> 32), X, y);
-  const dim3 g_fwd(kH / 64, (B + 63) / 64, 1);
-  gemm_kernel<1><<<g_fwd, 256, 0, st>>>(B, kH, kIn, X, kIn, 1, P + oW1, 1, kIn, H1, kH, P + oB1, Z1);
-  gemm_kernel<1><<<g_fwd, 256, 0, st>>>(B, kH, kH, H1, kH, 1, P + oW2, 1, kH, H2, kH, P + oB2, Z2);
-  head_kernel<<<(B + 7) / 8, 256, 0, st>>>(B, H2, Z2, P, y, d, dZ2, loss);
-  colsum_kernel<<<dim3((kH + 127) / 128, (B + kColRows - 1) / kColRows), 128, 0, st>>>(B, kH, H2, d, grads + oW3);
-  sum_kernel<<<1, 1024, 0, st>>>(B, d, grads + oB3);
-  const int splits = 4;
-  gemm_kernel<0><<<dim3(kH / 64, kH / 64, splits), 256, 0, st>>>(kH, kH, B, dZ2, 1, kH, H1, kH, 1, grads + oW2, kH,
-                                                                   nullptr, nullptr);
-  colsum_kernel<<<dim3((kH + 127) / 128, (B + kColRows - 1) / kColRows), 128, 0, st>>>(B, kH, dZ2, nullptr, grads + oB2);
-  gemm_kernel<2><<<g_fwd, 256, 0, st>>>(B, kH, kH, dZ2, kH, 1, P + oW2, kH, 1, dZ1, kH, nullptr, Z1);
-  gemm_kernel<0><<<dim3(kIn / 64, kH / 64, splits), 256, 0, st>>>(kH, kIn, B, dZ1, 1, kH, X, kIn, 1, grads + oW1,
-                                                                    kIn, nullptr, nullptr);
-  colsum_kernel<<<dim3((kH + 127) / 128, (B + kColRows - 1) / kColRows), 128, 0, st>>>(B, kH, dZ1, nullptr, grads + oB1);
-  adam_kernel<<<(kParams + 255) / 256, 256, 0, st>>>(kParams, P, grads, adam_m, adam_v, lr, 0.9f, 0.999f, 1e-8f,
-                                                     M->counters);
-  bump_kernel<<<1, 1, 0, st>>>(M->counters, 1);
-  if (M->loss_out) cudaMemcpyAsync(M->loss_out, loss, sizeof(float), cudaMemcpyDeviceToDevice, st);
-  N3_TRY(n3host::check_launch("n3_mlp_train_noalloc kernels"));
-  return n3host::launch_pack(M, st);
+  // the array keeps the previous call's contents; train_step clears the
+  // accumulated gradient and loss before use
+  return n3host::train_step(M, n_chains, batch, lr, seed, work, work + kNoAllocScratchFloats, adam_m, adam_v,
+                            (cudaStream_t)stream);
+}
+
+// ---------------------------------------------------------------------------
+// Expiry of a bounded wait, on purpose.  The tensor-core pipeline waits on
+// mbarriers with the bounded umma::mbar_wait and, when a wait gives up, sets
+// kErrTimeout and returns instead of hanging.  wait_expiry_kernel runs that
+// same wait where it must give up: one thread initialises an mbarrier that
+// nothing ever arrives on, waits for its phase 0 at most `tries` times,
+// records the expiry in the error word and invalidates the barrier.  No
+// counterpart in the reference (its kernels have no bounded waits).
+// ---------------------------------------------------------------------------
+namespace n3 {
+namespace mlp {
+__global__ void wait_expiry_kernel(uint32_t tries, uint32_t* error_word) {
+  __shared__ __align__(8) uint64_t bar;
+  if (threadIdx.x != 0) return;
+  const uint32_t s = (uint32_t)__cvta_generic_to_shared(&bar);
+  umma::mbar_init(s, 1);
+  umma::mbar_fence_init();
+  if (!umma::mbar_wait(s, 0, tries)) atomicOr(error_word, kErrTimeout);
+  asm volatile("mbarrier.inval.shared::cta.b64 [%0];" ::"r"(s) : "memory");
+}
+}  // namespace mlp
+}  // namespace n3
+
+extern "C" int n3_check_bounded_wait(uint32_t tries, uint32_t* error_word, void* stream) {
+  if (error_word == nullptr) return n3host::set_error(N3_ERR_ARG, "null error word");
+  if (tries < 1 || tries > (1u << 20)) return n3host::set_error(N3_ERR_RANGE, "tries %u outside [1, 2^20]", tries);
+  n3::mlp::wait_expiry_kernel<<<1, 32, 0, (cudaStream_t)stream>>>(tries, error_word);
+  return n3host::check_launch("wait_expiry_kernel");
 }

@@ -46,6 +46,11 @@ __device__ __forceinline__ int det_pivot_row(const int* __restrict__ cs, int n, 
   }
   int cnt = 0;
   const int2* rows2 = reinterpret_cast<const int2*>(cs);
+  // Each target T (one per pivot) matches at most one of the row's two
+  // products: P0 == P1 needs a_x == 0 (a lane slot always has a_x != 0; an
+  // idle slot has target -1).  So every target contributes one OR of two
+  // compares, and the count needs no per-test conversion.  Two hits of one
+  // register slot in one row do occur (two lines through x, one per pivot).
 #pragma unroll 2
   for (int row = rb0; row < rb1; ++row) {
     const int2 cy = rows2[row];
@@ -54,19 +59,18 @@ __device__ __forceinline__ int det_pivot_row(const int* __restrict__ cs, int n, 
     for (int r = 0; r < R; ++r) {
       const int P0 = ax[r] * cy.x, P1 = ax[r] * cy.y;
       const int T0 = ay * bx0[r] + k0[r], T1 = ay * bx1[r] + k1[r];
-      const int h00 = P0 == T0, h10 = P1 == T0, h01 = P0 == T1, h11 = P1 == T1;
-      cnt += (h00 + h10) + (h01 + h11);
-      if (BAD) {
-        if (h00 | h10 | h01 | h11) {
-          const int hits[4] = {h00, h10, h01, h11};
-#pragma unroll
-          for (int t = 0; t < 4; ++t) {
-            if (hits[t]) {
-              atomicAdd(bad + sx[r], 1);
-              atomicAdd(bad + 2 * rho + (t >> 1), 1);
-              atomicAdd(bad + 2 * row + (t & 1), 1);
-            }
-          }
+      const bool g0 = (P0 == T0) | (P1 == T0), g1 = (P0 == T1) | (P1 == T1);
+      cnt += (int)g0 + (int)g1;
+      if (BAD && (g0 | g1)) {
+        if (g0) {  // x, pivot 2 rho, and slot 2 row or 2 row + 1
+          atomicAdd(bad + sx[r], 1);
+          atomicAdd(bad + 2 * rho, 1);
+          atomicAdd(bad + 2 * row + (P0 == T0 ? 0 : 1), 1);
+        }
+        if (g1) {
+          atomicAdd(bad + sx[r], 1);
+          atomicAdd(bad + 2 * rho + 1, 1);
+          atomicAdd(bad + 2 * row + (P0 == T1 ? 0 : 1), 1);
         }
       }
     }

@@ -82,6 +82,24 @@ class LearnedStats:
     loss: float         # mean squared error (in units of (dE/16)^2) of the last training batch
 
 
+_lib.register("n3_check_bounded_wait", [ctypes.c_uint32, _P, _P])
+
+ERR_TIMEOUT = 8  # device error bit: a bounded wait gave up
+
+
+def check_bounded_wait(tries: int = 256) -> None:
+    """Runs the tensor-core pipeline's bounded mbarrier wait on a barrier that
+    nothing arrives on; the wait gives up after ``tries`` attempts and the
+    device reports it.  Raises TimeoutError, as a stalled pipeline would."""
+    t = _lib.torch()
+    dev = _lib.require_device()
+    err = t.zeros(1, dtype=t.int32, device=dev)
+    _lib.call("n3_check_bounded_wait", int(tries), err.data_ptr(), _lib.stream_ptr())
+    bits = int(err.item())
+    if bits & ERR_TIMEOUT:
+        raise TimeoutError(f"a bounded device wait gave up after {tries} tries (error bits {bits:#x})")
+
+
 class LearnedProposal:
     """Learned proposals driving a TemperingChains object's chains."""
 

@@ -213,12 +213,14 @@ def score_csr_population(p_batch, q_batch, tables: GeometryTables) -> np.ndarray
     return _run_csr(ids, tables.n, tables) if ids else np.zeros(0, np.int64)
 
 
-def _average_seconds(function, repeats: int) -> tuple[int, float]:
-    started = time.perf_counter()
-    value = None
-    for _ in range(repeats):
-        value = int(function())
-    return int(value), (time.perf_counter() - started) / repeats
+def _timed(score, calls: int) -> tuple[int, float]:
+    """Calls ``score`` ``calls`` times back to back; returns its last result
+    and the mean wall time of one call."""
+    result = 0
+    t0 = time.perf_counter()
+    for _ in range(calls):
+        result = score()
+    return int(result), (time.perf_counter() - t0) / calls
 
 
 def benchmark_precomputation(n: int, points) -> dict[str, object]:
@@ -230,21 +232,24 @@ def benchmark_precomputation(n: int, points) -> dict[str, object]:
     from .gpu import score_slope_gpu
     from .state import pq_to_columns, points_to_permutations
 
-    state = points_to_permutations(points, n)
-    p = np.asarray(state.P, dtype=np.int32)
-    q = np.asarray(state.Q, dtype=np.int32)
-    cols = pq_to_columns(p[None], q[None])
-    score_and_badness(p, q)
+    pq = points_to_permutations(points, n)
+    p, q = np.asarray(pq.P, np.int32), np.asarray(pq.Q, np.int32)
+    columns = pq_to_columns(p[None], q[None])
     tables = build_geometry_tables(n)
-    score_a, seconds_a = _average_seconds(lambda: score_and_badness(p, q)[0], 100)
-    score_b, seconds_b = _average_seconds(lambda: score_pair_table(points, tables), 100)
-    score_c, seconds_c = _average_seconds(lambda: score_slope_gpu(cols)[0][0], 5)
-    score_d, seconds_d = _average_seconds(lambda: score_csr(points, tables), 20)
-    if len({score_a, score_b, score_c, score_d}) != 1:
-        raise AssertionError(f"precompute scorers disagree: {score_a}, {score_b}, {score_c}, {score_d}")
+    scorers = {  # name in the result -> (scorer, calls timed)
+        "A_numba_determinants": (lambda: score_and_badness(p, q)[0], 100),
+        "B_pair_to_line": (lambda: score_pair_table(points, tables), 100),
+        "C_canonical_line_dict": (lambda: score_slope_gpu(columns)[0][0], 5),
+        "D_csr_line_scan": (lambda: score_csr(points, tables), 20),
+    }
+    score_and_badness(p, q)  # first launch outside the timing
+    results = {name: _timed(fn, calls) for name, (fn, calls) in scorers.items()}
+    scores = {score for score, _ in results.values()}
+    if len(scores) != 1:
+        raise AssertionError("precompute scorers disagree: " + ", ".join(f"{k}={v[0]}" for k, v in results.items()))
     return {
         "n": n,
-        "score": score_a,
+        "score": scores.pop(),
         "line_count": tables.line_count,
         "line_incidences": int(len(tables.indices)),
         "build_seconds": tables.build_seconds,
@@ -253,10 +258,5 @@ def benchmark_precomputation(n: int, points) -> dict[str, object]:
             "csr_offsets": int(tables.offsets.nbytes),
             "csr_indices": int(tables.indices.nbytes),
         },
-        "seconds_per_score": {
-            "A_numba_determinants": seconds_a,
-            "B_pair_to_line": seconds_b,
-            "C_canonical_line_dict": seconds_c,
-            "D_csr_line_scan": seconds_d,
-        },
+        "seconds_per_score": {name: seconds for name, (_, seconds) in results.items()},
     }

@@ -35,7 +35,12 @@ from random import Random
 import numpy as np
 
 HERE = Path(__file__).resolve().parent
-REFERENCE = Path(sys.argv[1] if len(sys.argv) > 1 else os.environ.get("N3_REFERENCE", "/root/reference"))
+if len(sys.argv) > 1:
+    REFERENCE = Path(sys.argv[1])
+elif os.environ.get("N3_REFERENCE"):
+    REFERENCE = Path(os.environ["N3_REFERENCE"])
+else:
+    raise SystemExit("usage: make_golden.py /path/to/reference  (or set N3_REFERENCE)")
 sys.path.insert(0, str(REFERENCE / "src"))
 os.environ.setdefault("NUMBA_CACHE_DIR", "/tmp/n3_numba_cache")
 

@@ -21,7 +21,12 @@ import tempfile
 from pathlib import Path
 
 HERE = Path(__file__).resolve().parent
-REFERENCE = Path(sys.argv[1] if len(sys.argv) > 1 else os.environ.get("N3_REFERENCE", "/root/reference"))
+if len(sys.argv) > 1:
+    REFERENCE = Path(sys.argv[1])
+elif os.environ.get("N3_REFERENCE"):
+    REFERENCE = Path(os.environ["N3_REFERENCE"])
+else:
+    raise SystemExit("usage: make_golden_io.py /path/to/reference  (or set N3_REFERENCE)")
 sys.path.insert(0, str(REFERENCE / "src"))
 
 from no_three_75 import io as ref_io  # noqa: E402

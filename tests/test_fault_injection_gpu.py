@@ -73,3 +73,21 @@ def test_checkpoint_with_corrupted_state_fails_validation(cuda, tmp_path):
     np.savez(tmp_path / "bad.npz", **arrays)
     with pytest.raises(AssertionError):
         tempering.TemperingChains.restore(tmp_path / "bad.npz")
+
+
+def test_bounded_device_wait_expires_without_hanging(cuda):
+    """A device wait that can never complete gives up after its bound, reports
+    it (TimeoutError on the host) and leaves the context usable."""
+    import time
+
+    from no_three_in_line_b200 import learned
+
+    t0 = time.perf_counter()
+    for tries in (1, 300, 1 << 16):
+        with pytest.raises(TimeoutError):
+            learned.check_bounded_wait(tries)
+    assert time.perf_counter() - t0 < 60
+    p, q = state.seeded_population(20, 4)
+    assert gpu.score_population_gpu(p, q).shape == (4,)  # the context still works
+    with pytest.raises(ValueError):
+        learned.check_bounded_wait(0)
