@@ -515,7 +515,7 @@ def run_time_to_target(args):
             **{k: v for k, v in res.items() if k.startswith("plain") or k.startswith("learned")},
             "common_level": res["common_level"], "time_to_level": res["time_to_level"],
             "data": "synthetic: random_state(75, Random(91001+c)) chain starts",
-            "runs": [{k: r[k] for k in ("method", "seed", "reached", "seconds", "best")} for r in res["runs"]],
+            "runs": [{k: r[k] for k in ("method", "seed", "reached", "seconds", "best", "mae")} for r in res["runs"]],
             "trajectories": {f'{r["method"]}-{r["seed"]}': r["trajectory"][::max(1, len(r["trajectory"]) // 40)]
                              for r in res["runs"]}}
     print(json.dumps(line), flush=True)
