@@ -62,12 +62,13 @@ def parse():
     ap.add_argument("--impl", choices=["b200", "reference"], default="b200")
     ap.add_argument("--states", type=int, default=STATES)
     ap.add_argument("--mode", choices=["checked", "det", "slope", "tempering", "learned", "time-to-target", "beam",
-                                       "scan", "lines"],
+                                       "scan", "lines", "exhaustive"],
                     default="checked",
                     help="kernel a step runs: fused checked scoring (default), determinant only, slope only; "
                          "tempering / learned chain rounds; one device beam-search generation (beam); one "
                          "four-cycle + double-switch neighbourhood scan (scan); the n = 75 line tables "
-                         "and both table scorers (lines); or the learned-vs-plain time-to-target comparison")
+                         "and both table scorers (lines); one exhaustive 2-switch beam generation (exhaustive); "
+                         "or the learned-vs-plain time-to-target comparison")
     ap.add_argument("--no-secondary", action="store_true", help="skip the delta/tempering/MLP measurements")
     ap.add_argument("--seeds", type=int, default=3, help="time-to-target: seeds per method")
     ap.add_argument("--budget", type=float, default=30.0, help="time-to-target: device seconds per run")
@@ -75,6 +76,7 @@ def parse():
     ap.add_argument("--methods", type=str, default="plain,plain:b85,learned:x16:b85",
                     help="time-to-target: comma-separated methods: plain, plain:b<bias>, learned, "
                          "learned:x<moves>, learned:x<moves>:b<bias> (b = the walk's badness-biased share)")
+    ap.add_argument("--log", type=str, default=None, help="time-to-target: append each finished run to this JSONL file")
     ap.add_argument("--learned-moves", type=str, default="1",
                     help="time-to-target: comma-separated moves per learned step to compare (1 = one move per "
                          "step); learned: the first value is the moves per step")
@@ -226,23 +228,28 @@ def bench_config(states: int, world: int) -> dict:
             "l2": "256 MiB buffer written between GPU steps, outside the per-step CUDA events"}
 
 
-def lines_cpu_baseline(tables, p, q, sample: int = 8):
+def lines_cpu_baseline(tables, p, q, sample: int = 24):
     """score_pair_table + score_csr (precompute.py:60-89, restated in NumPy in
-    oracle/) on the first `sample` states, one host thread."""
+    oracle/) on `sample` states after 2 warm-up states, one host thread (the
+    restatement is single-threaded NumPy)."""
     from oracle import oracle
 
     t = {"n": tables.n, "pair_to_line": tables.pair_to_line, "offsets": tables.offsets, "indices": tables.indices,
          "line_count": tables.line_count}
     n = tables.n
-    pts = [[(r, int(p[b, r])) for r in range(n)] + [(r, int(q[b, r])) for r in range(n)] for b in range(sample)]
+    pts = [[(r, int(p[b, r])) for r in range(n)] + [(r, int(q[b, r])) for r in range(n)]
+           for b in range(sample + 2)]
+    for x in pts[:2]:
+        oracle.score_pair_table(x, t)
+        oracle.score_csr(x, t)
     t0 = time.perf_counter()
-    for x in pts:
+    for x in pts[2:]:
         oracle.score_pair_table(x, t)
         oracle.score_csr(x, t)
     dt = time.perf_counter() - t0
     return {"value": sample / dt, "unit": "states/s", "cores": 1, "kind": "port",
-            "sample": f"{sample} n=75 states, score_pair_table + score_csr (precompute.py:60-89 restated in NumPy), "
-                      f"1 thread, {dt:.2f} s"}
+            "sample": f"{sample} n=75 states after 2 warm-up states, score_pair_table + score_csr (precompute.py:60-89 "
+                      f"restated in NumPy), 1 thread, {dt:.2f} s", "host": host_description()}
 
 
 def secondary_measurements(dev, p, q):
@@ -492,6 +499,42 @@ def run_lines_mode(args):
         end.record(stream)
         end.synchronize()
     secs = start.elapsed_time(end) / 1e3
+    # each scorer alone (events around each call), and the L2 random-gather rate
+    # of the pair table itself as the pair scorer's ceiling
+    pair_ev, csr_ev = [], []
+    for _ in range(5):
+        a, b, c = (torch.cuda.Event(enable_timing=True) for _ in range(3))
+        a.record(stream)
+        _lib.check(L.n3_lines_score_pairs(d_ids.data_ptr(), d_starts.data_ptr(), args.states, N,
+                                          d.pair_to_line.data_ptr(), pair_scores.data_ptr(), err.data_ptr(), sp),
+                   "n3_lines_score_pairs")
+        b.record(stream)
+        _lib.check(L.n3_lines_score_csr(d_ids.data_ptr(), d_starts.data_ptr(), args.states, N, tables.line_count,
+                                        d.offsets.data_ptr(), d.indices.data_ptr(), occ.data_ptr(),
+                                        csr_scores.data_ptr(), err.data_ptr() + 4, sp), "n3_lines_score_csr")
+        c.record(stream)
+        pair_ev.append((a, b))
+        csr_ev.append((b, c))
+    torch.cuda.synchronize()
+    pair_s = statistics.mean(x.elapsed_time(y) for x, y in pair_ev[1:]) / 1e3
+    csr_s = statistics.mean(x.elapsed_time(y) for x, y in csr_ev[1:]) / 1e3
+    gathers_per_state = math.comb(2 * N, 2)
+    scratch = torch.zeros(2, dtype=torch.int64, device=dev)
+    entries = int(d.pair_to_line.numel())
+    blocks = torch.cuda.get_device_properties(dev).multi_processor_count * 8
+    iters = 2048
+    _lib.check(L.n3_calibrate_l2_gather(d.pair_to_line.data_ptr(), entries, blocks, iters, scratch.data_ptr(), sp),
+               "l2 gather")
+    g0, g1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    g0.record(stream)
+    for _ in range(5):
+        _lib.check(L.n3_calibrate_l2_gather(d.pair_to_line.data_ptr(), entries, blocks, iters, scratch.data_ptr(),
+                                            sp), "l2 gather")
+    g1.record(stream)
+    torch.cuda.synchronize()
+    gather_peak = blocks * 256 * iters * 5 / (g0.elapsed_time(g1) / 1e3)
+    pair_gathers = args.states * gathers_per_state / pair_s
+    lookups = (args.states + 31) // 32 * int(len(tables.indices))
     line = {"metric": METRIC, "value": args.states * args.steps / secs, "unit": "states/s", "n_gpus": 1,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * secs / args.steps,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "int32",
@@ -499,8 +542,52 @@ def run_lines_mode(args):
             "config": {"workload": f"n=75 line tables: score_pair_table + score_csr of {args.states} states",
                        "mode": "lines", "line_count": tables.line_count, "line_incidences": int(len(tables.indices)),
                        "pair_table_bytes": int(tables.pair_to_line.nbytes)},
-            "table_build_ms_with_host_copies": build_ms, "gpu_launches": 3 * args.steps, "clocks": clocks.summary(),
+            "table_build_ms_with_host_copies": build_ms, "gpu_launches": 3 * args.steps,
+            "gpu_launches_note": "3 kernels per step (pair scorer; occupancy + CSR scorer); each step also issues "
+                                 "2 cudaMemsetAsync (the occupancy words and the scores)",
+            "per_scorer": {"pair_table_us": pair_s * 1e6, "csr_us": csr_s * 1e6,
+                           "pair_gathers_per_s": pair_gathers,
+                           "csr_occupancy_lookups_per_s": lookups / csr_s},
+            "roofline": {"bound": "L2 random 4-byte gathers (pair-table scorer)",
+                         "kernel": "n3::lines::pair_score_kernel", "achieved": pair_gathers / 1e9,
+                         "peak": gather_peak / 1e9, "unit": "G gathers/s", "frac": pair_gathers / gather_peak,
+                         "peak_source": "measured on this GPU: n3_calibrate_l2_gather, xorshift-indexed 4-byte "
+                                        f"loads from the {entries * 4 / 1e6:.0f} MB pair table itself (L2-resident)",
+                         "algorithmic": f"C(150,2) = {gathers_per_state} pair-table gathers per n=75 state"},
+            "clocks": clocks.summary(),
             "cpu_baseline": lines_cpu_baseline(tables, p, q)}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def run_exhaustive_mode(args):
+    """--mode exhaustive: gpu_exhaustive_beam_search (gpu_exhaustive_beam.py:91-325)
+    at the reference CLI defaults (elite 64, energy window 12, global anchors
+    every 25 generations) from a seeded n = 75 state; one step = one
+    generation: every legal 2-switch of every elite through a bad slot scored
+    exactly on the device, pooled, shuffled, and the host's retention step.
+    Timed by the host clock per generation (the retention step is host work)."""
+    from random import Random
+
+    from no_three_in_line_b200 import gpu_exhaustive_beam, state
+
+    snaps = []
+    total = max(3, args.warmup) + args.steps
+    gpu_exhaustive_beam.gpu_exhaustive_beam_search(state.random_state(N, Random(91001)), seed=1, generations=total,
+                                                   elite_size=64, energy_window=12, global_every=25,
+                                                   report_every=1, callback=snaps.append)
+    timed = snaps[-args.steps - 1:]
+    secs = timed[-1].elapsed_seconds - timed[0].elapsed_seconds
+    evals = timed[-1].evaluations - timed[0].evaluations
+    steps = len(timed) - 1
+    line = {"metric": METRIC, "value": evals / secs, "unit": "exact children scored/s", "n_gpus": 1,
+            "steps": steps, "warmup": len(snaps) - steps, "ms_per_step": 1e3 * secs / steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "int32",
+            "data": "synthetic: random_state(75, Random(91001)) initial state",
+            "config": {"workload": "exhaustive 2-switch beam, n=75, elite 64, window 12, global every 25",
+                       "mode": "exhaustive", "children_per_generation": evals / steps},
+            "best_E": timed[-1].best_score,
+            "timing": "host clock between generation reports (device work and the host retention step)"}
     print(json.dumps(line), flush=True)
     return 0
 
@@ -509,7 +596,7 @@ def run_time_to_target(args):
     from no_three_in_line_b200 import compare
 
     methods = tuple(m.strip() for m in args.methods.split(",") if m.strip())
-    res = compare.compare(list(range(1, args.seeds + 1)), args.target, args.budget, methods=methods)
+    res = compare.compare(list(range(1, args.seeds + 1)), args.target, args.budget, methods=methods, log=args.log)
     line = {"metric": "time-to-E<=target, learned vs plain proposal (n=75, 2048 chains, 64-temperature ladders)",
             "unit": "s", "higher_is_better": False, "target": args.target, "budget_s": args.budget,
             **{k: v for k, v in res.items() if k.startswith("plain") or k.startswith("learned")},
@@ -770,6 +857,8 @@ def main():
         return run_search_mode(args)
     if args.mode == "lines":
         return run_lines_mode(args)
+    if args.mode == "exhaustive":
+        return run_exhaustive_mode(args)
     return run_b200(args)
 
 

@@ -499,6 +499,13 @@ int n3_calibrate_det_ceiling(int blocks, int iters, unsigned long long* scratch2
  * bench.py states the scorer's roofline against.  scratch2: device uint64[2]. */
 int n3_calibrate_int_pipe(int kind, int blocks, int iters, unsigned long long* scratch2, void* stream);
 
+/* Random 4-byte gathers from `table` (int32 [entries], sized to stay in L2):
+ * blocks x 256 threads x iters loads at xorshift-drawn indices.  Event-timed,
+ * the rate is the ceiling bench.py states the pair-table scorer's gathers
+ * against.  scratch2: device uint64[2]. */
+int n3_calibrate_l2_gather(const int32_t* table, int64_t entries, int blocks, int iters,
+                           unsigned long long* scratch2, void* stream);
+
 /* Makes one bounded device wait expire, safely: an mbarrier that nothing
  * arrives on is waited for at most `tries` times (1 .. 2^20) with the wait
  * the tensor-core pipeline uses, which then ORs error bit 8 (a bounded wait

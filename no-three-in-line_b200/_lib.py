@@ -39,6 +39,7 @@ _SIGNATURES: dict[str, list] = {
     "n3_score_checked": [_P, _I, _I, _P, _P, _P, _P, _P],
     "n3_calibrate_det_ceiling": [_I, _I, _P, _P],
     "n3_calibrate_int_pipe": [_I, _I, _I, _P, _P],
+    "n3_calibrate_l2_gather": [_P, _I64, _I, _I, _P, _P],
     "n3_swap_delta": [_P, _I, _I, _P, _I, _P, _P, _P],
     "n3_swap_delta_pairs": [_P, _I, _I, _P, _I, _P, _P, _P],
     "n3_two_switch_scores": [_P, _P, _P, _I, _I, _P, _I, _P, _P],

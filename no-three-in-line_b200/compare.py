@@ -119,7 +119,9 @@ def time_to_reach(traj, level: int):
     return None
 
 
-def compare(seeds, target: int, budget: float, *, methods=("plain", "learned"), **kw) -> dict:
+def compare(seeds, target: int, budget: float, *, methods=("plain", "learned"), log=None, **kw) -> dict:
+    """Every method on every seed; with ``log`` (a path) each finished run is
+    appended to it as one JSON line, so an interrupted comparison keeps its runs."""
     specs = [parse_method(m) for m in methods]
     runs = []
     for s in seeds:
@@ -129,6 +131,9 @@ def compare(seeds, target: int, budget: float, *, methods=("plain", "learned"), 
             else:
                 runs.append(run_learned(s, target, budget, moves=sp["moves"], bad_bias=sp["bad_bias"],
                                         name=sp["name"], **kw))
+            if log is not None:
+                with open(log, "a", encoding="utf-8") as f:
+                    f.write(json.dumps(dict(asdict(runs[-1]), mae=getattr(runs[-1], "mae", None))) + "\n")
     out = {"target": target, "budget_s": budget, "runs": [dict(asdict(r), mae=getattr(r, "mae", None))
                                                           for r in runs]}
     names = [sp["name"] for sp in specs]

@@ -65,7 +65,32 @@ __global__ void __launch_bounds__(256) int_pipe_kernel(int iters, int seed, unsi
   if (x == 0x7fffffff) out[0] = (unsigned long long)x;  // keeps the chains live
 }
 
+// Random 4-byte gathers from a table that fits in L2 (the access pattern of
+// the pair-table scorer): each thread draws `iters` indices with a 32-bit
+// xorshift and sums the entries.  Gathers per launch = blocks * 256 * iters.
+__global__ void __launch_bounds__(256) l2_gather_kernel(const int32_t* __restrict__ table, uint32_t entries,
+                                                        int iters, int seed, unsigned long long* out) {
+  uint32_t x = (threadIdx.x + blockIdx.x * 256u) * 2654435761u + (uint32_t)seed + 1u;
+  int sum = 0;
+#pragma unroll 8
+  for (int it = 0; it < iters; ++it) {
+    x ^= x << 13;
+    x ^= x >> 17;
+    x ^= x << 5;
+    sum += __ldg(table + __umulhi(x, entries));
+  }
+  if (sum == 0x7fffffff) out[0] = (unsigned long long)sum;  // keeps the loads live
+}
+
 }  // namespace n3
+
+extern "C" int n3_calibrate_l2_gather(const int32_t* table, int64_t entries, int blocks, int iters,
+                                      unsigned long long* scratch2, void* stream) {
+  if (!table || entries < 1 || entries > 0xFFFFFFFFll || blocks < 1 || iters < 1 || !scratch2)
+    return n3host::set_error(N3_ERR_ARG, "calibrate: bad arguments");
+  n3::l2_gather_kernel<<<blocks, 256, 0, (cudaStream_t)stream>>>(table, (uint32_t)entries, iters, blocks, scratch2);
+  return n3host::check_launch("l2_gather_kernel");
+}
 
 extern "C" int n3_calibrate_int_pipe(int kind, int blocks, int iters, unsigned long long* scratch2, void* stream) {
   if (blocks < 1 || iters < 1 || scratch2 == nullptr || (kind != 0 && kind != 1))

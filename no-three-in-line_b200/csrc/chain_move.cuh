@@ -37,12 +37,18 @@ __device__ __forceinline__ bool umbrella_accept(int dE, int64_t umb_q, uint32_t 
 
 // FORCE: the move is applied whatever its dE (no Metropolis test).
 // UMB: the test adds the umbrella term umb_q (umbrella_accept).
-template <bool FORCE, bool UMB = false>
+// EARLY (plain Metropolis only): after the first new-side histogram,
+//   dE >= d1 = t(u') + j(u', v') - (bad[u] + bad[v] - joint)
+// because t(v') >= 0, and thr is non-increasing, so a proposal with d1 >= 1 and
+// (d1 >= W or z >= thr[d1]) is rejected exactly as the full test would reject
+// it, without the second histogram; *dE_out then holds d1.
+template <bool FORCE, bool UMB = false, bool EARLY = false>
 __device__ __forceinline__ int move_exact_t(int* __restrict__ cs, int* __restrict__ bs, int m,
                                             const uint16_t* __restrict__ lutf, uint32_t* __restrict__ hist, int lane,
                                             int u, int v, uint32_t z, const uint32_t* __restrict__ thr, int W, int& E,
                                             uint32_t& err, int* dE_out, int64_t umb_q = 0,
                                             const uint32_t* __restrict__ frac = nullptr) {
+  static_assert(!(EARLY && (FORCE || UMB)), "the early rejection needs the plain Metropolis test");
   const int ru = u >> 1, rv = v >> 1, cu = cs[u], cv = cs[v];
   int ids[kSlotsPerLane], cnt_new[kSlotsPerLane];
   // centre u' = (r_u, c_v)
@@ -50,6 +56,27 @@ __device__ __forceinline__ int move_exact_t(int* __restrict__ cs, int* __restric
   __syncwarp();
   const int line_new = dir_id_full(lutf, rv - ru, cu - cv);
   const int j_new = hist_get(hist, line_new);
+  // points of A on the old line (u, v)
+  int joint = 0;
+#pragma unroll
+  for (int t = 0; t < kSlotsPerLane; ++t) {
+    const int k = lane + 32 * t;
+    if (k < m && k != u && k != v) joint += (rv - ru) * (cs[k] - cu) == (cv - cu) * ((k >> 1) - ru);
+  }
+  int t_a, sum_joint;
+  if constexpr (EARLY) {
+    const int s1 = warp_sum(part_a + (joint << 16));
+    t_a = s1 & 0xFFFF;
+    sum_joint = s1 >> 16;
+    const int d1 = t_a + j_new - (bs[u] + bs[v] - sum_joint);
+    if (d1 >= 1 && (d1 >= W || z >= thr[d1])) {
+      __syncwarp();
+      hist_release(hist, ids);
+      __syncwarp();
+      *dE_out = d1;
+      return 0;
+    }
+  }
 #pragma unroll
   for (int t = 0; t < kSlotsPerLane; ++t)
     cnt_new[t] = ids[t] >= 0 ? hist_get(hist, ids[t]) - 1 + (ids[t] == line_new) : 0;
@@ -63,16 +90,15 @@ __device__ __forceinline__ int move_exact_t(int* __restrict__ cs, int* __restric
   for (int t = 0; t < kSlotsPerLane; ++t) cnt_new[t] += ids[t] >= 0 ? hist_get(hist, ids[t]) - 1 : 0;
   __syncwarp();
   hist_release(hist, ids);
-  // points of A on the old line (u, v)
-  int joint = 0;
-#pragma unroll
-  for (int t = 0; t < kSlotsPerLane; ++t) {
-    const int k = lane + 32 * t;
-    if (k < m && k != u && k != v) joint += (rv - ru) * (cs[k] - cu) == (cv - cu) * ((k >> 1) - ru);
+  int t_b;
+  if constexpr (EARLY) {
+    t_b = warp_sum(part_b);
+  } else {
+    const int sum_ab = warp_sum(part_a + (part_b << 16));
+    sum_joint = warp_sum(joint);
+    t_a = sum_ab & 0xFFFF;
+    t_b = sum_ab >> 16;
   }
-  const int sum_ab = warp_sum(part_a + (part_b << 16));
-  const int sum_joint = warp_sum(joint);
-  const int t_a = sum_ab & 0xFFFF, t_b = sum_ab >> 16;
   const int dE = (t_a + t_b + j_new) - (bs[u] + bs[v] - sum_joint);
   *dE_out = dE;
   const bool accept = FORCE || (UMB ? umbrella_accept(dE, umb_q, z, thr, W, frac)
@@ -197,7 +223,7 @@ __device__ __forceinline__ int propose_walk(int* __restrict__ cs, int* __restric
   }
   if (!legal_swap(cs, u, v)) return 0;
   int dE;
-  if (!UMB) return move_exact(cs, bs, m, lutf, hist, lane, u, v, rnd.z, thr, W, E, err, &dE);
+  if (!UMB) return move_exact_t<false, false, true>(cs, bs, m, lutf, hist, lane, u, v, rnd.z, thr, W, E, err, &dE);
   const int dd = umbrella_distance_delta(P.ref, u, v, cs[u], cs[v]);
   const int64_t umb = P.s_q * (int64_t)(2 * removed * dd + dd * dd) - P.c2s_q * (int64_t)dd;
   const int acc = move_exact_t<false, true>(cs, bs, m, lutf, hist, lane, u, v, rnd.z, thr, W, E, err, &dE, umb,

@@ -19,8 +19,11 @@
 //   D1 = A1 (128 x 16) [W1a | hi | lo]^T  -> ReLU, bf16 -> A2 (shared memory)
 //   D2 = A2 (128 x 256) W2^T              -> + b2, ReLU, . w3 + b3 -> predicted dE
 // both on tcgen05 with fp32 accumulators in tensor memory.
-// Training (SIMT fp32, hand-written GEMMs) uses MSE on dE / kTargetScale with
-// Adam; the packed bf16 images are rebuilt after each update.
+// Training uses MSE on dE / kTargetScale with Adam: the five GEMMs of a step
+// (two forward layers, two weight gradients, the backward through layer 2) run
+// on tcgen05 with bf16 operands and fp32 accumulators (tc_gemm_kernel), the
+// head, bias gradients and Adam in fp32 SIMT; the packed bf16 images are
+// rebuilt after each update.  fp32 master weights.
 #include <cuda.h>
 #include <cuda_bf16.h>
 #include <mutex>
@@ -206,13 +209,13 @@ __global__ void __launch_bounds__(kCand) candidates_kernel(const CandArgs A) {
 
 // Chain part of layer 1 for every chain: c1[c][n] = b1[n] + sum_k W1[n][12 + k] badn[c][k]
 // (k < 150).  One thread per output column n, kChainTile chains per CTA (their
-// badness rows staged in shared memory, zero-padded to 160; 2048 chains make 293
-// CTAs, two per SM).  W1's chain columns pass through shared memory in chunks of
+// badness rows staged in shared memory, zero-padded to 160; 2048 chains make 128
+// CTAs, so each CTA's pass over W1's chain columns serves 16 chains).  W1's chain columns pass through shared memory in chunks of
 // 32, read row-contiguously (coalesced, the next chunk in flight while this one
 // is used) and stored transposed with a 257-float stride (no bank conflicts
 // either way).  Columns up to 171 stay inside the 192-wide rows.  Deterministic:
 // one thread sums each output in a fixed order.
-constexpr int kChainTile = 7;
+constexpr int kChainTile = 16;
 constexpr int kChainPad = 160;
 constexpr int kWStride = kH + 1;
 __global__ void __launch_bounds__(kH) chain_part_kernel(int C, const float* __restrict__ badn,
@@ -723,7 +726,7 @@ __global__ void __launch_bounds__(kStepWarps * 32, 1) learned_step_kernel(const 
 }
 
 // ---------------------------------------------------------------------------
-// Training (SIMT fp32).
+// Training: batch gather, tensor-core GEMMs, fp32 head, bias sums and Adam.
 // ---------------------------------------------------------------------------
 struct Batch {
   float* X;   // [B][192]
@@ -762,101 +765,144 @@ __global__ void gather_kernel(const uint16_t* __restrict__ rb_feat, const uint8_
   }
 }
 
-// C[M x N] = sum_k A(m, k) B(k, n), A(m,k) = A[m*sam + k*sak], B(k,n) = B[k*sbk + n*sbn].
-// EPI 0: C = acc (+ atomically when split over gridDim.z)
-// EPI 1: Z = acc + bias[n]; C = relu(Z); aux = Z
-// EPI 2: C = acc * (aux[m, n] > 0)
-template <int EPI>
-__global__ void __launch_bounds__(256) gemm_kernel(int M, int N, int K, const float* __restrict__ A, int sam, int sak,
-                                                   const float* __restrict__ Bm, int sbk, int sbn,
-                                                   float* __restrict__ C, int ldc, const float* __restrict__ bias,
-                                                   float* __restrict__ aux) {
-  __shared__ float As[16][64 + 4];
-  __shared__ float Bs[16][64 + 4];
-  const int tx = threadIdx.x % 16, ty = threadIdx.x / 16;
-  const int m0 = blockIdx.y * 64, n0 = blockIdx.x * 64;
-  const int kchunk = (K + gridDim.z - 1) / gridDim.z;
-  const int kb = blockIdx.z * kchunk, ke = min(K, kb + kchunk);
-  float acc[4][4] = {};
-  // Each thread moves 4 A and 4 B elements per 16-deep tile; consecutive threads
-  // walk whichever index is contiguous in memory.  The next tile is fetched into
-  // registers while the current one is multiplied.
-  float ra[4], rb[4];
-  auto fetch = [&](int k0) {
-#pragma unroll
-    for (int r = 0; r < 4; ++r) {
-      const int i = threadIdx.x + 256 * r;
-      const int ka = sak == 1 ? (i & 15) : (i >> 6), ma = sak == 1 ? (i >> 4) : (i & 63);
-      const int kq = sbk == 1 ? (i & 15) : (i >> 6), nq = sbk == 1 ? (i >> 4) : (i & 63);
-      const int gka = k0 + ka, gkb = k0 + kq;
-      ra[r] = (m0 + ma < M && gka < ke) ? A[(size_t)(m0 + ma) * sam + (size_t)gka * sak] : 0.f;
-      rb[r] = (n0 + nq < N && gkb < ke) ? Bm[(size_t)gkb * sbk + (size_t)(n0 + nq) * sbn] : 0.f;
+
+// out = H2 . w3 + b3, d = 2 (out - y) / B, dZ2 = d w3 (Z2 > 0), loss += (out - y)^2
+// Training GEMMs on the tensor cores (tcgen05, kind::f16): C (M x N, fp32) =
+// sum_k A(m, k) B(k, n) for fp32 operands given by element strides (A(m, k) at
+// A[m sam + k sak], B(k, n) at Bm[k sbk + n sbn]), with the epilogues of the
+// training step: EPI 0 store (or add, with a K split over gridDim.z: the
+// weight gradients), EPI 1 Z = acc + bias, H = relu(Z) (the forward layers),
+// EPI 2 acc masked by Z > 0 (back through a ReLU).
+//
+// A CTA of 4 warps owns a 128 x kTcN output tile.  Per K slice of 64 it rounds
+// the operands to bf16 while staging them into 128B-swizzled K-major shared
+// tiles (two buffers: the next slice is staged while the tensor core reads the
+// current one), thread 0 issues the slice's four K = 16 MMAs into a 128 x kTcN
+// fp32 accumulator in tensor memory and commits them to the buffer's mbarrier,
+// and the epilogue reads the accumulator back with tcgen05.ld (warp w: rows
+// 32 w .. 32 w + 31).  Every mbarrier wait is bounded; an expired wait sets
+// error bit 8 and skips the epilogue.
+constexpr int kTcN = 64;                            // output columns per CTA (tensor-memory columns)
+constexpr uint32_t kTcA = 128 * 128;                // bytes of one A slice (128 rows x 64 bf16)
+constexpr uint32_t kTcB = kTcN * 128;               // bytes of one B slice
+constexpr uint32_t kTcBar = 2 * (kTcA + kTcB);      // two mbarriers and the tensor-memory address
+constexpr uint32_t kTcSmem = kTcBar + 64 + 1024;    // + alignment slack
+
+// Stages rows x 64 elements of an operand, element (r, k) at src[(r0 + r) sr + (k0 + k) sk],
+// zero outside r0 + r < R, k0 + k < Ke, into an SW128 K-major bf16 tile.
+__device__ __forceinline__ void tc_stage(uint8_t* tile, int rows, const float* __restrict__ src, int sr, int sk,
+                                         int r0, int R, int k0, int Ke, int tid) {
+  if (sk == 1) {  // k contiguous: pairs of k per thread, a warp reads 64 consecutive floats of a row
+    for (int i = tid; i < rows * 32; i += 128) {
+      const int r = i >> 5, k = 2 * (i & 31);
+      const bool rin = r0 + r < R;
+      const float a = rin && k0 + k < Ke ? src[(size_t)(r0 + r) * sr + (k0 + k)] : 0.f;
+      const float b = rin && k0 + k + 1 < Ke ? src[(size_t)(r0 + r) * sr + (k0 + k + 1)] : 0.f;
+      *reinterpret_cast<uint32_t*>(tile + umma::sw128_offset(r, k, rows)) = bf16x2_bits(a, b);
     }
-  };
-  auto stash = [&]() {
-#pragma unroll
-    for (int r = 0; r < 4; ++r) {
-      const int i = threadIdx.x + 256 * r;
-      const int ka = sak == 1 ? (i & 15) : (i >> 6), ma = sak == 1 ? (i >> 4) : (i & 63);
-      const int kq = sbk == 1 ? (i & 15) : (i >> 6), nq = sbk == 1 ? (i >> 4) : (i & 63);
-      As[ka][ma] = ra[r];
-      Bs[kq][nq] = rb[r];
-    }
-  };
-  if (kb < ke) {
-    fetch(kb);
-    stash();
-  }
-  __syncthreads();
-  for (int k0 = kb; k0 < ke; k0 += 16) {
-    const bool more = k0 + 16 < ke;
-    if (more) fetch(k0 + 16);
-#pragma unroll
-    for (int kk = 0; kk < 16; ++kk) {
-      float a[4], b[4];
-#pragma unroll
-      for (int i = 0; i < 4; ++i) {
-        a[i] = As[kk][ty * 4 + i];
-        b[i] = Bs[kk][tx * 4 + i];
-      }
-#pragma unroll
-      for (int i = 0; i < 4; ++i)
-#pragma unroll
-        for (int j = 0; j < 4; ++j) acc[i][j] = fmaf(a[i], b[j], acc[i][j]);
-    }
-    __syncthreads();
-    if (more) {
-      stash();
-      __syncthreads();
-    }
-  }
-#pragma unroll
-  for (int i = 0; i < 4; ++i) {
-    const int mm = m0 + ty * 4 + i;
-    if (mm >= M) continue;
-#pragma unroll
-    for (int j = 0; j < 4; ++j) {
-      const int nn = n0 + tx * 4 + j;
-      if (nn >= N) continue;
-      float v = acc[i][j];
-      const size_t o = (size_t)mm * ldc + nn;
-      if (EPI == 0) {
-        if (gridDim.z > 1)
-          atomicAdd(C + o, v);
-        else
-          C[o] = v;
-      } else if (EPI == 1) {
-        v += bias[nn];
-        aux[o] = v;
-        C[o] = fmaxf(v, 0.f);
-      } else {
-        C[o] = aux[o] > 0.f ? v : 0.f;
-      }
+  } else {  // rows contiguous (or neither): a warp reads 32 consecutive rows of one k
+    for (int i = tid; i < rows * 64; i += 128) {
+      const int k = i / rows, r = i % rows;
+      const float a = r0 + r < R && k0 + k < Ke ? src[(size_t)(r0 + r) * sr + (size_t)(k0 + k) * sk] : 0.f;
+      *reinterpret_cast<uint16_t*>(tile + umma::sw128_offset(r, k, rows)) = bf16_bits(a);
     }
   }
 }
 
-// out = H2 . w3 + b3, d = 2 (out - y) / B, dZ2 = d w3 (Z2 > 0), loss += (out - y)^2
+template <int EPI>
+__global__ void __launch_bounds__(128) tc_gemm_kernel(int M, int N, int K, const float* __restrict__ A, int sam,
+                                                      int sak, const float* __restrict__ Bm, int sbk, int sbn,
+                                                      float* __restrict__ C, int ldc, const float* __restrict__ bias,
+                                                      float* __restrict__ aux, uint32_t* error_word) {
+  extern __shared__ __align__(16) uint8_t tc_smem[];
+  const uint32_t raw = umma::smem_addr(tc_smem);
+  const uint32_t base = (raw + 1023u) & ~1023u;
+  uint8_t* sm = tc_smem + (base - raw);
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  const int m0 = blockIdx.y * 128, n0 = blockIdx.x * kTcN;
+  const int kchunk = ((K + (int)gridDim.z - 1) / (int)gridDim.z + 63) / 64 * 64;
+  const int kb = blockIdx.z * kchunk, ke = min(K, kb + kchunk);
+  const int slices = kb < ke ? (ke - kb + 63) / 64 : 0;
+  if (slices == 0) return;  // a K split with nothing to add (uniform across the CTA)
+  const uint32_t bar0 = base + kTcBar, bar1 = bar0 + 8, taddr_slot = bar0 + 16;
+  if (warp == 0) {
+    umma::tmem_alloc(taddr_slot, kTcN);
+    umma::tmem_relinquish();
+  }
+  if (tid == 0) {
+    umma::mbar_init(bar0, 1);
+    umma::mbar_init(bar1, 1);
+    umma::mbar_fence_init();
+  }
+  umma::fence_before_sync();
+  __syncthreads();
+  umma::fence_after_sync();
+  const uint32_t tmem = *reinterpret_cast<volatile uint32_t*>(sm + kTcBar + 16);
+  constexpr uint32_t idesc = umma::idesc_bf16_f32(128, kTcN);
+  bool ok = true;
+  for (int s = 0; s < slices; ++s) {
+    const int buf = s & 1;
+    const uint32_t bar = buf ? bar1 : bar0;
+    // the MMAs of slice s - 2 read this buffer: wait for their commit
+    if (s >= 2) ok = ok && umma::mbar_wait(bar, (uint32_t)((s - 2) >> 1) & 1u, kWaitTries);
+    uint8_t* ta = sm + buf * (kTcA + kTcB);
+    uint8_t* tb = ta + kTcA;
+    const int k0 = kb + 64 * s;
+    tc_stage(ta, 128, A, sam, sak, m0, M, k0, ke, tid);
+    tc_stage(tb, kTcN, Bm, sbn, sbk, n0, N, k0, ke, tid);
+    umma::fence_async_smem();
+    umma::fence_before_sync();
+    __syncthreads();
+    if (tid == 0) {
+      umma::fence_after_sync();
+      const uint32_t a_s = base + buf * (kTcA + kTcB), b_s = a_s + kTcA;
+#pragma unroll
+      for (int k16 = 0; k16 < 4; ++k16)
+        umma::mma_bf16(tmem, umma::desc_sw128(a_s + 32 * k16), umma::desc_sw128(b_s + 32 * k16), idesc,
+                       (s > 0 || k16 > 0) ? 1u : 0u);
+      umma::commit(bar);
+    }
+  }
+  // the last commit covers every MMA issued before it
+  const int last = slices - 1;
+  ok = ok && umma::mbar_wait((last & 1) ? bar1 : bar0, (uint32_t)(last >> 1) & 1u, kWaitTries);
+  ok = __syncthreads_and(ok);
+  umma::fence_after_sync();
+  if (ok) {
+    const int row = m0 + 32 * warp + lane;
+#pragma unroll 1
+    for (int c0 = 0; c0 < kTcN; c0 += 32) {
+      float v[32];
+      umma::tmem_ld32(tmem + ((uint32_t)(32 * warp) << 16) + (uint32_t)c0, v);
+      if (row < M) {
+#pragma unroll
+        for (int j = 0; j < 32; ++j) {
+          const int nn = n0 + c0 + j;
+          if (nn >= N) continue;
+          const size_t o = (size_t)row * ldc + nn;
+          if (EPI == 0) {
+            if (gridDim.z > 1)
+              atomicAdd(C + o, v[j]);
+            else
+              C[o] = v[j];
+          } else if (EPI == 1) {
+            const float z = v[j] + bias[nn];
+            aux[o] = z;
+            C[o] = fmaxf(z, 0.f);
+          } else {
+            C[o] = aux[o] > 0.f ? v[j] : 0.f;
+          }
+        }
+      }
+    }
+  } else if (tid == 0 && error_word) {
+    atomicOr(error_word, kErrTimeout);
+  }
+  umma::fence_before_sync();
+  __syncthreads();
+  if (warp == 0) umma::tmem_dealloc(tmem, kTcN);
+}
+
 __global__ void head_kernel(int B, const float* __restrict__ H2, const float* __restrict__ Z2,
                             const float* __restrict__ P, const float* __restrict__ y, float* __restrict__ d,
                             float* __restrict__ dZ2, float* __restrict__ loss) {
@@ -975,24 +1021,33 @@ static int train_step(const n3_mlp* M, int n_chains, int B, float lr, uint64_t s
     return check_launch("MLP training: clearing the gradient");
   gather_kernel<<<B, 64, 0, st>>>(M->rb_feat, M->rb_bad, M->rb_dE, M->counters, M->rb_capacity, n_chains, B,
                                   (uint32_t)seed, (uint32_t)(seed >> 32), X, y);
-  const dim3 g_fwd(kH / 64, (B + 63) / 64, 1);
+  // tensor-core GEMMs (tc_gemm_kernel): 128-row tiles of kTcN columns; the
+  // weight gradients split K = batch over up to 16 CTAs per tile
+  N3_TRY(allow_smem(reinterpret_cast<const void*>(tc_gemm_kernel<0>), kTcSmem));
+  N3_TRY(allow_smem(reinterpret_cast<const void*>(tc_gemm_kernel<1>), kTcSmem));
+  N3_TRY(allow_smem(reinterpret_cast<const void*>(tc_gemm_kernel<2>), kTcSmem));
+  const int row_tiles = (B + 127) / 128;
+  const int splits = B >= 4096 ? 16 : B >= 512 ? B / 256 : 1;
+  uint32_t* ew = M->error_word;
   // Z1 = X W1^T + b1 ; H1 = relu(Z1)     (W1 [256][192]: B(k, n) = W1[n*192 + k])
-  gemm_kernel<1><<<g_fwd, 256, 0, st>>>(B, kH, kIn, X, kIn, 1, P + oW1, 1, kIn, H1, kH, P + oB1, Z1);
-  gemm_kernel<1><<<g_fwd, 256, 0, st>>>(B, kH, kH, H1, kH, 1, P + oW2, 1, kH, H2, kH, P + oB2, Z2);
+  tc_gemm_kernel<1><<<dim3(kH / kTcN, row_tiles, 1), 128, kTcSmem, st>>>(B, kH, kIn, X, kIn, 1, P + oW1, 1, kIn,
+                                                                          H1, kH, P + oB1, Z1, ew);
+  tc_gemm_kernel<1><<<dim3(kH / kTcN, row_tiles, 1), 128, kTcSmem, st>>>(B, kH, kH, H1, kH, 1, P + oW2, 1, kH,
+                                                                          H2, kH, P + oB2, Z2, ew);
   head_kernel<<<(B + 7) / 8, 256, 0, st>>>(B, H2, Z2, P, y, d, dZ2, loss);
   // gradients of the head and layer 2
   colsum_kernel<<<dim3((kH + 127) / 128, (B + kColRows - 1) / kColRows), 128, 0, st>>>(B, kH, H2, d, grads + oW3);
   sum_kernel<<<1, 1024, 0, st>>>(B, d, grads + oB3);
-  const int splits = B >= 2048 ? 16 : 4;
   // gW2[n][k] = sum_b dZ2[b][n] H1[b][k]
-  gemm_kernel<0><<<dim3(kH / 64, kH / 64, splits), 256, 0, st>>>(kH, kH, B, dZ2, 1, kH, H1, kH, 1, grads + oW2, kH,
-                                                                   nullptr, nullptr);
+  tc_gemm_kernel<0><<<dim3(kH / kTcN, kH / 128, splits), 128, kTcSmem, st>>>(kH, kH, B, dZ2, 1, kH, H1, kH, 1,
+                                                                              grads + oW2, kH, nullptr, nullptr, ew);
   colsum_kernel<<<dim3((kH + 127) / 128, (B + kColRows - 1) / kColRows), 128, 0, st>>>(B, kH, dZ2, nullptr, grads + oB2);
   // dZ1 = (dZ2 W2) * (Z1 > 0)            (B(k, n) = W2[k*256 + n])
-  gemm_kernel<2><<<g_fwd, 256, 0, st>>>(B, kH, kH, dZ2, kH, 1, P + oW2, kH, 1, dZ1, kH, nullptr, Z1);
+  tc_gemm_kernel<2><<<dim3(kH / kTcN, row_tiles, 1), 128, kTcSmem, st>>>(B, kH, kH, dZ2, kH, 1, P + oW2, kH, 1,
+                                                                          dZ1, kH, nullptr, Z1, ew);
   // gW1[n][k] = sum_b dZ1[b][n] X[b][k]
-  gemm_kernel<0><<<dim3(kIn / 64, kH / 64, splits), 256, 0, st>>>(kH, kIn, B, dZ1, 1, kH, X, kIn, 1, grads + oW1,
-                                                                    kIn, nullptr, nullptr);
+  tc_gemm_kernel<0><<<dim3(kIn / kTcN, kH / 128, splits), 128, kTcSmem, st>>>(kH, kIn, B, dZ1, 1, kH, X, kIn, 1,
+                                                                               grads + oW1, kIn, nullptr, nullptr, ew);
   colsum_kernel<<<dim3((kH + 127) / 128, (B + kColRows - 1) / kColRows), 128, 0, st>>>(B, kH, dZ1, nullptr, grads + oB1);
   adam_kernel<<<(kParams + 255) / 256, 256, 0, st>>>(kParams, P, grads, adam_m, adam_v, lr, 0.9f, 0.999f, 1e-8f,
                                                      M->counters);

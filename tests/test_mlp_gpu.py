@@ -73,6 +73,11 @@ def test_inference_matches_bf16_reference(cuda):
 
 
 def test_training_gradients_match_autograd(cuda):
+    """The five training GEMMs run on the tensor cores with bf16 operands and
+    fp32 accumulation: each is checked against an fp64 product of the same
+    bf16-rounded device operands (only the summation order differs); the head,
+    bias sums and Adam in fp32 against fp64 formulas; and the whole gradient
+    against fp64 autograd of the unrounded network within the bf16 tolerance."""
     import torch
 
     ch = make(chains=64, L=16)
@@ -82,31 +87,70 @@ def test_training_gradients_match_autograd(cuda):
     p0 = lp.params.clone()
     lp.train()
     torch.cuda.synchronize()
-    B = lp.batch
-    X = lp.scratch[:B * 192].view(B, 192).double().cpu()
-    y = lp.scratch[B * 192:B * 192 + B].double().cpu()
-    P = p0.double().cpu().requires_grad_(True)
-    W1 = P[learned.O_W1:learned.O_B1].view(256, 192)
+    B, H = lp.batch, 256
+    sc = lp.scratch.double().cpu().numpy()
+    off = 0
+
+    def take(size, shape):
+        nonlocal off
+        a = sc[off:off + size].reshape(shape)
+        off += size
+        return a
+
+    X, y, d = take(B * 192, (B, 192)), take(B, (B,)), take(B, (B,))
+    Z1, H1, Z2, H2, dZ2, dZ1 = (take(B * H, (B, H)) for _ in range(6))
+    P = p0.double().cpu().numpy()
+    W1 = P[learned.O_W1:learned.O_B1].reshape(H, 192)
     b1 = P[learned.O_B1:learned.O_W2]
-    W2 = P[learned.O_W2:learned.O_B2].view(256, 256)
+    W2 = P[learned.O_W2:learned.O_B2].reshape(H, H)
     b2 = P[learned.O_B2:learned.O_W3]
     w3 = P[learned.O_W3:learned.O_B3]
-    b3 = P[learned.O_B3]
-    h1 = torch.relu(X @ W1.T + b1)
-    h2 = torch.relu(h1 @ W2.T + b2)
-    out = h2 @ w3 + b3
-    loss = ((out - y) ** 2).mean()
+    g = lp.grads.double().cpu().numpy()
+    gW1 = g[learned.O_W1:learned.O_B1].reshape(H, 192)
+    gW2 = g[learned.O_W2:learned.O_B2].reshape(H, H)
+
+    def close(got, want, rtol=2e-4):
+        scale = max(np.abs(want).max(), 1e-30)
+        assert np.allclose(got, want, rtol=rtol, atol=rtol * scale), np.abs(got - want).max() / scale
+
+    # tensor-core GEMMs against fp64 on the same bf16-rounded operands
+    close(Z1, bf16(X) @ bf16(W1).T + b1)
+    assert np.array_equal(H1, np.maximum(Z1, 0))
+    close(Z2, bf16(H1) @ bf16(W2).T + b2)
+    assert np.array_equal(H2, np.maximum(Z2, 0))
+    close(gW2, bf16(dZ2).T @ bf16(H1))
+    close(dZ1, (bf16(dZ2) @ bf16(W2)) * (Z1 > 0))
+    close(gW1, bf16(dZ1).T @ bf16(X))
+    # fp32 parts: bias sums and the head's gradients from the device activations
+    close(g[learned.O_B1:learned.O_W2], dZ1.sum(0), rtol=1e-5)
+    close(g[learned.O_B2:learned.O_W3], dZ2.sum(0), rtol=1e-5)
+    close(g[learned.O_W3:learned.O_B3], H2.T @ d, rtol=1e-5)
+    assert abs(g[learned.O_B3] - d.sum()) <= 1e-5 * (1 + np.abs(d).sum())
+    close(dZ2, d[:, None] * w3[None, :] * (Z2 > 0), rtol=1e-5)
+    # the whole gradient against autograd of the unrounded fp64 network
+    Pt = p0.double().cpu().requires_grad_(True)
+    tW1 = Pt[learned.O_W1:learned.O_B1].view(H, 192)
+    tb1 = Pt[learned.O_B1:learned.O_W2]
+    tW2 = Pt[learned.O_W2:learned.O_B2].view(H, H)
+    tb2 = Pt[learned.O_B2:learned.O_W3]
+    tw3 = Pt[learned.O_W3:learned.O_B3]
+    tb3 = Pt[learned.O_B3]
+    Xt, yt = torch.from_numpy(X), torch.from_numpy(y)
+    h1 = torch.relu(Xt @ tW1.T + tb1)
+    h2 = torch.relu(h1 @ tW2.T + tb2)
+    out = h2 @ tw3 + tb3
+    loss = ((out - yt) ** 2).mean()
     loss.backward()
-    g_ref = P.grad.numpy()
-    g = lp.grads.cpu().numpy().astype(np.float64)
-    scale = np.abs(g_ref).max()
-    assert np.allclose(g[:learned.O_B3 + 1], g_ref[:learned.O_B3 + 1], rtol=1e-3, atol=1e-4 * scale)
+    g_ref = Pt.grad.numpy()
+    for lo, hi in ((learned.O_W1, learned.O_B1), (learned.O_W2, learned.O_B2), (learned.O_W3, learned.O_B3)):
+        err = np.linalg.norm(g[lo:hi] - g_ref[lo:hi]) / max(np.linalg.norm(g_ref[lo:hi]), 1e-30)
+        assert err < 3e-2, (lo, err)
     # the applied update is Adam's first step from these gradients
     m = 0.1 * g
     v = 0.001 * g * g
-    p1_ref = p0.double().cpu().numpy() - 1e-3 * (m / 0.1) / (np.sqrt(v / 0.001) + 1e-8)
+    p1_ref = P - 1e-3 * (m / 0.1) / (np.sqrt(v / 0.001) + 1e-8)
     assert np.allclose(lp.params.cpu().numpy(), p1_ref, rtol=1e-5, atol=1e-6)
-    assert abs(float(lp.loss.item()) / B - float(loss)) < 1e-3 * (1 + float(loss))
+    assert abs(float(lp.loss.item()) / B - float(loss)) < 2e-2 * (1 + float(loss))
 
 
 def test_learned_steps_keep_energies_exact(cuda):
