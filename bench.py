@@ -77,6 +77,8 @@ def parse():
                     help="time-to-target: comma-separated methods: plain, plain:b<bias>, learned, "
                          "learned:x<moves>, learned:x<moves>:b<bias> (b = the walk's badness-biased share)")
     ap.add_argument("--log", type=str, default=None, help="time-to-target: append each finished run to this JSONL file")
+    ap.add_argument("--anneal-sweeps", type=int, default=0,
+                    help="tempering / learned: untimed sweeps first, so the timed rounds run at low energies")
     ap.add_argument("--learned-moves", type=str, default="1",
                     help="time-to-target: comma-separated moves per learned step to compare (1 = one move per "
                          "step); learned: the first value is the moves per step")
@@ -357,6 +359,9 @@ def run_chain_mode(args):
     pc, qc = state.seeded_population(N, 2048)
     ch = tempering.TemperingChains(state.pq_to_columns(pc, qc), np.tile(tempering.geometric_ladder(0.05, 5.0, 64), 32),
                                    seed=1, ladder_size=64)
+    if args.anneal_sweeps:
+        ch.run(args.anneal_sweeps - args.anneal_sweeps % 10, exchange_every=10, sweeps_per_launch=100)
+    e_start = ch.energy.float().mean().item()
     if args.mode == "tempering":
         step = lambda: ch.run(10, exchange_every=10, sweeps_per_launch=10)  # noqa: E731
         per_step, unit, what = 2048 * 150 * 10, "deltas/s", "exact swap deltas (proposals)"
@@ -378,8 +383,9 @@ def run_chain_mode(args):
             "scaling": "weak", "vs_baseline": None, "dtype": "int32" if args.mode == "tempering" else "bf16",
             "data": "synthetic: random_state(75, Random(91001+c)) chain starts",
             "config": {"workload": f"n=75, 2048 chains, 32 ladders x 64 temperatures (0.05..5.0): {what}",
-                       "mode": args.mode, **({"moves_per_step": moves} if args.mode == "learned" else {})},
-            "best_E": int(ch.best_energy.min().item())}
+                       "mode": args.mode, **({"moves_per_step": moves} if args.mode == "learned" else {}),
+                       "anneal_sweeps": args.anneal_sweeps},
+            "mean_E_at_start": e_start, "best_E": int(ch.best_energy.min().item())}
     print(json.dumps(line), flush=True)
     return 0
 

@@ -209,13 +209,13 @@ __global__ void __launch_bounds__(kCand) candidates_kernel(const CandArgs A) {
 
 // Chain part of layer 1 for every chain: c1[c][n] = b1[n] + sum_k W1[n][12 + k] badn[c][k]
 // (k < 150).  One thread per output column n, kChainTile chains per CTA (their
-// badness rows staged in shared memory, zero-padded to 160; 2048 chains make 128
-// CTAs, so each CTA's pass over W1's chain columns serves 16 chains).  W1's chain columns pass through shared memory in chunks of
+// badness rows staged in shared memory, zero-padded to 160; 2048 chains make 293
+// CTAs, two per SM; 16 chains per CTA measured slower).  W1's chain columns pass through shared memory in chunks of
 // 32, read row-contiguously (coalesced, the next chunk in flight while this one
 // is used) and stored transposed with a 257-float stride (no bank conflicts
 // either way).  Columns up to 171 stay inside the 192-wide rows.  Deterministic:
 // one thread sums each output in a fixed order.
-constexpr int kChainTile = 16;
+constexpr int kChainTile = 7;
 constexpr int kChainPad = 160;
 constexpr int kWStride = kH + 1;
 __global__ void __launch_bounds__(kH) chain_part_kernel(int C, const float* __restrict__ badn,
@@ -788,23 +788,39 @@ constexpr uint32_t kTcB = kTcN * 128;               // bytes of one B slice
 constexpr uint32_t kTcBar = 2 * (kTcA + kTcB);      // two mbarriers and the tensor-memory address
 constexpr uint32_t kTcSmem = kTcBar + 64 + 1024;    // + alignment slack
 
-// Stages rows x 64 elements of an operand, element (r, k) at src[(r0 + r) sr + (k0 + k) sk],
-// zero outside r0 + r < R, k0 + k < Ke, into an SW128 K-major bf16 tile.
-__device__ __forceinline__ void tc_stage(uint8_t* tile, int rows, const float* __restrict__ src, int sr, int sk,
-                                         int r0, int R, int k0, int Ke, int tid) {
-  if (sk == 1) {  // k contiguous: pairs of k per thread, a warp reads 64 consecutive floats of a row
-    for (int i = tid; i < rows * 32; i += 128) {
-      const int r = i >> 5, k = 2 * (i & 31);
+// Stages ROWS x 64 elements of an operand, element (r, k) at src[(r0 + r) sr + (k0 + k) sk],
+// zero outside r0 + r < R, k0 + k < Ke, into an SW128 K-major bf16 tile.  All
+// of a thread's loads are issued before any conversion (a fixed count per
+// thread, in registers), so their latencies overlap.
+template <int ROWS>
+__device__ __forceinline__ void tc_stage(uint8_t* tile, const float* __restrict__ src, int sr, int sk, int r0, int R,
+                                         int k0, int Ke, int tid) {
+  constexpr int kPer = ROWS * 64 / 128;  // elements per thread
+  float v[kPer];
+  if (sk == 1) {  // k contiguous: a warp reads 64 consecutive floats (two per lane) of one row
+#pragma unroll
+    for (int e = 0; e < kPer / 2; ++e) {
+      const int i = tid + 128 * e, r = i >> 5, k = 2 * (i & 31);
       const bool rin = r0 + r < R;
-      const float a = rin && k0 + k < Ke ? src[(size_t)(r0 + r) * sr + (k0 + k)] : 0.f;
-      const float b = rin && k0 + k + 1 < Ke ? src[(size_t)(r0 + r) * sr + (k0 + k + 1)] : 0.f;
-      *reinterpret_cast<uint32_t*>(tile + umma::sw128_offset(r, k, rows)) = bf16x2_bits(a, b);
+      const float* q = src + (size_t)(r0 + r) * sr + (k0 + k);
+      v[2 * e] = rin && k0 + k < Ke ? __ldg(q) : 0.f;
+      v[2 * e + 1] = rin && k0 + k + 1 < Ke ? __ldg(q + 1) : 0.f;
+    }
+#pragma unroll
+    for (int e = 0; e < kPer / 2; ++e) {
+      const int i = tid + 128 * e, r = i >> 5, k = 2 * (i & 31);
+      *reinterpret_cast<uint32_t*>(tile + umma::sw128_offset(r, k, ROWS)) = bf16x2_bits(v[2 * e], v[2 * e + 1]);
     }
   } else {  // rows contiguous (or neither): a warp reads 32 consecutive rows of one k
-    for (int i = tid; i < rows * 64; i += 128) {
-      const int k = i / rows, r = i % rows;
-      const float a = r0 + r < R && k0 + k < Ke ? src[(size_t)(r0 + r) * sr + (size_t)(k0 + k) * sk] : 0.f;
-      *reinterpret_cast<uint16_t*>(tile + umma::sw128_offset(r, k, rows)) = bf16_bits(a);
+#pragma unroll
+    for (int e = 0; e < kPer; ++e) {
+      const int i = tid + 128 * e, k = i / ROWS, r = i % ROWS;
+      v[e] = r0 + r < R && k0 + k < Ke ? __ldg(src + (size_t)(r0 + r) * sr + (size_t)(k0 + k) * sk) : 0.f;
+    }
+#pragma unroll
+    for (int e = 0; e < kPer; ++e) {
+      const int i = tid + 128 * e, k = i / ROWS, r = i % ROWS;
+      *reinterpret_cast<uint16_t*>(tile + umma::sw128_offset(r, k, ROWS)) = bf16_bits(v[e]);
     }
   }
 }
@@ -848,8 +864,8 @@ __global__ void __launch_bounds__(128) tc_gemm_kernel(int M, int N, int K, const
     uint8_t* ta = sm + buf * (kTcA + kTcB);
     uint8_t* tb = ta + kTcA;
     const int k0 = kb + 64 * s;
-    tc_stage(ta, 128, A, sam, sak, m0, M, k0, ke, tid);
-    tc_stage(tb, kTcN, Bm, sbn, sbk, n0, N, k0, ke, tid);
+    tc_stage<128>(ta, A, sam, sak, m0, M, k0, ke, tid);
+    tc_stage<kTcN>(tb, Bm, sbn, sbk, n0, N, k0, ke, tid);
     umma::fence_async_smem();
     umma::fence_before_sync();
     __syncthreads();
@@ -869,31 +885,38 @@ __global__ void __launch_bounds__(128) tc_gemm_kernel(int M, int N, int K, const
   ok = __syncthreads_and(ok);
   umma::fence_after_sync();
   if (ok) {
-    const int row = m0 + 32 * warp + lane;
+    // Each thread reads its row's 32 columns of a chunk from tensor memory; the
+    // warp's 32 x 32 block goes through shared memory (the staging tiles are
+    // free now) so that each store instruction writes one row's 32 columns.
+    float* blk = reinterpret_cast<float*>(sm) + warp * (32 * 33);
 #pragma unroll 1
     for (int c0 = 0; c0 < kTcN; c0 += 32) {
       float v[32];
       umma::tmem_ld32(tmem + ((uint32_t)(32 * warp) << 16) + (uint32_t)c0, v);
-      if (row < M) {
 #pragma unroll
-        for (int j = 0; j < 32; ++j) {
-          const int nn = n0 + c0 + j;
-          if (nn >= N) continue;
-          const size_t o = (size_t)row * ldc + nn;
-          if (EPI == 0) {
-            if (gridDim.z > 1)
-              atomicAdd(C + o, v[j]);
-            else
-              C[o] = v[j];
-          } else if (EPI == 1) {
-            const float z = v[j] + bias[nn];
-            aux[o] = z;
-            C[o] = fmaxf(z, 0.f);
-          } else {
-            C[o] = aux[o] > 0.f ? v[j] : 0.f;
-          }
+      for (int j = 0; j < 32; ++j) blk[lane * 33 + j] = v[j];
+      __syncwarp();
+      const int nn = n0 + c0 + lane;
+#pragma unroll 4
+      for (int rr = 0; rr < 32; ++rr) {
+        const int row = m0 + 32 * warp + rr;
+        if (row >= M || nn >= N) continue;
+        const float x = blk[rr * 33 + lane];
+        const size_t o = (size_t)row * ldc + nn;
+        if (EPI == 0) {
+          if (gridDim.z > 1)
+            atomicAdd(C + o, x);
+          else
+            C[o] = x;
+        } else if (EPI == 1) {
+          const float z = x + bias[nn];
+          aux[o] = z;
+          C[o] = fmaxf(z, 0.f);
+        } else {
+          C[o] = aux[o] > 0.f ? x : 0.f;
         }
       }
+      __syncwarp();
     }
   } else if (tid == 0 && error_word) {
     atomicOr(error_word, kErrTimeout);
