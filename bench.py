@@ -306,9 +306,9 @@ def secondary_measurements(dev, p, q):
     mixed = tempering.TemperingChains.mixed(groups, tempering.geometric_ladder(0.05, 5.0, 32), seed=2)
     tune = autotune.autotune(mixed, probe_sweeps=20)
     mixed.run(max(tune.ladder_sweeps), exchange_every=10, chains_per_block=tune.chains_per_block,
-              ladder_sweeps=tune.ladder_sweeps)
+              ladder_sweeps=tune.ladder_sweeps, threads_per_chain=tune.threads_per_chain)
     res = mixed.run(max(tune.ladder_sweeps), exchange_every=10, chains_per_block=tune.chains_per_block,
-                    ladder_sweeps=tune.ladder_sweeps)
+                    ladder_sweeps=tune.ladder_sweeps, threads_per_chain=tune.threads_per_chain)
     mixed.validate()
     per = {}
     for n in sorted(tune.size_sweeps):
@@ -317,10 +317,25 @@ def secondary_measurements(dev, p, q):
     out["mixed_sizes_one_launch"] = {"autotuned": {"threads_per_chain": tune.threads_per_chain,
                                                    "chains_per_block": tune.chains_per_block,
                                                    "sweeps_per_launch": {str(k): v for k, v in tune.size_sweeps.items()},
-                                                   "cpb_candidates_deltas_per_s": {str(k): v for k, v in
-                                                                                   tune.candidates.items()}},
+                                                   "shape_candidates_deltas_per_s": dict(tune.candidates)},
                                      "seconds": res.seconds, "deltas_per_s_per_size": per,
                                      "deltas_per_s_total": res.proposals / res.seconds}
+    launches += 2
+    # the reference CLI's default run shape (tempering.py:233-236): 128 replicas in
+    # ladders of 16 temperatures 0.2..4, every (threads per chain, cpb) timed
+    pr, qr = state.seeded_population(N, 128)
+    small = tempering.TemperingChains(state.pq_to_columns(pr, qr),
+                                      np.tile(tempering.geometric_ladder(0.2, 4.0, 16), 8), seed=3, ladder_size=16)
+    tune_s = autotune.autotune(small, probe_sweeps=20)
+    small.run(20, exchange_every=10, chains_per_block=tune_s.chains_per_block,
+              threads_per_chain=tune_s.threads_per_chain)
+    res = small.run(100, exchange_every=10, chains_per_block=tune_s.chains_per_block,
+                    threads_per_chain=tune_s.threads_per_chain)
+    small.validate()
+    out["tempering_n75_128_chains"] = {"autotuned": {"threads_per_chain": tune_s.threads_per_chain,
+                                                     "chains_per_block": tune_s.chains_per_block,
+                                                     "shape_candidates_deltas_per_s": dict(tune_s.candidates)},
+                                       "seconds": res.seconds, "deltas_per_s": res.proposals / res.seconds}
     launches += 2
     # C5: learned proposals, 2048 chains at n=75, 128 candidates per chain per step
     lp = learned.LearnedProposal(ch, seed=1, batch=4096)

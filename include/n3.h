@@ -185,11 +185,14 @@ typedef struct n3_temper_config {
   int exchange;                 /* 1: neighbour exchange after every round */
   int target_energy;            /* >= 0: record the first chain reaching E <= target (and raise *stop) */
   int bad_bias;                 /* percent of proposals whose slot u is drawn by badness (tempering.py:51-55) */
+  int threads_per_chain;        /* 32 (or 0), 64, 128 or 256: warps that evaluate one chain's moves together;
+                                   chains_per_block x threads_per_chain / 32 <= 16 warps per CTA */
 } n3_temper_config;
 
 /* Runs cfg->rounds rounds (proposals, then an exchange) on every ladder in one
- * persistent launch: grid C/cpb CTAs of cpb warps, clusters of L/cpb CTAs
- * when a ladder spans several CTAs.  Capturable in a CUDA graph (fixed
+ * persistent launch: grid C/cpb CTAs of cpb x threads_per_chain threads,
+ * clusters of L/cpb CTAs when a ladder spans several CTAs.  Results do not
+ * depend on cpb or threads_per_chain (the same proposals, dE and acceptances).  Capturable in a CUDA graph (fixed
  * arguments; the per-device tables must have been set up by an earlier call).
  *
  * A proposal is the reference walk's (tempering.py:49-58): slot u uniform, or,

@@ -37,65 +37,133 @@ __device__ __forceinline__ bool umbrella_accept(int dE, int64_t umb_q, uint32_t 
 
 // FORCE: the move is applied whatever its dE (no Metropolis test).
 // UMB: the test adds the umbrella term umb_q (umbrella_accept).
+// The threads that evaluate one chain's moves: WPC warps, 32 WPC threads.
+// Thread t of the team owns slots t, t + 32 WPC, ... (kSlots of them).  With
+// WPC = 1 the team is a warp (__syncwarp, warp reductions); with WPC > 1 the
+// team meets at the named barrier `bar` (ids 1..15; id 0 is __syncthreads)
+// and reduces through `red`, 2 WPC ints of shared memory used alternately, so
+// a reduction's buffer is rewritten only after every thread has passed the
+// next reduction's barrier.  Every decision a team takes (legality, dE,
+// acceptance) is computed from team-wide values, so all its threads follow
+// the same path through barriers and reductions.
+template <int WPC>
+struct Team {
+  static constexpr int kThreads = 32 * WPC;
+  static constexpr int kSlots = (kMaxM + kThreads - 1) / kThreads;  // 5, 3, 2, 1
+  int t;         // rank in the team
+  int bar;       // named barrier id (WPC > 1)
+  int* red;      // reduction scratch (WPC > 1)
+  int phase;     // which half of red the next reduction uses
+  __device__ __forceinline__ void sync() const {
+    if constexpr (WPC == 1) {
+      __syncwarp();
+    } else {
+      // non-.aligned form: correct even where a warp has not reconverged
+      asm volatile("barrier.sync %0, %1;" ::"r"(bar), "n"(kThreads) : "memory");
+    }
+  }
+  __device__ __forceinline__ int sum(int v) {
+    const int w = warp_sum(v);
+    if constexpr (WPC == 1) {
+      return w;
+    } else {
+      int* buf = red + phase * WPC;
+      phase ^= 1;
+      if ((t & 31) == 0) buf[t >> 5] = w;
+      sync();
+      int s = 0;
+#pragma unroll
+      for (int i = 0; i < WPC; ++i) s += buf[i];
+      return s;
+    }
+  }
+};
+
+// hist_build_full for a team: slot k = t + 32 WPC j, j < kSlots.
+template <int WPC>
+__device__ __forceinline__ int team_hist_build(const Team<WPC>& tm, const int* __restrict__ cs, int m, int rx, int cx,
+                                               int skip0, int skip1, const uint16_t* __restrict__ lutf,
+                                               uint32_t* __restrict__ hist, int (&ids)[Team<WPC>::kSlots]) {
+  const uint16_t* base = lutf + kFullLutCentre - (rx * kLutW + cx);
+  int pairs = 0;
+#pragma unroll
+  for (int j = 0; j < Team<WPC>::kSlots; ++j) {
+    const int k = tm.t + Team<WPC>::kThreads * j;
+    ids[j] = -1;
+    if (k < m && k != skip0 && k != skip1 && (k >> 1) != rx) {
+      const int id = base[(k >> 1) * kLutW + cs[k]];
+      ids[j] = id;
+      pairs += hist_add(hist, id);
+    }
+  }
+  return pairs;
+}
+
+template <int WPC>
+__device__ __forceinline__ void team_hist_release(uint32_t* hist, const int (&ids)[Team<WPC>::kSlots]) {
+#pragma unroll
+  for (int j = 0; j < Team<WPC>::kSlots; ++j)
+    if (ids[j] >= 0) hist_clear(hist, ids[j]);
+}
+
 // EARLY (plain Metropolis only): after the first new-side histogram,
 //   dE >= d1 = t(u') + j(u', v') - (bad[u] + bad[v] - joint)
 // because t(v') >= 0, and thr is non-increasing, so a proposal with d1 >= 1 and
 // (d1 >= W or z >= thr[d1]) is rejected exactly as the full test would reject
 // it, without the second histogram; *dE_out then holds d1.
-template <bool FORCE, bool UMB = false, bool EARLY = false>
-__device__ __forceinline__ int move_exact_t(int* __restrict__ cs, int* __restrict__ bs, int m,
-                                            const uint16_t* __restrict__ lutf, uint32_t* __restrict__ hist, int lane,
-                                            int u, int v, uint32_t z, const uint32_t* __restrict__ thr, int W, int& E,
-                                            uint32_t& err, int* dE_out, int64_t umb_q = 0,
-                                            const uint32_t* __restrict__ frac = nullptr) {
+template <int WPC, bool FORCE, bool UMB = false, bool EARLY = false>
+__device__ __forceinline__ int team_move(Team<WPC>& tm, int* __restrict__ cs, int* __restrict__ bs, int m,
+                                         const uint16_t* __restrict__ lutf, uint32_t* __restrict__ hist, int u, int v,
+                                         uint32_t z, const uint32_t* __restrict__ thr, int W, int& E, uint32_t& err,
+                                         int* dE_out, int64_t umb_q = 0, const uint32_t* __restrict__ frac = nullptr) {
   static_assert(!(EARLY && (FORCE || UMB)), "the early rejection needs the plain Metropolis test");
+  constexpr int S = Team<WPC>::kSlots, TT = Team<WPC>::kThreads;
   const int ru = u >> 1, rv = v >> 1, cu = cs[u], cv = cs[v];
-  int ids[kSlotsPerLane], cnt_new[kSlotsPerLane];
+  int ids[S], cnt_new[S];
   // centre u' = (r_u, c_v)
-  const int part_a = hist_build_full(cs, m, ru, cv, u, v, lutf, hist, lane, ids);
-  __syncwarp();
+  const int part_a = team_hist_build(tm, cs, m, ru, cv, u, v, lutf, hist, ids);
+  tm.sync();
   const int line_new = dir_id_full(lutf, rv - ru, cu - cv);
   const int j_new = hist_get(hist, line_new);
   // points of A on the old line (u, v)
   int joint = 0;
 #pragma unroll
-  for (int t = 0; t < kSlotsPerLane; ++t) {
-    const int k = lane + 32 * t;
+  for (int j = 0; j < S; ++j) {
+    const int k = tm.t + TT * j;
     if (k < m && k != u && k != v) joint += (rv - ru) * (cs[k] - cu) == (cv - cu) * ((k >> 1) - ru);
   }
   int t_a, sum_joint;
   if constexpr (EARLY) {
-    const int s1 = warp_sum(part_a + (joint << 16));
+    const int s1 = tm.sum(part_a + (joint << 16));
     t_a = s1 & 0xFFFF;
     sum_joint = s1 >> 16;
     const int d1 = t_a + j_new - (bs[u] + bs[v] - sum_joint);
     if (d1 >= 1 && (d1 >= W || z >= thr[d1])) {
-      __syncwarp();
-      hist_release(hist, ids);
-      __syncwarp();
+      tm.sync();
+      team_hist_release<WPC>(hist, ids);
+      tm.sync();
       *dE_out = d1;
       return 0;
     }
   }
 #pragma unroll
-  for (int t = 0; t < kSlotsPerLane; ++t)
-    cnt_new[t] = ids[t] >= 0 ? hist_get(hist, ids[t]) - 1 + (ids[t] == line_new) : 0;
-  __syncwarp();
-  hist_release(hist, ids);
-  __syncwarp();
+  for (int j = 0; j < S; ++j) cnt_new[j] = ids[j] >= 0 ? hist_get(hist, ids[j]) - 1 + (ids[j] == line_new) : 0;
+  tm.sync();
+  team_hist_release<WPC>(hist, ids);
+  tm.sync();
   // centre v' = (r_v, c_u)
-  const int part_b = hist_build_full(cs, m, rv, cu, u, v, lutf, hist, lane, ids);
-  __syncwarp();
+  const int part_b = team_hist_build(tm, cs, m, rv, cu, u, v, lutf, hist, ids);
+  tm.sync();
 #pragma unroll
-  for (int t = 0; t < kSlotsPerLane; ++t) cnt_new[t] += ids[t] >= 0 ? hist_get(hist, ids[t]) - 1 : 0;
-  __syncwarp();
-  hist_release(hist, ids);
+  for (int j = 0; j < S; ++j) cnt_new[j] += ids[j] >= 0 ? hist_get(hist, ids[j]) - 1 : 0;
+  tm.sync();
+  team_hist_release<WPC>(hist, ids);
   int t_b;
   if constexpr (EARLY) {
-    t_b = warp_sum(part_b);
+    t_b = tm.sum(part_b);
   } else {
-    const int sum_ab = warp_sum(part_a + (part_b << 16));
-    sum_joint = warp_sum(joint);
+    const int sum_ab = tm.sum(part_a + (part_b << 16));
+    sum_joint = tm.sum(joint);
     t_a = sum_ab & 0xFFFF;
     t_b = sum_ab >> 16;
   }
@@ -104,46 +172,57 @@ __device__ __forceinline__ int move_exact_t(int* __restrict__ cs, int* __restric
   const bool accept = FORCE || (UMB ? umbrella_accept(dE, umb_q, z, thr, W, frac)
                                      : (dE <= 0 || (dE < W && z < thr[dE])));
   if (!accept) {
-    __syncwarp();
+    tm.sync();
     return 0;
   }
   // Old-side histograms: exact badness change of every other point.
-  __syncwarp();
-  int dB[kSlotsPerLane];
-  const int part_c = hist_build_full(cs, m, ru, cu, u, v, lutf, hist, lane, ids);
-  __syncwarp();
+  tm.sync();
+  int dB[S];
+  const int part_c = team_hist_build(tm, cs, m, ru, cu, u, v, lutf, hist, ids);
+  tm.sync();
   const int line_old = dir_id_full(lutf, rv - ru, cv - cu);
   const int j_old = hist_get(hist, line_old);
 #pragma unroll
-  for (int t = 0; t < kSlotsPerLane; ++t)
-    dB[t] = cnt_new[t] - (ids[t] >= 0 ? hist_get(hist, ids[t]) - 1 + (ids[t] == line_old) : 0);
-  __syncwarp();
-  hist_release(hist, ids);
-  __syncwarp();
-  const int part_d = hist_build_full(cs, m, rv, cv, u, v, lutf, hist, lane, ids);
-  __syncwarp();
+  for (int j = 0; j < S; ++j)
+    dB[j] = cnt_new[j] - (ids[j] >= 0 ? hist_get(hist, ids[j]) - 1 + (ids[j] == line_old) : 0);
+  tm.sync();
+  team_hist_release<WPC>(hist, ids);
+  tm.sync();
+  const int part_d = team_hist_build(tm, cs, m, rv, cv, u, v, lutf, hist, ids);
+  tm.sync();
 #pragma unroll
-  for (int t = 0; t < kSlotsPerLane; ++t) dB[t] -= ids[t] >= 0 ? hist_get(hist, ids[t]) - 1 : 0;
-  __syncwarp();
-  hist_release(hist, ids);
-  const int sum_cd = warp_sum(part_c + (part_d << 16));
+  for (int j = 0; j < S; ++j) dB[j] -= ids[j] >= 0 ? hist_get(hist, ids[j]) - 1 : 0;
+  tm.sync();
+  team_hist_release<WPC>(hist, ids);
+  const int sum_cd = tm.sum(part_c + (part_d << 16));
   const int t_c = sum_cd & 0xFFFF, t_d = sum_cd >> 16;
   if (bs[u] != t_c + j_old || bs[v] != t_d + j_old || j_old != sum_joint) err |= kErrAudit;
-  __syncwarp();
+  tm.sync();
 #pragma unroll
-  for (int t = 0; t < kSlotsPerLane; ++t) {
-    const int k = lane + 32 * t;
-    if (k < m && k != u && k != v) bs[k] += dB[t];
+  for (int j = 0; j < S; ++j) {
+    const int k = tm.t + TT * j;
+    if (k < m && k != u && k != v) bs[k] += dB[j];
   }
-  if (lane == 0) {
+  if (tm.t == 0) {
     bs[u] = t_a + j_new;
     bs[v] = t_b + j_new;
     cs[u] = cv;
     cs[v] = cu;
   }
-  __syncwarp();
+  tm.sync();
   E += dE;
   return 1;
+}
+
+// The move evaluated by one warp (lane = its lane index).
+template <bool FORCE, bool UMB = false, bool EARLY = false>
+__device__ __forceinline__ int move_exact_t(int* __restrict__ cs, int* __restrict__ bs, int m,
+                                            const uint16_t* __restrict__ lutf, uint32_t* __restrict__ hist, int lane,
+                                            int u, int v, uint32_t z, const uint32_t* __restrict__ thr, int W, int& E,
+                                            uint32_t& err, int* dE_out, int64_t umb_q = 0,
+                                            const uint32_t* __restrict__ frac = nullptr) {
+  Team<1> tm{lane, 0, nullptr, 0};
+  return team_move<1, FORCE, UMB, EARLY>(tm, cs, bs, m, lutf, hist, u, v, z, thr, W, E, err, dE_out, umb_q, frac);
 }
 
 __device__ __forceinline__ int move_exact(int* __restrict__ cs, int* __restrict__ bs, int m,
@@ -209,25 +288,26 @@ struct WalkParams {
 // w the bias coin.  With UMB the acceptance energy carries the umbrella
 // restraint s((off + dd)^2 - off^2), off = removed - center (tempering.py:93-94),
 // and an accepted move adds dd to `removed`.  Returns 1 if accepted.
-template <bool BIAS, bool UMB>
-__device__ __forceinline__ int propose_walk(int* __restrict__ cs, int* __restrict__ bs, int m,
-                                            const uint16_t* __restrict__ lutf, uint32_t* __restrict__ hist, int lane,
-                                            U4 rnd, uint64_t ctr, int chain, const uint32_t* __restrict__ thr, int W,
-                                            int& E, uint32_t& err, const WalkParams& P, int& removed) {
+template <int WPC, bool BIAS, bool UMB>
+__device__ __forceinline__ int propose_walk(Team<WPC>& tm, int* __restrict__ cs, int* __restrict__ bs, int m,
+                                            const uint16_t* __restrict__ lutf, uint32_t* __restrict__ hist, U4 rnd,
+                                            uint64_t ctr, int chain, const uint32_t* __restrict__ thr, int W, int& E,
+                                            uint32_t& err, const WalkParams& P, int& removed) {
   if (E <= 0) return 0;
   int u = (int)__umulhi(rnd.x, (unsigned)m);
   const int v = (int)__umulhi(rnd.y, (unsigned)m);
   if (BIAS && __umulhi(rnd.w, 100u) < (unsigned)P.bad_bias) {
+    // every warp of the team draws the same slot from the same badness
     const U4 r2 = philox4x32_10(U4{(uint32_t)ctr, (uint32_t)(ctr >> 32), (uint32_t)chain, kTagBias}, P.k0, P.k1);
-    u = bias_pick(bs, m, __umulhi(r2.x, 3u * (unsigned)E), lane);
+    u = bias_pick(bs, m, __umulhi(r2.x, 3u * (unsigned)E), tm.t & 31);
   }
   if (!legal_swap(cs, u, v)) return 0;
   int dE;
-  if (!UMB) return move_exact_t<false, false, true>(cs, bs, m, lutf, hist, lane, u, v, rnd.z, thr, W, E, err, &dE);
+  if (!UMB) return team_move<WPC, false, false, true>(tm, cs, bs, m, lutf, hist, u, v, rnd.z, thr, W, E, err, &dE);
   const int dd = umbrella_distance_delta(P.ref, u, v, cs[u], cs[v]);
   const int64_t umb = P.s_q * (int64_t)(2 * removed * dd + dd * dd) - P.c2s_q * (int64_t)dd;
-  const int acc = move_exact_t<false, true>(cs, bs, m, lutf, hist, lane, u, v, rnd.z, thr, W, E, err, &dE, umb,
-                                            P.frac);
+  const int acc = team_move<WPC, false, true>(tm, cs, bs, m, lutf, hist, u, v, rnd.z, thr, W, E, err, &dE, umb,
+                                              P.frac);
   if (acc) removed += dd;
   return acc;
 }

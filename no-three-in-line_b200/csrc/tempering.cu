@@ -4,7 +4,9 @@
 // Reference: the per-replica walk kernel and host-side exchange of
 // src/no_three_75/tempering.py:29-191.  Layout and scheduling here:
 //
-// * One warp per chain.  A CTA holds `cpb` chains.  A ladder of L
+// * One team of WPC warps per chain (WPC = threads_per_chain / 32: 1, 2, 4, 8;
+//   the team shares the chain's histogram and splits its slots).  A CTA
+//   holds `cpb` chains (cpb * WPC <= 16 warps).  A ladder of L
 //   temperatures lives either inside one CTA (cpb a multiple of L) or across a
 //   thread-block cluster of L / cpb CTAs; its exchange step uses the CTA
 //   barrier or the cluster barrier and distributed shared memory, never a
@@ -52,12 +54,14 @@ __device__ __forceinline__ uint64_t global_ns() {
 }
 
 // Shared-memory layout of the tempering kernel (dynamic): the full direction
-// table, then per chain a histogram, columns and badness, then the leader arrays.
+// table, then per chain a histogram, columns and badness, then the leader
+// arrays, then the teams' reduction scratch (2 WPC ints per chain).
+constexpr int kTeamScratch = 2 * 16;
 struct TemperSmem {
   static constexpr size_t lut_bytes = kFullLutBytes;
   static __host__ __device__ size_t bytes(int cpb) {
     return lut_bytes + (size_t)cpb * (sizeof(uint32_t) * kDirWords + 2 * sizeof(int) * kMaxM) +
-           3 * sizeof(int) * 64 + 16;
+           3 * sizeof(int) * 64 + 16 + sizeof(int) * kTeamScratch;
   }
 };
 
@@ -86,8 +90,9 @@ __device__ void exchange_ladder(int* tmp_chain, int* tmp_temp, const int* e, int
   }
 }
 
-template <bool BIAS, bool UMB>
+template <int WPC, bool BIAS, bool UMB>
 __global__ void __launch_bounds__(512, 1) temper_kernel(const TemperArgs A) {
+  constexpr int TT = Team<WPC>::kThreads;
   extern __shared__ __align__(16) unsigned char smem[];
   const n3_chains& ch = A.ch;
   const n3_temper_config& cfg = A.cfg;
@@ -100,6 +105,7 @@ __global__ void __launch_bounds__(512, 1) temper_kernel(const TemperArgs A) {
   int* ld_temp = ld_e + 64;
   int* ld_chain = ld_temp + 64;
   int* ld_stop = ld_chain + 64;
+  int* team_red = ld_stop + 4;  // 16-byte aligned: ld_stop's block holds 4 ints
 
   cg::cluster_group cluster = cg::this_cluster();
   const int rank = CS > 1 ? (int)cluster.block_rank() : 0;
@@ -114,7 +120,8 @@ __global__ void __launch_bounds__(512, 1) temper_kernel(const TemperArgs A) {
   int* L_temp = CS > 1 ? cluster.map_shared_rank(ld_temp, 0) : ld_temp;
   int* L_stop = CS > 1 ? cluster.map_shared_rank(ld_stop, 0) : ld_stop;
 
-  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int warp = threadIdx.x / TT;  // this chain's index in the CTA
+  Team<WPC> tm{(int)threadIdx.x % TT, 1 + warp, team_red + 2 * WPC * warp, 0};
   const int c = blockIdx.x * cpb + warp;
   const int lad = c / L;
   const int li = c % L;
@@ -127,7 +134,7 @@ __global__ void __launch_bounds__(512, 1) temper_kernel(const TemperArgs A) {
 
   full_lut_copy(lut, A.lut);
   for (int i = threadIdx.x; i < cpb * kDirWords; i += blockDim.x) hist_all[i] = 0u;
-  for (int s = lane; s < m; s += 32) {
+  for (int s = tm.t; s < m; s += TT) {
     cs[s] = ch.cols[(size_t)c * kMaxM + s];
     bs[s] = ch.badness[(size_t)c * kMaxM + s];
   }
@@ -151,7 +158,7 @@ __global__ void __launch_bounds__(512, 1) temper_kernel(const TemperArgs A) {
     if (threadIdx.x == 0) *ld_stop = 0;
   }
   uint32_t lround = 0, lexch = 0;  // leader-thread copies (one leader per ladder)
-  const bool ladder_leader = leader_cta && lane == 0 && (CS > 1 ? warp == 0 : (warp % L) == 0);
+  const bool ladder_leader = leader_cta && tm.t == 0 && (CS > 1 ? warp == 0 : (warp % L) == 0);
   if (ladder_leader) {
     lround = ch.ladder_round[lad];
     lexch = ch.ladder_exchanges[lad];
@@ -182,18 +189,18 @@ __global__ void __launch_bounds__(512, 1) temper_kernel(const TemperArgs A) {
     for (int p = 0; p < per_round; ++p) {
       const U4 rnd = philox4x32_10(U4{(uint32_t)counter, (uint32_t)(counter >> 32), (uint32_t)c, kTagPropose},
                                    k0, k1);
-      const int acc = propose_walk<BIAS, UMB>(cs, bs, m, lut, hist, lane, rnd, counter, c, thr, W, E, err, wp,
-                                              removed);
+      const int acc = propose_walk<WPC, BIAS, UMB>(tm, cs, bs, m, lut, hist, rnd, counter, c, thr, W, E, err, wp,
+                                                   removed);
       ++counter;
       if (acc) {
         ++accepted;
         if (E < bestE) {
           bestE = E;
-          for (int s = lane; s < m; s += 32) ch.best_cols[(size_t)c * kMaxM + s] = (int16_t)cs[s];
+          for (int s = tm.t; s < m; s += TT) ch.best_cols[(size_t)c * kMaxM + s] = (int16_t)cs[s];
         }
         if (cfg.target_energy >= 0 && E <= cfg.target_energy && !hit_done) {
           hit_done = true;
-          if (lane == 0 && ch.hit != nullptr && atomicCAS(ch.hit, -1, c) == -1) {
+          if (tm.t == 0 && ch.hit != nullptr && atomicCAS(ch.hit, -1, c) == -1) {
             const uint64_t now = global_ns();
             ch.hit[1] = (int32_t)(uint32_t)counter;
             ch.hit[2] = (int32_t)(uint32_t)now;
@@ -204,7 +211,7 @@ __global__ void __launch_bounds__(512, 1) temper_kernel(const TemperArgs A) {
       }
     }
     if (!cfg.exchange) continue;
-    if (lane == 0) L_e[lidx] = E;
+    if (tm.t == 0) L_e[lidx] = E;
     barrier();
     if (ladder_leader) {
       exchange_ladder(ld_chain + lbase, ld_temp + lbase, ld_e + lbase, L, lad, lround, ch.exch_thresh,
@@ -217,17 +224,17 @@ __global__ void __launch_bounds__(512, 1) temper_kernel(const TemperArgs A) {
   }
 
   // write back
-  for (int s = lane; s < m; s += 32) {
+  for (int s = tm.t; s < m; s += TT) {
     ch.cols[(size_t)c * kMaxM + s] = (int16_t)cs[s];
     ch.badness[(size_t)c * kMaxM + s] = bs[s];
   }
-  if (lane == 0) {
+  if (err && ch.error_word) atomicOr(ch.error_word, err);
+  if (tm.t == 0) {
     ch.energy[c] = E;
     ch.best_energy[c] = bestE;
     ch.counter[c] = counter;
     ch.accepted[c] = accepted;
     if (UMB) ch.removed[c] = removed;
-    if (err && ch.error_word) atomicOr(ch.error_word, err);
     if (ch.global_best) atomicMin(ch.global_best, bestE);
   }
   if (ladder_leader) {
@@ -300,11 +307,33 @@ static int check_chains(const n3_chains* ch) {
   return N3_OK;
 }
 
+using TemperKernel = void (*)(const n3::TemperArgs);
+
+template <int WPC>
+static TemperKernel temper_instance_w(bool bias, bool umb) {
+  return umb ? (bias ? n3::temper_kernel<WPC, true, true> : n3::temper_kernel<WPC, false, true>)
+             : (bias ? n3::temper_kernel<WPC, true, false> : n3::temper_kernel<WPC, false, false>);
+}
+
+static TemperKernel temper_instance(int wpc, bool bias, bool umb) {
+  switch (wpc) {
+    case 8: return temper_instance_w<8>(bias, umb);
+    case 4: return temper_instance_w<4>(bias, umb);
+    case 2: return temper_instance_w<2>(bias, umb);
+    default: return temper_instance_w<1>(bias, umb);
+  }
+}
+
 int temper_launch(const n3_chains* ch, const n3_temper_config* cfg, cudaStream_t st) {
   N3_TRY(check_chains(ch));
   if (cfg == nullptr) return set_error(N3_ERR_ARG, "null config");
   const int L = ch->ladder_size, cpb = cfg->chains_per_block;
-  if (cpb < 1 || cpb > 16) return set_error(N3_ERR_ARG, "chains_per_block %d outside [1, 16]", cpb);
+  const int tpc = cfg->threads_per_chain == 0 ? 32 : cfg->threads_per_chain;
+  if (tpc != 32 && tpc != 64 && tpc != 128 && tpc != 256)
+    return set_error(N3_ERR_ARG, "threads_per_chain %d is not 32, 64, 128 or 256", cfg->threads_per_chain);
+  const int wpc = tpc / 32;
+  if (cpb < 1 || cpb * wpc > 16)
+    return set_error(N3_ERR_ARG, "chains_per_block %d x %d warps per chain outside [1, 16] warps", cpb, wpc);
   int cluster = 1;
   if (cpb < L) {
     if (L % cpb) return set_error(N3_ERR_ARG, "chains_per_block %d does not divide ladder_size %d", cpb, L);
@@ -334,12 +363,11 @@ int temper_launch(const n3_chains* ch, const n3_temper_config* cfg, cudaStream_t
   args.cluster = cluster;
   const size_t smem = n3::TemperSmem::bytes(cpb);
   const bool bias = cfg->bad_bias > 0;
-  void (*kern)(const n3::TemperArgs) = umb ? (bias ? n3::temper_kernel<true, true> : n3::temper_kernel<false, true>)
-                                           : (bias ? n3::temper_kernel<true, false> : n3::temper_kernel<false, false>);
+  void (*kern)(const n3::TemperArgs) = temper_instance(wpc, bias, umb);
   N3_TRY(allow_smem(reinterpret_cast<const void*>(kern), n3::TemperSmem::bytes(16)));
   cudaLaunchConfig_t lc = {};
   lc.gridDim = dim3(ch->n_chains / cpb);
-  lc.blockDim = dim3(cpb * 32);
+  lc.blockDim = dim3(cpb * tpc);
   lc.dynamicSmemBytes = smem;
   lc.stream = st;
   cudaLaunchAttribute attr[1];
@@ -358,10 +386,10 @@ int temper_launch(const n3_chains* ch, const n3_temper_config* cfg, cudaStream_t
 
 namespace n3host {
 int prepare_tempering() {
-  N3_TRY(allow_smem(reinterpret_cast<const void*>(n3::temper_kernel<false, false>), n3::TemperSmem::bytes(16)));
-  N3_TRY(allow_smem(reinterpret_cast<const void*>(n3::temper_kernel<true, false>), n3::TemperSmem::bytes(16)));
-  N3_TRY(allow_smem(reinterpret_cast<const void*>(n3::temper_kernel<false, true>), n3::TemperSmem::bytes(16)));
-  N3_TRY(allow_smem(reinterpret_cast<const void*>(n3::temper_kernel<true, true>), n3::TemperSmem::bytes(16)));
+  for (int wpc : {1, 2, 4, 8})
+    for (int b = 0; b < 2; ++b)
+      for (int u = 0; u < 2; ++u)
+        N3_TRY(allow_smem(reinterpret_cast<const void*>(temper_instance(wpc, b, u)), n3::TemperSmem::bytes(16)));
   return allow_smem(reinterpret_cast<const void*>(n3::audit_kernel), n3::kAuditSmem);
 }
 }  // namespace n3host

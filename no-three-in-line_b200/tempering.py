@@ -51,7 +51,7 @@ class N3TemperConfig(ctypes.Structure):
     _fields_ = [("seed", ctypes.c_uint64), ("chains_per_block", ctypes.c_int), ("rounds", ctypes.c_int),
                 ("ladder_rounds", ctypes.c_void_p), ("round_sweeps", ctypes.c_int),
                 ("round_proposals", ctypes.c_int), ("exchange", ctypes.c_int), ("target_energy", ctypes.c_int),
-                ("bad_bias", ctypes.c_int)]
+                ("bad_bias", ctypes.c_int), ("threads_per_chain", ctypes.c_int)]
 
 
 _lib.register("n3_temper_run", [ctypes.POINTER(N3Chains), ctypes.POINTER(N3TemperConfig), ctypes.c_void_p])
@@ -166,6 +166,9 @@ class TemperingChains:
         self.ladder_n_host = np.asarray(ladder_n, np.int32)
         self.n = int(self.ladder_n_host.max())
         self.seed = int(seed) & 0xFFFFFFFFFFFFFFFF
+        # threads that evaluate one chain's moves (32, 64, 128 or 256); a launch
+        # shape only, chosen by the autotuner
+        self.threads_per_chain = 32
         padded = np.zeros((R, STRIDE), np.int16)
         for lad, n in enumerate(self.ladder_n_host):
             block = cols[lad * L:(lad + 1) * L, :2 * n]
@@ -307,24 +310,31 @@ class TemperingChains:
         if not umbrella:
             self._removed_exact = False
 
-    def default_chains_per_block(self) -> int:
-        """Chains (warps) per CTA: whole ladders per CTA when L <= 16 (as many as
-        fit in 16 warps and divide the ladder count), else the largest divisor
-        of L up to 16 whose cluster (L / cpb CTAs) has at most 8 CTAs."""
+    def default_chains_per_block(self, threads_per_chain: int = 32) -> int:
+        """Chains per CTA for teams of ``threads_per_chain`` threads (at most 16
+        warps per CTA, so cap = 16 / warps per chain): whole ladders per CTA
+        when L <= cap (as many as fit and divide the ladder count), else the
+        largest divisor of L up to cap whose cluster (L / cpb CTAs) has at most
+        8 CTAs."""
+        if threads_per_chain not in (32, 64, 128, 256):
+            raise ValueError("threads_per_chain must be 32, 64, 128 or 256")
+        cap = 16 // (threads_per_chain // 32)
         L, ladders = self.L, self.cols.shape[0] // self.L
-        if L <= 16:
-            k = max(k for k in range(1, 16 // L + 1) if ladders % k == 0)
+        if L <= cap:
+            k = max(k for k in range(1, cap // L + 1) if ladders % k == 0)
             return k * L
-        for d in range(16, 0, -1):
+        for d in range(cap, 0, -1):
             if L % d == 0 and L // d <= 8:
                 return d
-        raise ValueError(f"ladder size {L} cannot be split over at most 8 CTAs of at most 16 chains")
+        raise ValueError(f"ladder size {L} cannot be split over at most 8 CTAs of at most {cap} chains "
+                         f"({threads_per_chain} threads per chain)")
 
     def _config(self, *, rounds, round_sweeps=0, round_proposals=0, exchange=True, chains_per_block=None,
-                target=-1, ladder_rounds=None, bad_bias=0) -> N3TemperConfig:
+                target=-1, ladder_rounds=None, bad_bias=0, threads_per_chain=None) -> N3TemperConfig:
         c = N3TemperConfig()
         c.seed = self.seed
-        c.chains_per_block = chains_per_block or self.default_chains_per_block()
+        c.threads_per_chain = int(threads_per_chain or self.threads_per_chain)
+        c.chains_per_block = chains_per_block or self.default_chains_per_block(c.threads_per_chain)
         c.rounds = rounds
         c.ladder_rounds = None if ladder_rounds is None else ladder_rounds.data_ptr()
         c.round_sweeps = round_sweeps
@@ -387,13 +397,16 @@ class TemperingChains:
     def run(self, sweeps: int, *, exchange_every: int = 10, chains_per_block: int | None = None,
             sweeps_per_launch: int | None = None, target: int | None = None, ladder_sweeps=None,
             max_seconds: float | None = None, graph: bool = True, bad_bias: int = 0,
-            exchange: bool = True) -> RunResult:
+            exchange: bool = True, threads_per_chain: int | None = None) -> RunResult:
         """Native path: ``sweeps`` sweeps (one sweep = 2n proposals per chain)
         with a neighbour exchange every ``exchange_every`` sweeps, all on the
         device.  With ``target`` the run stops at the first exchange boundary
         after some chain reaches E <= target; ``hit`` then reports when.
         ``bad_bias`` as in ``advance``; ``exchange=False`` runs the rounds
-        without exchanges (required while an umbrella is active)."""
+        without exchanges (required while an umbrella is active).
+        ``threads_per_chain`` (32, 64, 128 or 256; default the chain set's
+        ``threads_per_chain``) and ``chains_per_block`` shape the launch only:
+        results are the same for every choice."""
         t = _lib.torch()
         if sweeps % exchange_every:
             raise ValueError("sweeps must be a multiple of exchange_every")
@@ -408,7 +421,8 @@ class TemperingChains:
         launches = -(-sweeps // per_launch)
         rounds_per_launch = per_launch // exchange_every
         ladder_rounds = None
-        cpb = chains_per_block or self.default_chains_per_block()
+        tpc = int(threads_per_chain or self.threads_per_chain)
+        cpb = chains_per_block or self.default_chains_per_block(tpc)
         if ladder_sweeps is not None:
             ls = np.asarray(ladder_sweeps, np.int32)
             if ls.shape != (self.cols.shape[0] // self.L,) or np.any(ls % exchange_every) or np.any(ls < 0):
@@ -420,11 +434,11 @@ class TemperingChains:
         self.stop.zero_()
         self.hit.fill_(-1)
         cfg = self._config(rounds=rounds_per_launch, round_sweeps=exchange_every, exchange=exchange,
-                           chains_per_block=chains_per_block, target=tgt, ladder_rounds=ladder_rounds,
-                           bad_bias=bad_bias)
+                           chains_per_block=cpb, target=tgt, ladder_rounds=ladder_rounds,
+                           bad_bias=bad_bias, threads_per_chain=tpc)
         stream = t.cuda.current_stream()
         if graph:
-            key = (rounds_per_launch, exchange_every, cfg.chains_per_block, tgt,
+            key = (rounds_per_launch, exchange_every, cfg.chains_per_block, tpc, tgt,
                    None if ladder_sweeps is None else tuple(int(x) for x in np.asarray(ladder_sweeps)),
                    int(bad_bias), bool(exchange), umb)
             if key not in self._graphs:
