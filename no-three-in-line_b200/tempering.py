@@ -166,9 +166,11 @@ class TemperingChains:
         self.ladder_n_host = np.asarray(ladder_n, np.int32)
         self.n = int(self.ladder_n_host.max())
         self.seed = int(seed) & 0xFFFFFFFFFFFFFFFF
-        # threads that evaluate one chain's moves (32, 64, 128 or 256); a launch
-        # shape only, chosen by the autotuner
+        # launch shape (threads that evaluate one chain's moves: 32, 64, 128
+        # or 256; chains per CTA, None for the default), e.g. the autotuner's
+        # choice; results do not depend on it
         self.threads_per_chain = 32
+        self.chains_per_block = None
         padded = np.zeros((R, STRIDE), np.int16)
         for lad, n in enumerate(self.ladder_n_host):
             block = cols[lad * L:(lad + 1) * L, :2 * n]
@@ -329,12 +331,19 @@ class TemperingChains:
         raise ValueError(f"ladder size {L} cannot be split over at most 8 CTAs of at most {cap} chains "
                          f"({threads_per_chain} threads per chain)")
 
+    def _shape_cpb(self, threads_per_chain: int) -> int:
+        """The set's chains_per_block when it was chosen for this team width,
+        else the default."""
+        if self.chains_per_block and threads_per_chain == self.threads_per_chain:
+            return int(self.chains_per_block)
+        return self.default_chains_per_block(threads_per_chain)
+
     def _config(self, *, rounds, round_sweeps=0, round_proposals=0, exchange=True, chains_per_block=None,
                 target=-1, ladder_rounds=None, bad_bias=0, threads_per_chain=None) -> N3TemperConfig:
         c = N3TemperConfig()
         c.seed = self.seed
         c.threads_per_chain = int(threads_per_chain or self.threads_per_chain)
-        c.chains_per_block = chains_per_block or self.default_chains_per_block(c.threads_per_chain)
+        c.chains_per_block = chains_per_block or self._shape_cpb(c.threads_per_chain)
         c.rounds = rounds
         c.ladder_rounds = None if ladder_rounds is None else ladder_rounds.data_ptr()
         c.round_sweeps = round_sweeps
@@ -422,7 +431,7 @@ class TemperingChains:
         rounds_per_launch = per_launch // exchange_every
         ladder_rounds = None
         tpc = int(threads_per_chain or self.threads_per_chain)
-        cpb = chains_per_block or self.default_chains_per_block(tpc)
+        cpb = chains_per_block or self._shape_cpb(tpc)
         if ladder_sweeps is not None:
             ls = np.asarray(ladder_sweeps, np.int32)
             if ls.shape != (self.cols.shape[0] // self.L,) or np.any(ls % exchange_every) or np.any(ls < 0):
@@ -730,6 +739,8 @@ def main(argv=None) -> int:
     parser.add_argument("--resume")
     parser.add_argument("--umbrella-max", type=float, default=0)
     parser.add_argument("--umbrella-strength", type=float, default=0.2)
+    parser.add_argument("--threads-per-chain", default="auto", choices=["auto", "32", "64", "128", "256"],
+                        help="launch shape; auto: the autotuner times every shape on copies of the chains")
     args = parser.parse_args(argv)
     output = Path(args.output)
     output.mkdir(parents=True, exist_ok=True)
@@ -755,10 +766,19 @@ def main(argv=None) -> int:
         chains.centers = np.repeat(np.linspace(0, args.umbrella_max, args.replicas // args.ladder_size),
                                    args.ladder_size).astype(np.float32)
         chains.strengths.fill(args.umbrella_strength)
+    if args.threads_per_chain == "auto":
+        from .autotune import autotune
+
+        tune = autotune(chains, probe_sweeps=2, exchange_every=2)
+        chains.threads_per_chain, chains.chains_per_block = tune.threads_per_chain, tune.chains_per_block
+    else:
+        chains.threads_per_chain = int(args.threads_per_chain)
     reference = set((i // 2, int(c)) for i, c in enumerate(rows[0]))
     start = time.perf_counter()
     best, proposals, archive = 10 ** 9, 0, {}
-    (output / "parameters.json").write_text(json.dumps(vars(args), indent=2) + "\n", encoding="utf-8")
+    # the reference's parameters (the launch shape does not change results)
+    params = {k: v for k, v in vars(args).items() if k != "threads_per_chain"}
+    (output / "parameters.json").write_text(json.dumps(params, indent=2) + "\n", encoding="utf-8")
     for epoch in range(1, args.rounds + 1):
         exchanges = chains.epoch(args.steps, args.bad_bias)
         proposals += args.steps * args.replicas
