@@ -424,6 +424,14 @@ int n3_py_random_seed(uint32_t* state, uint64_t seed, void* stream);
  * advancing it exactly as CPython does (_randbelow by getrandbits). */
 int n3_py_random_shuffle(uint32_t* state, int32_t* values, int count, void* stream);
 
+/* The draws of random.shuffle over `count` items from the same state, without
+ * applying them: steps_j[s] = the j that step s (count - 1 down to 1) swaps
+ * with, steps_j[0] = 0; the state advances exactly as the shuffle's does.  The
+ * beam selection resolves its window shuffle this way (one CTA; the draws of a
+ * wide bit width are resolved by the whole CTA at once).  count <= 65536.
+ * Replaces: the draws of rng.shuffle(diverse) (gpu_device_search.py:352). */
+int n3_py_shuffle_steps(uint32_t* state, int count, int32_t* steps_j, void* stream);
+
 #define N3_BEAM_STATUS 8 /* int64 status words, see n3_beam */
 
 typedef struct n3_beam {

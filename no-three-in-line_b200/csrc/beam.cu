@@ -12,13 +12,16 @@
 //   rank_kernel        rank_elites order (gpu_device_search.py:185-197) and the
 //                      best-so-far update by elite_key (:200-203, :388-396)
 // The reference does the selection and ranking on the host with a copy of
-// every child's score each generation.  Here the selection is one CTA: a radix
-// select of the elite_size-th smallest score, a bitonic sort of the scores
-// below it, ordered compactions by per-warp counts, the MT19937 state blocks
-// twisted by the whole CTA, the shuffle's draws by one warp (they must be
-// exactly CPython's: the warp tries 32 steps per round), and the first
-// elite_size shuffled positions traced back through the draws.
+// every child's score each generation.  Here the selection is one CTA: a
+// one-pass histogram (or radix) select of the elite_size-th smallest score, a
+// bitonic sort of the scores below it, ordered compactions by per-warp counts,
+// the MT19937 state blocks twisted by the whole CTA, the shuffle's draws
+// (exactly CPython's: by the whole CTA for the wide draw widths, by one warp
+// for the last ones), and the first elite_size shuffled positions traced back
+// through the draws.
 #include <stdint.h>
+
+#include <climits>
 
 #include "chain_move.cuh"
 #include "dirs.cuh"
@@ -331,40 +334,181 @@ __device__ void mt_twist_cta(const uint32_t* src, uint32_t* dst) {
   __syncthreads();
 }
 
-// The shuffle's draws by one warp, as py_shuffle_warp resolves them, from the
-// tempered outputs out[0, avail) (consecutive blocks of the stream; out holds 32
-// more words, read and ignored), starting at output pos, for steps i, i - 1,
-// ... >= 1: the j of step s goes to jstep[s] and no swap is made.  Stops when
-// the steps end or the outputs do (a round near the end uses the outputs left);
-// i and pos advance.
+// The shuffle's draws by one warp from the tempered outputs out[0, avail)
+// (consecutive blocks of the stream; out holds 32 more words, read and
+// ignored), starting at output pos, for steps i, i - 1, ... >= 1: the j of
+// step s goes to jstep[s] and no swap is made.  A round takes the next 32
+// words: word l serves step i - A_l (A_l: accepted words before it), so with
+// bounds A_lo <= A_l <= A_hi it is accepted for sure when r <= i - A_hi and
+// rejected for sure when r > i - A_lo.  Ballots of the decided words give the
+// bounds (A_lo: accepted below the lane; A_hi: the lane less the rejected
+// below it), and the lowest undecided lane always has exact bounds, so a few
+// iterations decide all 32.  The round keeps the words up to the m-th
+// acceptance (m: the steps left in this draw width, at most 32).  Stops when
+// the steps end or the outputs do; i and pos advance.
 __device__ void shuffle_draws_warp(const uint32_t* out, int avail, int& pos, int& i, uint16_t* jstep, int lane) {
   const unsigned below = (1u << lane) - 1u;
   while (i >= 1 && pos < avail) {
     const int shift = __clz((uint32_t)i + 1u);
-    const int m = min(32, i + 2 - (1 << (31 - shift)));
+    const int lo = max(1, (int)(0x80000000u >> shift) - 1);  // the width's last step
+    const int m = min(32, i - lo + 1);
     const int draws = min(32, avail - pos);
-    const uint32_t r = out[pos + lane] >> shift;
-    const bool acc = lane < draws && (int)r <= i - (m - 1);
-    const bool amb = lane < draws && !acc && (int)r <= i;
-    const unsigned amb_mask = __ballot_sync(0xffffffffu, amb);
-    const int a = amb_mask ? __ffs(amb_mask) - 1 : draws;
-    unsigned acc_mask = __ballot_sync(0xffffffffu, acc) & ((a < 32 ? (1u << a) : 0u) - 1u);
-    int used = a;
-    if (__popc(acc_mask) < m && a < draws) {
-      const int sa = i - __popc(acc_mask);
-      if ((int)__shfl_sync(0xffffffffu, r, a) <= sa) acc_mask |= 1u << a;
-      used = a + 1;
+    const int r = (int)(out[pos + lane] >> shift);
+    unsigned accm = 0u, rejm = draws < 32 ? ~0u << draws : 0u;  // lanes past the outputs: decided, unused
+    for (;;) {
+      const bool und = !(((accm | rejm) >> lane) & 1u);
+      const int a_lo = __popc(accm & below), a_hi = lane - __popc(rejm & below);
+      accm |= __ballot_sync(0xffffffffu, und && r <= i - a_hi);
+      rejm |= __ballot_sync(0xffffffffu, und && r > i - a_lo);
+      if ((accm | rejm) == 0xffffffffu) break;  // uniform
     }
-    if (__popc(acc_mask) >= m) {
-      const int z = __ffs(__ballot_sync(0xffffffffu, ((acc_mask >> lane) & 1u) &&
-                                                      __popc(acc_mask & ((2u << lane) - 1u)) == m)) - 1;
-      acc_mask &= (2u << z) - 1u;
+    int used = draws;
+    if (__popc(accm) >= m) {  // the m-th acceptance ends this width
+      const int z = __ffs(__ballot_sync(0xffffffffu, ((accm >> lane) & 1u) &&
+                                                      __popc(accm & ((2u << lane) - 1u)) == m)) - 1;
       used = z + 1;
     }
-    if ((acc_mask >> lane) & 1u) jstep[i - __popc(acc_mask & below)] = (uint16_t)r;
-    i -= __popc(acc_mask);
+    const unsigned take = used < 32 ? accm & ((1u << used) - 1u) : accm;
+    if ((take >> lane) & 1u) jstep[i - __popc(take & below)] = (uint16_t)r;
+    i -= __popc(take);
     pos += used;
   }
+}
+
+// Exclusive scan over the CTA (thread order) of a 32-bit value, with the total.
+// wsum: 32 words of shared memory; consecutive calls must alternate between
+// two such buffers (a call's buffer is rewritten only after every thread has
+// passed the next call's barriers).  blockDim.x == 1024.
+__device__ __forceinline__ uint32_t cta_exscan32(uint32_t v, uint32_t* wsum, uint32_t& total) {
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  uint32_t x = v;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    const uint32_t y = __shfl_up_sync(0xffffffffu, x, o);
+    if (lane >= o) x += y;
+  }
+  if (lane == 31) wsum[warp] = x;
+  __syncthreads();
+  if (warp == 0) {
+    uint32_t w = wsum[lane];
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const uint32_t y = __shfl_up_sync(0xffffffffu, w, o);
+      if (lane >= o) w += y;
+    }
+    wsum[lane] = w;
+  }
+  __syncthreads();
+  total = wsum[31];
+  return (warp ? wsum[warp - 1] : 0u) + x - v;
+}
+
+// The shuffle's draws for the steps i, i - 1, ... that share i's draw width
+// (down to 2^(k-1) - 1, k = bit_length(i + 1)), resolved by the whole CTA from
+// the tempered outputs out[pos, avail), the same as shuffle_draws_warp: step s
+// takes words in order until one has r = word >> (32 - k) <= s, and j = r.
+// Word w (w = 0, 1, ... from pos) serves step i - A_w, A_w the number of
+// accepted words before it, so it is accepted for sure when r <= i - A_hi and
+// rejected for sure when r > i - A_lo, for any bounds A_lo <= A_w <= A_hi.
+// Each pass bounds A_w by prefix counts over the CTA of the words decided so
+// far (A_lo: accepted before w; A_hi: w less the rejected before w) and
+// decides what the bounds allow; the first undecided word always has exact
+// bounds, so a pass never ends without progress.  Thread t holds words
+// kDrawPer t .. kDrawPer t + kDrawPer - 1.  After at most kDrawPasses passes
+// the call stops at the first undecided word, or after the acceptance of the
+// width's last step, or at the end of the outputs; i and pos advance.  All
+// threads call it with the same i and pos (>= 1 step, >= 1 word left).  A
+// call takes at most 2 need + 64 words (a draw is accepted with probability
+// above 1/2): more words per call mean more passes, as a word's bounds widen
+// with the number of words before it.
+constexpr int kDrawPer = 5;       // 5120 words per call: one batch of kSelBatch blocks
+constexpr int kDrawPasses = 48;
+__device__ void shuffle_draws_cta(const uint32_t* out, int avail, int& pos, int& i, uint16_t* jstep,
+                                  uint32_t* wsum /* [2][32] */, int* cut /* [3] */) {
+  const int tid = threadIdx.x;
+  const int shift = __clz((uint32_t)i + 1u);
+  const int lo = max(1, (int)(0x80000000u >> shift) - 1);  // the width's last step
+  const int need = i - lo + 1;
+  const int nw = min(min(avail - pos, (int)blockDim.x * kDrawPer), 2 * need + 64);
+  const int w0 = tid * kDrawPer;
+  uint32_t r[kDrawPer];
+  uint32_t st = 0u;  // 2 bits per word: 0 undecided, 1 accepted, 2 rejected, 3 absent
+#pragma unroll
+  for (int e = 0; e < kDrawPer; ++e) {
+    const int w = w0 + e;
+    r[e] = w < nw ? out[pos + w] >> shift : 0u;
+    if (w >= nw) st |= 3u << (2 * e);
+  }
+  // scanned counts: accepted | rejected << 16 (at most 5120 each); undecided = words - both
+  uint32_t before = 0u, total = 0u;
+  int la = 0, lu = 0;
+  for (int pass = 0; pass < kDrawPasses; ++pass) {
+    int a = (int)(before & 0xFFFFu), rj = (int)(before >> 16);
+    la = 0;
+    lu = 0;
+    int lr = 0;
+#pragma unroll
+    for (int e = 0; e < kDrawPer; ++e) {
+      uint32_t d = (st >> (2 * e)) & 3u;
+      if (d == 0u) {
+        const int w = w0 + e;
+        if ((int)r[e] <= i - (w - rj)) d = 1u;
+        else if ((int)r[e] > i - a) d = 2u;
+        st |= d << (2 * e);
+      }
+      if (d == 1u) { ++a; ++la; }
+      else if (d == 2u) { ++rj; ++lr; }
+      else if (d == 0u) ++lu;
+    }
+    before = cta_exscan32((uint32_t)la | ((uint32_t)lr << 16), wsum + 32 * (pass & 1), total);
+    if ((int)(total & 0xFFFFu) + (int)(total >> 16) == nw) break;  // uniform: every word decided
+  }
+  // `before` counts exactly for the words before the first undecided one, F.
+  if (tid == 0) {
+    cut[0] = nw;       // F
+    cut[1] = INT_MAX;  // the word after the need-th acceptance
+  }
+  __syncthreads();
+  const int a0 = (int)(before & 0xFFFFu);
+  // no undecided word before this thread's (words before it: min(w0, nw))
+  const bool clean = a0 + (int)(before >> 16) == min(w0, nw);
+  if (clean && lu > 0) {  // this thread holds F
+    int acc = a0;
+    for (int e = 0; e < kDrawPer; ++e) {
+      const uint32_t d = (st >> (2 * e)) & 3u;
+      if (d == 0u) {
+        cut[0] = w0 + e;
+        cut[2] = acc;  // acceptances before F
+        break;
+      }
+      acc += d == 1u;
+    }
+  }
+  if (a0 < need && a0 + la >= need) {  // this thread holds the need-th acceptance (exact if before F)
+    int acc = a0;
+    for (int e = 0; e < kDrawPer; ++e) {
+      if (((st >> (2 * e)) & 3u) == 1u && ++acc == need) {
+        cut[1] = w0 + e + 1;
+        break;
+      }
+    }
+  }
+  __syncthreads();
+  const int F = cut[0], cA = cut[1];
+  const int used = min(F, cA);
+  const int accepted = cA <= F ? need : (F == nw ? (int)(total & 0xFFFFu) : cut[2]);
+  {
+    int acc = a0;
+#pragma unroll
+    for (int e = 0; e < kDrawPer; ++e) {
+      if (((st >> (2 * e)) & 3u) == 1u) {
+        if (w0 + e < used) jstep[i - acc] = (uint16_t)r[e];
+        ++acc;
+      }
+    }
+  }
+  i -= accepted;
+  pos += used;
 }
 
 // --------------------------------------------------------------------------
@@ -374,6 +518,10 @@ constexpr int kSelThreads = 1024;
 constexpr int kMaxPopulation = 65536;
 constexpr int kMaxElite = 2048;
 constexpr int kSelBatch = 8;  // MT state blocks generated per batch for the shuffle's draws
+constexpr int kCtaDrawMin = 2048;  // steps from which the CTA resolves the draws (below: one warp)
+constexpr int kSelHistBins = 4096;  // one-pass selection when every score is below this
+static_assert(kSelBatch * kMT <= kSelThreads * kDrawPer, "one resolver call covers a batch");
+static_assert(kSelHistBins <= kSelBatch * kMT && kSelHistBins % 1024 == 0, "histogram in the MT words' space");
 
 constexpr int kSelWarps = kSelThreads / 32;
 static_assert(kSelWarps == 32, "the per-warp offsets are scanned by one warp, one lane per warp");
@@ -386,15 +534,89 @@ struct SelArgs {
   int32_t* selected;      // [elite_size]
 };
 
-// One group of 32 steps b .. b + 31 (lane l holds j of step b + l, or -1) in
-// the trace back of one shuffled position: the item moves to every step whose
-// j equals its position, in step order.
-__device__ __forceinline__ int trace_group(int js, int b, int pos, int lane) {
-  unsigned hit = __ballot_sync(0xffffffffu, js == pos);
-  while (hit) {  // uniform
-    const int f = __ffs(hit) - 1;
-    pos = b + f;
-    hit = __ballot_sync(0xffffffffu, js == pos) & ~((2u << f) - 1u);
+// The draws of random.shuffle over `count` items (steps s = count - 1 .. 1,
+// j_s = _randbelow(s + 1)) into jstep[s], from the state in shared memory (mt,
+// the current block; idx the position in it, 624 when it is used up), with
+// no swap made.  The CTA twists and tempers the state blocks kSelBatch at a
+// time (words: kSelBatch blocks; out: their outputs and 32 words of padding);
+// the CTA resolves the draws while many steps are left (shuffle_draws_cta) and
+// warp 0 the last ones (shuffle_draws_warp).  On return mt and idx are the
+// state CPython leaves: the block of the last draw and the position after it.
+// Every thread calls it; idx is uniform.
+__device__ void shuffle_steps_cta(uint32_t* mt, int& idx, int count, uint16_t* jstep, uint32_t* words, uint32_t* out,
+                                  uint32_t* wsum, int* cut, int* s_misc) {
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  int steps_left = count - 1;
+  if (steps_left >= 1) {
+    int pos = idx;
+    if (pos < kMT) {
+      for (int k = tid; k < kMT; k += blockDim.x) words[k] = mt[k];
+      __syncthreads();
+    } else {  // the current block is used up: the first draw twists
+      mt_twist_cta(mt, words);
+      pos = 0;
+    }
+    if (tid < 32) out[kSelBatch * kMT + tid] = 0u;  // the padding a last warp round reads
+    for (;;) {
+      for (int g = 1; g < kSelBatch; ++g) mt_twist_cta(words + (g - 1) * kMT, words + g * kMT);
+      for (int k = tid; k < kSelBatch * kMT; k += blockDim.x) out[k] = mt_temper(words[k]);
+      __syncthreads();
+      while (steps_left >= kCtaDrawMin && pos < kSelBatch * kMT)
+        shuffle_draws_cta(out, kSelBatch * kMT, pos, steps_left, jstep, wsum, cut);
+      if (steps_left >= 1 && pos < kSelBatch * kMT) {  // uniform
+        if (warp == 0) {
+          shuffle_draws_warp(out, kSelBatch * kMT, pos, steps_left, jstep, lane);
+          if (lane == 0) {
+            s_misc[0] = steps_left;
+            s_misc[1] = pos;
+          }
+        }
+        __syncthreads();
+        steps_left = s_misc[0];
+        pos = s_misc[1];
+        __syncthreads();
+      }
+      if (steps_left < 1) break;  // uniform
+      mt_twist_cta(words + (kSelBatch - 1) * kMT, words);  // the next batch starts after the last block
+      pos = 0;
+    }
+    const int last = pos - 1;  // >= 0: every round uses at least one word
+    for (int k = tid; k < kMT; k += blockDim.x) mt[k] = words[(last / kMT) * kMT + k];
+    idx = last % kMT + 1;
+  }
+  __syncthreads();
+}
+
+// Shuffled position p traced back through the steps after it: the item moves
+// to step s wherever j_s equals its position (s > its current step).  The warp
+// reads 256 steps at a time (8 packed 16-bit j per lane, compared two at a
+// time); a chunk with a match is re-read after each move, in step order.
+// jstep is 16-byte aligned and holds kMaxPopulation entries.
+__device__ __forceinline__ int trace_position(const uint16_t* jstep, int p, int n_window, int lane) {
+  int pos = p == 0 ? 0 : (int)jstep[p];
+  int cur = p;  // the steps up to cur are behind the item
+  const uint4* j8 = reinterpret_cast<const uint4*>(jstep);
+  for (int b = (p + 1) & ~7; b < n_window; b += 256) {
+    const int s0 = b + 8 * lane;
+    const uint4 v = s0 < kMaxPopulation ? j8[s0 >> 3] : make_uint4(0u, 0u, 0u, 0u);
+    for (;;) {
+      const uint32_t pp = (uint32_t)pos * 0x10001u;
+      const uint32_t e0 = __vcmpeq2(v.x, pp), e1 = __vcmpeq2(v.y, pp), e2 = __vcmpeq2(v.z, pp),
+                     e3 = __vcmpeq2(v.w, pp);
+      // bit h: step s0 + h has j == pos
+      uint32_t hits = (e0 & 1u) | ((e0 >> 15) & 2u) | ((e1 & 1u) << 2) | ((e1 >> 13) & 8u) | ((e2 & 1u) << 4) |
+                      ((e2 >> 11) & 32u) | ((e3 & 1u) << 6) | ((e3 >> 9) & 128u);
+      // only steps after cur and inside the window count
+      const int lo_h = cur + 1 - s0, hi_h = n_window - s0;  // valid h in [lo_h, hi_h)
+      if (lo_h > 0) hits &= lo_h >= 8 ? 0u : ~((1u << lo_h) - 1u);
+      if (hi_h < 8) hits &= hi_h <= 0 ? 0u : (1u << hi_h) - 1u;
+      const unsigned any = __ballot_sync(0xffffffffu, hits != 0u);
+      if (!any) break;  // uniform
+      const int fl = __ffs(any) - 1;
+      const uint32_t hm = __shfl_sync(0xffffffffu, hits, fl);
+      cur = b + 8 * fl + __ffs(hm) - 1;
+      pos = cur;
+    }
   }
   return pos;
 }
@@ -417,6 +639,8 @@ __global__ void __launch_bounds__(kSelThreads, 1) select_kernel(const SelArgs A)
   __shared__ uint32_t hist[256];
   __shared__ int tie_off[kSelWarps], win_off[kSelWarps];
   __shared__ int s_misc[4];
+  __shared__ uint32_t draw_wsum[64];
+  __shared__ int draw_cut[3];
   if (A.status[1] == 0) return;  // uniform: the search has reached E = 0
   const int64_t limit = A.status[1] + (int64_t)A.energy_window;
   for (int i = tid; i < kMaxPopulation / 32; i += kSelThreads) mark[i] = 0u;
@@ -443,6 +667,50 @@ __global__ void __launch_bounds__(kSelThreads, 1) select_kernel(const SelArgs A)
   while (shift > 0 && (top >> shift) == 0u) shift -= 8;  // the skipped high bytes are zero in every score
   uint32_t prefix = 0u, mask = 0u;
   int remaining = E;  // 1-based rank of the E-th element among those matching prefix
+  if (top < (uint32_t)kSelHistBins) {
+    // every score below 4096: one pass, one bin per score value (in the MT words'
+    // space, free until the shuffle), then a scan over the bins
+    uint32_t* h12 = words;
+    for (int i = tid; i < kSelHistBins; i += kSelThreads) h12[i] = 0u;
+    __syncthreads();
+#pragma unroll 4
+    for (int b = s_lo; b < s_hi; b += 32) {
+      const int i = b + lane;
+      const bool valid = i < s_hi;
+      const uint32_t x = valid ? (uint32_t)A.scores[i] : 0u;
+      const unsigned act = __ballot_sync(0xffffffffu, valid);
+      if (valid) {
+        const unsigned peers = __match_any_sync(act, x);
+        if (lane == __ffs(peers) - 1) atomicAdd(&h12[x], (uint32_t)__popc(peers));
+      }
+    }
+    __syncthreads();
+    constexpr int kPerT = kSelHistBins / kSelThreads;
+    uint32_t c[kPerT], local = 0u;
+#pragma unroll
+    for (int k = 0; k < kPerT; ++k) {
+      c[k] = h12[kPerT * tid + k];
+      local += c[k];
+    }
+    uint32_t tot;
+    int run = (int)cta_exscan32(local, draw_wsum, tot);
+    if (run < E && run + (int)local >= E) {  // this thread's bins hold the E-th smallest score
+#pragma unroll
+      for (int k = 0; k < kPerT; ++k) {
+        if (run + (int)c[k] >= E) {
+          s_misc[0] = kPerT * tid + k;
+          s_misc[1] = E - run;
+          break;
+        }
+        run += (int)c[k];
+      }
+    }
+    __syncthreads();
+    prefix = (uint32_t)s_misc[0];
+    remaining = s_misc[1];
+    shift = -8;  // done
+    __syncthreads();
+  }
   for (; shift >= 0; shift -= 8) {
     for (int i = tid; i < 256; i += kSelThreads) hist[i] = 0u;
     __syncthreads();
@@ -552,44 +820,12 @@ __global__ void __launch_bounds__(kSelThreads, 1) select_kernel(const SelArgs A)
   for (int i = tid; i < n_less; i += kSelThreads) order[i] = (int32_t)(uint32_t)keys[i];
 
   // 4. the draws of the window list's shuffle (gpu_device_search.py:340-373):
-  //    the j of every step s in jstep[s], no swap made.  The CTA twists and
-  //    tempers the MT state blocks kSelBatch at a time; warp 0 resolves the
-  //    draws from the tempered words.
-  //    The state left is the block of the last draw, as CPython leaves it.
-  int steps_left = n_window - 1;  // uniform
-  if (steps_left >= 1) {
-    int pos = (int)A.rng[kMT];
-    if (pos < kMT) {
-      for (int k = tid; k < kMT; k += kSelThreads) words[k] = mt[k];
-      __syncthreads();
-    } else {  // the current block is used up: the first draw twists
-      mt_twist_cta(mt, words);
-      pos = 0;
-    }
-    if (tid < 32) tw[kSelBatch * kMT + tid] = 0u;  // the padding a last round reads
-    for (;;) {
-      for (int g = 1; g < kSelBatch; ++g) mt_twist_cta(words + (g - 1) * kMT, words + g * kMT);
-      for (int k = tid; k < kSelBatch * kMT; k += kSelThreads) tw[k] = mt_temper(words[k]);
-      __syncthreads();
-      if (warp == 0) {
-        shuffle_draws_warp(tw, kSelBatch * kMT, pos, steps_left, jstep, lane);
-        if (lane == 0) {
-          s_misc[0] = steps_left;
-          s_misc[1] = pos;
-        }
-      }
-      __syncthreads();
-      steps_left = s_misc[0];
-      pos = s_misc[1];
-      if (steps_left < 1) break;  // uniform
-      mt_twist_cta(words + (kSelBatch - 1) * kMT, words);  // the next batch starts after the last block
-      pos = 0;
-    }
-    const int last = pos - 1;  // >= 0: every round uses at least one draw
-    for (int k = tid; k < kMT; k += kSelThreads) mt[k] = words[(last / kMT) * kMT + k];
-    if (tid == 0) A.rng[kMT] = (uint32_t)(last % kMT + 1);
+  //    the j of every step s in jstep[s], no swap made (shuffle_steps_cta).
+  {
+    int idx = (int)A.rng[kMT];  // uniform
+    shuffle_steps_cta(mt, idx, n_window, jstep, words, tw, draw_wsum, draw_cut, s_misc);
+    if (tid == 0) A.rng[kMT] = (uint32_t)idx;
   }
-  __syncthreads();
 
   // 5. the first K = min(E, window) shuffled positions, one warp each.  Step s
   //    fixes position s for good, so position p holds what sat at j_p before
@@ -600,20 +836,7 @@ __global__ void __launch_bounds__(kSelThreads, 1) select_kernel(const SelArgs A)
   const int K = min(E, n_window);
   int32_t* picked = reinterpret_cast<int32_t*>(keys);  // [K]; keys is free once order is written
   for (int p = warp; p < K; p += kSelWarps) {
-    int pos = p == 0 ? 0 : (int)jstep[p];
-    int b = p + 1;
-    for (; b + 128 <= n_window; b += 128) {  // four groups of 32 steps, loaded together
-      const int j0 = jstep[b + lane], j1 = jstep[b + 32 + lane], j2 = jstep[b + 64 + lane],
-                j3 = jstep[b + 96 + lane];
-      pos = trace_group(j0, b, pos, lane);
-      pos = trace_group(j1, b + 32, pos, lane);
-      pos = trace_group(j2, b + 64, pos, lane);
-      pos = trace_group(j3, b + 96, pos, lane);
-    }
-    for (; b < n_window; b += 32) {
-      const int st = b + lane;
-      pos = trace_group(st < n_window ? (int)jstep[st] : -1, b, pos, lane);
-    }
+    const int pos = trace_position(jstep, p, n_window, lane);
     const unsigned owners = __ballot_sync(0xffffffffu, win_off[lane] <= pos);  // bit 0 always set
     const int w = 31 - __clz(owners);
     int rank = pos - win_off[w];
@@ -660,6 +883,26 @@ __global__ void __launch_bounds__(kSelThreads, 1) select_kernel(const SelArgs A)
   }
   __syncthreads();
   for (int i = tid; i < kMT; i += kSelThreads) A.rng[i] = mt[i];
+}
+
+// The shuffle's draws alone (shuffle_steps_cta), for callers that apply the
+// permutation themselves and for tests: j of step s in jout[s], jout[0] = 0.
+constexpr size_t kStepsSmem = sizeof(uint32_t) * (kMT + 2 * kSelBatch * kMT + 32) + sizeof(uint16_t) * kMaxPopulation;
+__global__ void __launch_bounds__(kSelThreads, 1) py_steps_kernel(uint32_t* state, int count, int32_t* jout) {
+  extern __shared__ __align__(16) unsigned char smem[];
+  uint32_t* mt = reinterpret_cast<uint32_t*>(smem);
+  uint32_t* words = mt + kMT;
+  uint32_t* out = words + kSelBatch * kMT;
+  uint16_t* jstep = reinterpret_cast<uint16_t*>(out + kSelBatch * kMT + 32);
+  __shared__ uint32_t wsum[64];
+  __shared__ int cut[3], s_misc[4];
+  for (int i = threadIdx.x; i < kMT; i += blockDim.x) mt[i] = state[i];
+  __syncthreads();
+  int idx = (int)state[kMT];
+  shuffle_steps_cta(mt, idx, count, jstep, words, out, wsum, cut, s_misc);
+  for (int s = threadIdx.x; s < count; s += blockDim.x) jout[s] = s == 0 ? 0 : (int32_t)jstep[s];
+  for (int i = threadIdx.x; i < kMT; i += blockDim.x) state[i] = mt[i];
+  if (threadIdx.x == 0) state[kMT] = (uint32_t)idx;
 }
 
 constexpr size_t kSelSmem = sizeof(uint64_t) * kMaxElite + sizeof(uint32_t) * kMT + sizeof(int32_t) * kMaxElite +
@@ -889,6 +1132,16 @@ int n3_py_random_shuffle(uint32_t* state, int32_t* values, int count, void* stre
   if (count < 0 || count > n3::beam::kMaxPopulation) return n3host::set_error(N3_ERR_RANGE, "shuffle: bad count");
   n3::beam::py_shuffle_kernel<<<1, 256, 0, (cudaStream_t)stream>>>(state, values, count);
   return n3host::check_launch("py_shuffle_kernel");
+}
+
+int n3_py_shuffle_steps(uint32_t* state, int count, int32_t* steps_j, void* stream) {
+  if (!state || (!steps_j && count > 0)) return n3host::set_error(N3_ERR_ARG, "null shuffle-steps buffer");
+  if (count < 0 || count > n3::beam::kMaxPopulation)
+    return n3host::set_error(N3_ERR_RANGE, "shuffle steps: count %d outside [0, %d]", count, n3::beam::kMaxPopulation);
+  N3_TRY(n3host::allow_smem(reinterpret_cast<const void*>(n3::beam::py_steps_kernel), n3::beam::kStepsSmem));
+  n3::beam::py_steps_kernel<<<1, n3::beam::kSelThreads, n3::beam::kStepsSmem, (cudaStream_t)stream>>>(state, count,
+                                                                                                      steps_j);
+  return n3host::check_launch("py_steps_kernel");
 }
 
 int n3_beam_init(const n3_beam* b, int base_count, void* stream) {

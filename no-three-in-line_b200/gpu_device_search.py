@@ -51,6 +51,7 @@ class BeamDesc(ctypes.Structure):
 _lib.register("n3_beam_mutate", [_P, _P, _P] + [_I] * 7 + [ctypes.c_uint64, _I, _P, _P, _P])
 _lib.register("n3_py_random_seed", [_P, ctypes.c_uint64, _P])
 _lib.register("n3_py_random_shuffle", [_P, _P, _I, _P])
+_lib.register("n3_py_shuffle_steps", [_P, _I, _P, _P])
 _lib.register("n3_beam_init", [ctypes.POINTER(BeamDesc), _I, _P])
 _lib.register("n3_beam_generation", [ctypes.POINTER(BeamDesc), _I, _P])
 
@@ -132,6 +133,23 @@ def py_random_shuffle_device(values, seed: int):
     _lib.call("n3_py_random_seed", _lib.ptr(state), abs(int(seed)) & (2**64 - 1), None)
     _lib.call("n3_py_random_shuffle", _lib.ptr(state), _lib.ptr(v), int(v.numel()), None)
     return v.cpu().numpy()
+
+
+def py_shuffle_steps_device(counts, seed: int):
+    """The j of every step of random.Random(seed).shuffle over each count in
+    ``counts`` in turn (one generator), resolved on the device as the beam
+    selection resolves its shuffle; returns one int32 array per count
+    (entry s = the j of step s, entry 0 = 0)."""
+    t = _lib.torch()
+    dev = _lib.require_device()
+    state = t.empty(625, dtype=t.int32, device=dev)
+    _lib.call("n3_py_random_seed", _lib.ptr(state), abs(int(seed)) & (2**64 - 1), None)
+    out = []
+    for count in counts:
+        js = t.empty(max(1, int(count)), dtype=t.int32, device=dev)
+        _lib.call("n3_py_shuffle_steps", _lib.ptr(state), int(count), _lib.ptr(js), None)
+        out.append(js[:int(count)].cpu().numpy())
+    return out
 
 
 class DeviceBeam:

@@ -166,3 +166,27 @@ def test_rejects_unsupported_sizes(cuda):
     with pytest.raises(ValueError):
         gds.gpu_device_beam_search(init, seed=1, generations=1, population=70000, elite_size=8, max_strength=2,
                                    energy_window=2)
+
+
+def cpython_steps(counts, seed):
+    """The j of every step of random.Random(seed).shuffle, for each count in turn."""
+    rng = Random(seed)
+    out = []
+    for count in counts:
+        js = [0] * count
+        for i in reversed(range(1, count)):
+            js[i] = rng._randbelow(i + 1)
+        out.append(np.asarray(js, np.int32))
+    return out
+
+
+@pytest.mark.parametrize("seed", [0, 7, 91001, 2**63 + 12345])
+def test_shuffle_draws_resolved_by_the_cta_are_cpythons(cuda, seed):
+    """The CTA-wide resolver (wide draw widths) and the warp (the last steps),
+    over one generator: counts across block, batch and width boundaries, a
+    fresh and a part-used state, the largest count."""
+    counts = [0, 1, 2, 3, 257, 300, 1000, 4097, 5000, 12345, 40000, 65536, 511, 70]
+    got = gds.py_shuffle_steps_device(counts, seed)
+    want = cpython_steps(counts, seed)
+    for c, g, w in zip(counts, got, want):
+        assert np.array_equal(g, w), c

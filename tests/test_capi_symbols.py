@@ -86,3 +86,5 @@ def test_beam_entry_points_check_arguments_on_the_host():
         assert L.n3_beam_generation(ctypes.byref(d), 1, None) == _lib.N3_ERR_RANGE, field
     assert L.n3_beam_mutate(None, None, None, 4, 1, 75, 64, 2, 12, 85, 1, 1, None, None, None) == _lib.N3_ERR_ARG
     assert L.n3_py_random_shuffle(None, None, 3, None) == _lib.N3_ERR_ARG
+    assert L.n3_py_shuffle_steps(None, 3, None, None) == _lib.N3_ERR_ARG
+    assert L.n3_py_shuffle_steps(ctypes.c_void_p(16), 65537, ctypes.c_void_p(16), None) == _lib.N3_ERR_RANGE
