@@ -186,9 +186,17 @@ __global__ void __launch_bounds__(512, 1) temper_kernel(const TemperArgs A) {
       wp.s_q = ch.umbrella[2 * pos];
       wp.c2s_q = ch.umbrella[2 * pos + 1];
     }
+    // The proposals' Philox blocks 32 at a time: lane l makes the block of
+    // proposal p + l (counter + l), and proposal p + j takes lane j's by shuffle.
+    U4 batch = {0u, 0u, 0u, 0u};
     for (int p = 0; p < per_round; ++p) {
-      const U4 rnd = philox4x32_10(U4{(uint32_t)counter, (uint32_t)(counter >> 32), (uint32_t)c, kTagPropose},
-                                   k0, k1);
+      const int j = p & 31;
+      if (j == 0) {
+        const uint64_t cl = counter + (uint64_t)(tm.t & 31);
+        batch = philox4x32_10(U4{(uint32_t)cl, (uint32_t)(cl >> 32), (uint32_t)c, kTagPropose}, k0, k1);
+      }
+      const U4 rnd = {__shfl_sync(0xffffffffu, batch.x, j), __shfl_sync(0xffffffffu, batch.y, j),
+                      __shfl_sync(0xffffffffu, batch.z, j), __shfl_sync(0xffffffffu, batch.w, j)};
       const int acc = propose_walk<WPC, BIAS, UMB>(tm, cs, bs, m, lut, hist, rnd, counter, c, thr, W, E, err, wp,
                                                    removed);
       ++counter;
