@@ -626,9 +626,14 @@ __global__ void __launch_bounds__(kStepWarps * 32, 1) learned_step_kernel(const 
   int bestE = ch.best_energy[c];
   uint32_t err = 0, n_acc = 0;
   float st_abs = 0.f, st_n = 0.f, st_acc = 0.f, st_dE = 0.f;  // this chain's statistics (lane-uniform)
+  // the moves' Philox blocks 32 at a time: lane l makes move k0 + l's, move k takes lane k % 32's
+  U4 batch = {0u, 0u, 0u, 0u};
   for (int k = 0; k < A.moves; ++k) {
-    const U4 r = philox4x32_10(U4{(uint32_t)step, (uint32_t)(step >> 32), (uint32_t)c,
-                                  kTagCandidate | 0xFF00u | (uint32_t)k}, A.k0, A.k1);
+    const int j = k & 31;
+    if (j == 0)
+      batch = philox4x32_10(U4{(uint32_t)step, (uint32_t)(step >> 32), (uint32_t)c,
+                               kTagCandidate | 0xFF00u | (uint32_t)(k + lane)}, A.k0, A.k1);
+    const U4 r = {__shfl_sync(0xffffffffu, batch.x, j), __shfl_sync(0xffffffffu, batch.y, j), 0u, 0u};
     // inclusive prefix of the weights in candidate order: within the lane, then across lanes
     float pre[kPer];
     pre[0] = w[0];
