@@ -54,6 +54,10 @@ struct Team {
   int bar;       // named barrier id (WPC > 1)
   int* red;      // reduction scratch (WPC > 1)
   int phase;     // which half of red the next reduction uses
+  // KEYED moves only: the direction-table key row * kLutW + column of each of
+  // this thread's slots (set by the caller from the state; a KEYED move keeps
+  // it up to date)
+  int key[kSlots];
   __device__ __forceinline__ void sync() const {
     if constexpr (WPC == 1) {
       __syncwarp();
@@ -79,8 +83,9 @@ struct Team {
   }
 };
 
-// hist_build_full for a team: slot k = t + 32 WPC j, j < kSlots.
-template <int WPC>
+// hist_build_full for a team: slot k = t + 32 WPC j, j < kSlots; KEYED: the
+// slots' table keys come from tm.key instead of the columns in cs.
+template <int WPC, bool KEYED = false>
 __device__ __forceinline__ int team_hist_build(const Team<WPC>& tm, const int* __restrict__ cs, int m, int rx, int cx,
                                                int skip0, int skip1, const uint16_t* __restrict__ lutf,
                                                uint32_t* __restrict__ hist, int (&ids)[Team<WPC>::kSlots]) {
@@ -91,7 +96,7 @@ __device__ __forceinline__ int team_hist_build(const Team<WPC>& tm, const int* _
     const int k = tm.t + Team<WPC>::kThreads * j;
     ids[j] = -1;
     if (k < m && k != skip0 && k != skip1 && (k >> 1) != rx) {
-      const int id = base[(k >> 1) * kLutW + cs[k]];
+      const int id = base[KEYED ? tm.key[j] : (k >> 1) * kLutW + cs[k]];
       ids[j] = id;
       pairs += hist_add(hist, id);
     }
@@ -111,7 +116,9 @@ __device__ __forceinline__ void team_hist_release(uint32_t* hist, const int (&id
 // because t(v') >= 0, and thr is non-increasing, so a proposal with d1 >= 1 and
 // (d1 >= W or z >= thr[d1]) is rejected exactly as the full test would reject
 // it, without the second histogram; *dE_out then holds d1.
-template <int WPC, bool FORCE, bool UMB = false, bool EARLY = false>
+// KEYED: the histograms and the joint count take the slots' table keys from
+// tm.key (see Team), and an accepted move updates them.
+template <int WPC, bool FORCE, bool UMB = false, bool EARLY = false, bool KEYED = false>
 __device__ __forceinline__ int team_move(Team<WPC>& tm, int* __restrict__ cs, int* __restrict__ bs, int m,
                                          const uint16_t* __restrict__ lutf, uint32_t* __restrict__ hist, int u, int v,
                                          uint32_t z, const uint32_t* __restrict__ thr, int W, int& E, uint32_t& err,
@@ -121,7 +128,7 @@ __device__ __forceinline__ int team_move(Team<WPC>& tm, int* __restrict__ cs, in
   const int ru = u >> 1, rv = v >> 1, cu = cs[u], cv = cs[v];
   int ids[S], cnt_new[S];
   // centre u' = (r_u, c_v)
-  const int part_a = team_hist_build(tm, cs, m, ru, cv, u, v, lutf, hist, ids);
+  const int part_a = team_hist_build<WPC, KEYED>(tm, cs, m, ru, cv, u, v, lutf, hist, ids);
   tm.sync();
   const int line_new = dir_id_full(lutf, rv - ru, cu - cv);
   const int j_new = hist_get(hist, line_new);
@@ -130,7 +137,10 @@ __device__ __forceinline__ int team_move(Team<WPC>& tm, int* __restrict__ cs, in
 #pragma unroll
   for (int j = 0; j < S; ++j) {
     const int k = tm.t + TT * j;
-    if (k < m && k != u && k != v) joint += (rv - ru) * (cs[k] - cu) == (cv - cu) * ((k >> 1) - ru);
+    if (k < m && k != u && k != v) {
+      const int ck = KEYED ? tm.key[j] - (k >> 1) * kLutW : cs[k];
+      joint += (rv - ru) * (ck - cu) == (cv - cu) * ((k >> 1) - ru);
+    }
   }
   int t_a, sum_joint;
   if constexpr (EARLY) {
@@ -152,7 +162,7 @@ __device__ __forceinline__ int team_move(Team<WPC>& tm, int* __restrict__ cs, in
   team_hist_release<WPC>(hist, ids);
   tm.sync();
   // centre v' = (r_v, c_u)
-  const int part_b = team_hist_build(tm, cs, m, rv, cu, u, v, lutf, hist, ids);
+  const int part_b = team_hist_build<WPC, KEYED>(tm, cs, m, rv, cu, u, v, lutf, hist, ids);
   tm.sync();
 #pragma unroll
   for (int j = 0; j < S; ++j) cnt_new[j] += ids[j] >= 0 ? hist_get(hist, ids[j]) - 1 : 0;
@@ -178,7 +188,7 @@ __device__ __forceinline__ int team_move(Team<WPC>& tm, int* __restrict__ cs, in
   // Old-side histograms: exact badness change of every other point.
   tm.sync();
   int dB[S];
-  const int part_c = team_hist_build(tm, cs, m, ru, cu, u, v, lutf, hist, ids);
+  const int part_c = team_hist_build<WPC, KEYED>(tm, cs, m, ru, cu, u, v, lutf, hist, ids);
   tm.sync();
   const int line_old = dir_id_full(lutf, rv - ru, cv - cu);
   const int j_old = hist_get(hist, line_old);
@@ -188,7 +198,7 @@ __device__ __forceinline__ int team_move(Team<WPC>& tm, int* __restrict__ cs, in
   tm.sync();
   team_hist_release<WPC>(hist, ids);
   tm.sync();
-  const int part_d = team_hist_build(tm, cs, m, rv, cv, u, v, lutf, hist, ids);
+  const int part_d = team_hist_build<WPC, KEYED>(tm, cs, m, rv, cv, u, v, lutf, hist, ids);
   tm.sync();
 #pragma unroll
   for (int j = 0; j < S; ++j) dB[j] -= ids[j] >= 0 ? hist_get(hist, ids[j]) - 1 : 0;
@@ -202,6 +212,7 @@ __device__ __forceinline__ int team_move(Team<WPC>& tm, int* __restrict__ cs, in
   for (int j = 0; j < S; ++j) {
     const int k = tm.t + TT * j;
     if (k < m && k != u && k != v) bs[k] += dB[j];
+    if (KEYED) tm.key[j] += k == u ? cv - cu : (k == v ? cu - cv : 0);
   }
   if (tm.t == 0) {
     bs[u] = t_a + j_new;
@@ -221,7 +232,7 @@ __device__ __forceinline__ int move_exact_t(int* __restrict__ cs, int* __restric
                                             int u, int v, uint32_t z, const uint32_t* __restrict__ thr, int W, int& E,
                                             uint32_t& err, int* dE_out, int64_t umb_q = 0,
                                             const uint32_t* __restrict__ frac = nullptr) {
-  Team<1> tm{lane, 0, nullptr, 0};
+  Team<1> tm{lane, 0, nullptr, 0, {}};
   return team_move<1, FORCE, UMB, EARLY>(tm, cs, bs, m, lutf, hist, u, v, z, thr, W, E, err, dE_out, umb_q, frac);
 }
 
@@ -303,11 +314,12 @@ __device__ __forceinline__ int propose_walk(Team<WPC>& tm, int* __restrict__ cs,
   }
   if (!legal_swap(cs, u, v)) return 0;
   int dE;
-  if (!UMB) return team_move<WPC, false, false, true>(tm, cs, bs, m, lutf, hist, u, v, rnd.z, thr, W, E, err, &dE);
+  if (!UMB)
+    return team_move<WPC, false, false, true, true>(tm, cs, bs, m, lutf, hist, u, v, rnd.z, thr, W, E, err, &dE);
   const int dd = umbrella_distance_delta(P.ref, u, v, cs[u], cs[v]);
   const int64_t umb = P.s_q * (int64_t)(2 * removed * dd + dd * dd) - P.c2s_q * (int64_t)dd;
-  const int acc = team_move<WPC, false, true>(tm, cs, bs, m, lutf, hist, u, v, rnd.z, thr, W, E, err, &dE, umb,
-                                              P.frac);
+  const int acc = team_move<WPC, false, true, false, true>(tm, cs, bs, m, lutf, hist, u, v, rnd.z, thr, W, E, err,
+                                                           &dE, umb, P.frac);
   if (acc) removed += dd;
   return acc;
 }

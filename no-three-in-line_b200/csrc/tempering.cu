@@ -121,7 +121,7 @@ __global__ void __launch_bounds__(512, 1) temper_kernel(const TemperArgs A) {
   int* L_stop = CS > 1 ? cluster.map_shared_rank(ld_stop, 0) : ld_stop;
 
   const int warp = threadIdx.x / TT;  // this chain's index in the CTA
-  Team<WPC> tm{(int)threadIdx.x % TT, 1 + warp, team_red + 2 * WPC * warp, 0};
+  Team<WPC> tm{(int)threadIdx.x % TT, 1 + warp, team_red + 2 * WPC * warp, 0, {}};
   const int c = blockIdx.x * cpb + warp;
   const int lad = c / L;
   const int li = c % L;
@@ -137,6 +137,11 @@ __global__ void __launch_bounds__(512, 1) temper_kernel(const TemperArgs A) {
   for (int s = tm.t; s < m; s += TT) {
     cs[s] = ch.cols[(size_t)c * kMaxM + s];
     bs[s] = ch.badness[(size_t)c * kMaxM + s];
+  }
+#pragma unroll
+  for (int j = 0; j < Team<WPC>::kSlots; ++j) {  // this thread's slots (the ones it loaded)
+    const int k = tm.t + TT * j;
+    tm.key[j] = k < m ? (k >> 1) * kLutW + (int)ch.cols[(size_t)c * kMaxM + k] : 0;
   }
   int E = ch.energy[c], bestE = ch.best_energy[c];
   int removed = UMB ? ch.removed[c] : 0;
