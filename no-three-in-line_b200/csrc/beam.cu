@@ -254,12 +254,15 @@ __global__ void __launch_bounds__(kDeltaWarps * 32, 1) child_delta_kernel(const 
       bs[s] = A.ebad[(size_t)par * m + s];
     }
     __syncwarp();
+    Team<1> tm{lane, 0, nullptr, 0, {}};
+    team_load_keys(tm, cs, m);  // the slots' table keys, kept in registers across the moves
     int E = A.es[par];
     const int k_end = min(A.nmoves[c], A.moves_cap);
     for (int k = 0; k < k_end; ++k) {
       const int mv = A.moves[(size_t)c * A.moves_cap + k];
       int dE;
-      move_exact_t<true>(cs, bs, m, lutf, hist, lane, mv & 0xFF, (mv >> 8) & 0xFF, 0u, nullptr, 0, E, err, &dE);
+      team_move<1, true, false, false, true>(tm, cs, bs, m, lutf, hist, mv & 0xFF, (mv >> 8) & 0xFF, 0u, nullptr, 0,
+                                             E, err, &dE);
     }
     if (lane == 0) A.scores[c] = E;
     for (int s = lane; s < m; s += 32) A.badness[(size_t)c * m + s] = bs[s];

@@ -104,6 +104,17 @@ __device__ __forceinline__ int team_hist_build(const Team<WPC>& tm, const int* _
   return pairs;
 }
 
+// tm.key from this thread's own slots of the state in cs (the thread reads
+// only the slots it owns, so it needs no barrier after storing them itself).
+template <int WPC>
+__device__ __forceinline__ void team_load_keys(Team<WPC>& tm, const int* __restrict__ cs, int m) {
+#pragma unroll
+  for (int j = 0; j < Team<WPC>::kSlots; ++j) {
+    const int k = tm.t + Team<WPC>::kThreads * j;
+    tm.key[j] = k < m ? (k >> 1) * kLutW + cs[k] : 0;
+  }
+}
+
 template <int WPC>
 __device__ __forceinline__ void team_hist_release(uint32_t* hist, const int (&ids)[Team<WPC>::kSlots]) {
 #pragma unroll

@@ -596,6 +596,8 @@ __global__ void __launch_bounds__(kStepWarps * 32, 1) learned_step_kernel(const 
     cs[s] = ch.cols[(size_t)c * kMaxM + s];
     bs[s] = ch.badness[(size_t)c * kMaxM + s];
   }
+  Team<1> tm{lane, 0, nullptr, 0, {}};
+  team_load_keys(tm, cs, m);  // the slots' table keys, kept in registers across the moves
   const int temp = ch.temp_of[c];
   const float T = A.temps[temp];
   // softmax(-pred / T) over the legal candidates, sampled by inverse CDF;
@@ -698,7 +700,8 @@ __global__ void __launch_bounds__(kStepWarps * 32, 1) learned_step_kernel(const 
       A.rb_bad[slot * kChainFeat + s] = (uint8_t)(s < m ? min(bs[s], 255) : 0);
     __syncwarp();
     int dE = 0;
-    const int acc = move_exact(cs, bs, m, lut, hist, lane, u, v, r.y, thr, ch.acc_width, E, err, &dE);
+    const int acc = team_move<1, false, false, false, true>(tm, cs, bs, m, lut, hist, u, v, r.y, thr, ch.acc_width, E,
+                                                            err, &dE);
     if (lane == 0) A.rb_dE[slot] = (int16_t)max(-32768, min(32767, dE));
     n_acc += acc ? 1u : 0u;
     st_abs += fabsf(p - (float)dE);
