@@ -26,9 +26,20 @@ namespace multi {
 
 constexpr int kT = kSlotsPerLane;  // 5 slots per lane
 
+// This lane's slots' direction-table keys row * kLutW + column (the state is
+// fixed for the whole kernel, so the keys stay in registers).
+__device__ __forceinline__ void lane_keys(const int* __restrict__ cs, int m, int lane, int (&key)[kT]) {
+#pragma unroll
+  for (int t = 0; t < kT; ++t) {
+    const int k = lane + 32 * t;
+    key[t] = k < m ? (k >> 1) * kLutW + cs[k] : 0;
+  }
+}
+
 // hist_build_full over A: slots whose bit t is set in `skip` (this lane's slot
 // lane + 32 t is a moved one) are left out, and so are the points in row rx.
-__device__ __forceinline__ int hist_build_excl(const int* __restrict__ cs, int m, int rx, int cx, uint32_t skip,
+// key: lane_keys of the state.
+__device__ __forceinline__ int hist_build_excl(const int (&key)[kT], int m, int rx, int cx, uint32_t skip,
                                                const uint16_t* __restrict__ lutf, uint32_t* __restrict__ hist,
                                                int lane, int (&ids)[kT]) {
   const uint16_t* base = lutf + kFullLutCentre - (rx * kLutW + cx);
@@ -38,7 +49,7 @@ __device__ __forceinline__ int hist_build_excl(const int* __restrict__ cs, int m
     const int k = lane + 32 * t;
     ids[t] = -1;
     if (k < m && !((skip >> t) & 1u) && (k >> 1) != rx) {
-      const int id = base[(k >> 1) * kLutW + cs[k]];
+      const int id = base[key[t]];
       ids[t] = id;
       pairs += hist_add(hist, id);
     }
@@ -61,12 +72,12 @@ __device__ __forceinline__ int collinear(int r0, int c0, int r1, int c1, int r2,
 }
 
 // side() of `count` positions (distinct rows) over A; all lanes return the sum.
-__device__ int side_sum(const int* __restrict__ cs, int m, const int* rows, const int* cols, int count, uint32_t skip,
+__device__ __forceinline__ int side_sum(const int (&key)[kT], int m, const int* rows, const int* cols, int count, uint32_t skip,
                         const uint16_t* __restrict__ lutf, uint32_t* __restrict__ hist, int lane) {
   int total = 0;
   for (int i = 0; i < count; ++i) {
     int ids[kT];
-    const int part = hist_build_excl(cs, m, rows[i], cols[i], skip, lutf, hist, lane, ids);
+    const int part = hist_build_excl(key, m, rows[i], cols[i], skip, lutf, hist, lane, ids);
     __syncwarp();
     int pair_lines = 0;
     if (lane == 0)
@@ -105,6 +116,8 @@ __global__ void __launch_bounds__(kWarps * 32) three_cycle_kernel(const int32_t*
   __syncthreads();
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   uint32_t* hist = hist_all + warp * kDirWords;
+  int key[kT];
+  lane_keys(cs, m, lane, key);
   for (int c = blockIdx.x * kWarps + warp; c < count; c += gridDim.x * kWarps) {
     const int u = cand[4 * c], v = cand[4 * c + 1], w = cand[4 * c + 2], o = cand[4 * c + 3];
     // the moves search.py:38-65 generates: three slots in three rows, three
@@ -128,8 +141,8 @@ __global__ void __launch_bounds__(kWarps * 32) three_cycle_kernel(const int32_t*
     const int rows[3] = {u >> 1, v >> 1, w >> 1};
     const int old_cols[3] = {cs[u], cs[v], cs[w]};
     const int new_cols[3] = {nu, nv, nw};
-    const int before = side_sum(cs, m, rows, old_cols, 3, skip, lutf, hist, lane);
-    const int after = side_sum(cs, m, rows, new_cols, 3, skip, lutf, hist, lane);
+    const int before = side_sum(key, m, rows, old_cols, 3, skip, lutf, hist, lane);
+    const int after = side_sum(key, m, rows, new_cols, 3, skip, lutf, hist, lane);
     if (lane == 0) out[c] = current - before + after;
   }
 }
@@ -205,13 +218,15 @@ __global__ void __launch_bounds__(kWarps * 32) scan_kernel(const ScanArgs A) {
     partner[i] = cs[T[i] ^ 1];
   }
   const uint32_t skip = skip_mask(lane, T, 4);
-  const int before = side_sum(cs, m, rowT, colT, 4, skip, lutf, hist, lane);
+  int key[kT];
+  lane_keys(cs, m, lane, key);
+  const int before = side_sum(key, m, rowT, colT, 4, skip, lutf, hist, lane);
   // the 12 candidate positions: target i with the column of source j != i (index 3 i + (j > i ? j - 1 : j))
   for (int a = 0; a < 12; ++a) {
     const int i = a / 3, jj = a % 3, j = jj >= i ? jj + 1 : jj;
     const int rx = rowT[i], cx = colT[j];
     int ids[kT];
-    const int part = hist_build_excl(cs, m, rx, cx, skip, lutf, hist, lane, ids);
+    const int part = hist_build_excl(key, m, rx, cx, skip, lutf, hist, lane, ids);
     __syncwarp();
     if (lane < 12) {
       const int b = lane, ib = b / 3, jb = b % 3 >= ib ? b % 3 + 1 : b % 3;
