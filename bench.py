@@ -286,6 +286,31 @@ def secondary_measurements(dev, p, q):
     out["swap_delta_batch"] = {"moves": M, "legal": legal, "deltas_per_s": 10 * M / (a.elapsed_time(b) / 1e3),
                                "kernel": "n3::swap_delta_kernel<false> (direction-class, no badness output)"}
     launches += 13
+    # every 2-switch partner of every slot of 64 n=75 states (the reference plugin's
+    # two_switch_scores, gpu_delta.py:19-75): 9600 anchors x 150 partners
+    S = 64
+    sc = torch.empty(S, dtype=torch.int32, device=dev)
+    sb = torch.empty((S, 2 * N), dtype=torch.int32, device=dev)
+    _lib.check(L.n3_score_columns(cols.data_ptr(), S, N, sc.data_ptr(), sb.data_ptr(), sptr), "n3_score_columns")
+    anchors = torch.from_numpy(np.stack([np.repeat(np.arange(S), 2 * N), np.tile(np.arange(2 * N), S)], 1)
+                               .astype(np.int32)).to(dev)
+    A = anchors.shape[0]
+    ts = torch.empty((A, 2 * N), dtype=torch.int32, device=dev)
+    for _ in range(3):
+        _lib.check(L.n3_two_switch_scores(cols.data_ptr(), sb.data_ptr(), sc.data_ptr(), S, N, anchors.data_ptr(), A,
+                                          ts.data_ptr(), sptr), "n3_two_switch_scores")
+    a.record()
+    for _ in range(10):
+        _lib.check(L.n3_two_switch_scores(cols.data_ptr(), sb.data_ptr(), sc.data_ptr(), S, N, anchors.data_ptr(), A,
+                                          ts.data_ptr(), sptr), "n3_two_switch_scores")
+    b.record()
+    b.synchronize()
+    legal_ts = int((ts != gpu_delta.SENTINEL).sum().item())
+    out["two_switch_scores"] = {"anchors": A, "partners_scored": A * 2 * N, "legal": legal_ts,
+                                "us_per_call": a.elapsed_time(b) / 10 * 1e3,
+                                "scores_per_s": 10 * A * 2 * N / (a.elapsed_time(b) / 1e3),
+                                "kernel": "n3::partner_scores_kernel<false>"}
+    launches += 14
     # C3: 2048 chains at n=75, 32 ladders of 64 temperatures, exchange every 10 sweeps
     pc, qc = state.seeded_population(N, 2048)
     ch = tempering.TemperingChains(state.pq_to_columns(pc, qc), np.tile(tempering.geometric_ladder(0.05, 5.0, 64), 32),

@@ -206,26 +206,35 @@ __global__ void __launch_bounds__(kDeltaWarps * 32) swap_delta_kernel(const int1
   }
 }
 
+// Shared memory of partner_scores_kernel: the full signed direction table, a
+// histogram per warp, the anchor's state.
+struct PartnerSmem {
+  static constexpr size_t bytes = kFullLutBytes + sizeof(uint32_t) * kDirWords * kDeltaWarps + sizeof(int) * kMaxM;
+};
+
 // Scores of every partner of anchor slots (the reference plugin
 // two_switch_scores, src/no_three_75/gpu_delta.py:19-75, and
 // evaluate_two_switches / evaluate_transpositions, accelerated.py:40-195):
 //   out = current - (bad[u] + bad[v] - joint(u, v)) + t(u') + t(v') + j(u', v')
 // One CTA per anchor; its warps split the partners.  SAME_LAYER restricts
-// partners to slots of u's layer and indexes the output by partner row.
+// partners to slots of u's layer and indexes the output by partner row.  The
+// anchor's state is fixed for all its partners, so each lane keeps the
+// direction-table keys row * kLutW + column of its slots in registers and a
+// histogram insertion is one load from the full signed table and one atomic.
 template <bool SAME_LAYER>
 __global__ void __launch_bounds__(kDeltaWarps * 32) partner_scores_kernel(
     const int16_t* __restrict__ cols, const int32_t* __restrict__ badness, const int32_t* __restrict__ current,
-    int B, int n, const int32_t* __restrict__ anchors, int A, const uint16_t* __restrict__ g_lut,
+    int B, int n, const int32_t* __restrict__ anchors, int A, const uint16_t* __restrict__ g_lut_full,
     int32_t* __restrict__ out) {
   extern __shared__ __align__(16) unsigned char smem[];
-  uint16_t* lut;
-  uint32_t* hist_all;
-  int *cs_all, *aux_all;
-  load_lut_and_clear(smem, g_lut, lut, hist_all, cs_all, aux_all);
+  uint16_t* lutf = reinterpret_cast<uint16_t*>(smem);
+  uint32_t* hist_all = reinterpret_cast<uint32_t*>(smem + kFullLutBytes);
+  int* cs = reinterpret_cast<int*>(hist_all + kDirWords * kDeltaWarps);  // one state per CTA: shared by all warps
+  full_lut_copy(lutf, g_lut_full);
+  for (int i = threadIdx.x; i < kDirWords * kDeltaWarps; i += blockDim.x) hist_all[i] = 0u;
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int m = 2 * n;
   const int width = SAME_LAYER ? n : m;
-  int* cs = cs_all;  // one state per CTA: shared by all warps
   uint32_t* hist = hist_all + warp * kDirWords;
   for (int a = blockIdx.x; a < A; a += gridDim.x) {
     const int b = anchors[2 * a], u = anchors[2 * a + 1];
@@ -241,6 +250,28 @@ __global__ void __launch_bounds__(kDeltaWarps * 32) partner_scores_kernel(
     const int ru = u >> 1, cu = cs[u];
     const int cur = current[b];
     const int bad_u = badness[(size_t)b * m + u];
+    int key[kSlotsPerLane];
+#pragma unroll
+    for (int t = 0; t < kSlotsPerLane; ++t) {
+      const int k = lane + 32 * t;
+      key[t] = k < m ? (k >> 1) * kLutW + cs[k] : 0;
+    }
+    // one histogram of centre (rx, cx) over the slots other than u, v and row rx
+    auto build = [&](int rx, int cx, int v, int (&ids)[kSlotsPerLane]) {
+      const uint16_t* base = lutf + kFullLutCentre - (rx * kLutW + cx);
+      int pairs = 0;
+#pragma unroll
+      for (int t = 0; t < kSlotsPerLane; ++t) {
+        const int k = lane + 32 * t;
+        ids[t] = -1;
+        if (k < m && k != u && k != v && (k >> 1) != rx) {
+          const int id = base[key[t]];
+          ids[t] = id;
+          pairs += hist_add(hist, id);
+        }
+      }
+      return pairs;
+    };
     for (int w = warp; w < width; w += kDeltaWarps) {
       const int v = SAME_LAYER ? 2 * w + (u & 1) : w;
       // The reference's partner rule (accelerated.py:146-151, gpu_delta.py:175-180):
@@ -253,17 +284,21 @@ __global__ void __launch_bounds__(kDeltaWarps * 32) partner_scores_kernel(
       const int rv = v >> 1, cv = cs[v];
       // joint(u, v): points other than u, v on the line through u and v
       int joint = 0;
-      for (int k = lane; k < m; k += 32)
-        if (k != u && k != v) joint += (rv - ru) * (cs[k] - cu) == (cv - cu) * ((k >> 1) - ru);
+#pragma unroll
+      for (int t = 0; t < kSlotsPerLane; ++t) {
+        const int k = lane + 32 * t;
+        if (k < m && k != u && k != v)
+          joint += (rv - ru) * (key[t] - (k >> 1) * kLutW - cu) == (cv - cu) * ((k >> 1) - ru);
+      }
       int part = joint << 16;  // two sums in one reduction: joint (high) and pairs (low)
       int ids[kSlotsPerLane];
-      part += hist_build(cs, m, ru, cv, u, v, lut, hist, lane, ids);  // u' = (r_u, c_v)
+      part += build(ru, cv, v, ids);  // u' = (r_u, c_v)
       __syncwarp();
-      const int j_new = hist_get(hist, dir_id(lut, rv - ru, cu - cv));
+      const int j_new = hist_get(hist, dir_id_full(lutf, rv - ru, cu - cv));
       __syncwarp();
       hist_release(hist, ids);
       __syncwarp();
-      part += hist_build(cs, m, rv, cu, u, v, lut, hist, lane, ids);  // v' = (r_v, c_u)
+      part += build(rv, cu, v, ids);  // v' = (r_v, c_u)
       __syncwarp();
       hist_release(hist, ids);
       __syncwarp();
@@ -282,15 +317,15 @@ __global__ void __launch_bounds__(kDeltaWarps * 32) partner_scores_kernel(
 namespace n3host {
 
 template <class K>
-static int prepare(K kernel) {
-  return allow_smem(reinterpret_cast<const void*>(kernel), n3::DeltaSmem::bytes);
+static int prepare(K kernel, size_t bytes = n3::DeltaSmem::bytes) {
+  return allow_smem(reinterpret_cast<const void*>(kernel), bytes);
 }
 
 int prepare_delta() {
   N3_TRY(prepare(n3::swap_delta_kernel<true>));
   N3_TRY(prepare(n3::swap_delta_kernel<false>));
-  N3_TRY(prepare(n3::partner_scores_kernel<true>));
-  return prepare(n3::partner_scores_kernel<false>);
+  N3_TRY(prepare(n3::partner_scores_kernel<true>, n3::PartnerSmem::bytes));
+  return prepare(n3::partner_scores_kernel<false>, n3::PartnerSmem::bytes);
 }
 
 static int check_state_args(int B, int n, const void* cols) {
@@ -329,16 +364,16 @@ static int launch_partners(bool same_layer, const int16_t* cols, const int32_t* 
   if (A == 0) return N3_OK;
   if (!badness || !current || !anchors || !out) return set_error(N3_ERR_ARG, "null pointer");
   N3_TRY(ensure_device_tables());
-  const uint16_t* lut = dir_lut_device_ptr();
+  const uint16_t* lutf = dir_lut_full_device_ptr();
   const int grid = A < sm_count() * 4 ? A : sm_count() * 4;
   if (same_layer) {
-    N3_TRY(prepare(n3::partner_scores_kernel<true>));
-    n3::partner_scores_kernel<true><<<grid, n3::kDeltaWarps * 32, n3::DeltaSmem::bytes, st>>>(
-        cols, badness, current, B, n, anchors, A, lut, out);
+    N3_TRY(prepare(n3::partner_scores_kernel<true>, n3::PartnerSmem::bytes));
+    n3::partner_scores_kernel<true><<<grid, n3::kDeltaWarps * 32, n3::PartnerSmem::bytes, st>>>(
+        cols, badness, current, B, n, anchors, A, lutf, out);
   } else {
-    N3_TRY(prepare(n3::partner_scores_kernel<false>));
-    n3::partner_scores_kernel<false><<<grid, n3::kDeltaWarps * 32, n3::DeltaSmem::bytes, st>>>(
-        cols, badness, current, B, n, anchors, A, lut, out);
+    N3_TRY(prepare(n3::partner_scores_kernel<false>, n3::PartnerSmem::bytes));
+    n3::partner_scores_kernel<false><<<grid, n3::kDeltaWarps * 32, n3::PartnerSmem::bytes, st>>>(
+        cols, badness, current, B, n, anchors, A, lutf, out);
   }
   return check_launch("partner_scores_kernel");
 }
