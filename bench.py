@@ -384,23 +384,30 @@ def secondary_measurements(dev, p, q):
                                       "infer_frac_of_bf16_peak": flop / infer_s / 1e12 / peaks["bf16_tflops"],
                                       "peak_kind": kind}
     launches += 13
-    # learned vs plain: time to an energy level, one seed, 20 s of device time per
-    # run (the full comparison over seeds and longer budgets is --mode time-to-target)
+    # learned vs plain: time to an energy level, seeds 1 and 2, 20 s of device time per
+    # run (the full comparison over more seeds and budgets is --mode time-to-target)
     from no_three_in_line_b200 import compare
 
-    budget, methods = 20.0, ("plain", "learned:x16:b85")
-    res = compare.compare([1], 12, budget, methods=methods)
-    lvl = res["common_level"]
-    t_plain, t_learned = (res[m]["median_s_to_common_level"] for m in methods)
+    budget, methods, seeds = 20.0, ("plain", "learned:x16:b85"), [1, 2]
+    res = compare.compare(seeds, 12, budget, methods=methods)
+    levels = {}
+    for k, v in res["time_to_level"].items():
+        if int(k) > 50:
+            continue
+        row = {m: (v[m]["median_s"] if v[m]["reached"] == len(seeds) else None) for m in methods}
+        if row[methods[0]] is not None and row[methods[1]]:
+            row["ratio"] = row[methods[0]] / row[methods[1]]
+        levels[k] = row
+    both = [k for k, r in levels.items() if "ratio" in r]
     out["time_to_level_short"] = {
-        "workload": "n=75, 2048 chains, 32 ladders x 64 temperatures (0.05..5.0), seed 1",
-        "methods": list(methods), "budget_s_per_run": budget, "target": 12,
+        "workload": "n=75, 2048 chains, 32 ladders x 64 temperatures (0.05..5.0)",
+        "methods": list(methods), "seeds": seeds, "budget_s_per_run": budget, "target": 12,
         "target_reached": {m: res[m]["reached"] for m in methods},
-        "best_E": {m: res[m]["best_per_seed"][0] for m in methods},
-        "common_level": lvl, "seconds_to_common_level": {methods[0]: t_plain, methods[1]: t_learned},
-        "ratio_plain_over_learned": t_plain / t_learned if t_learned else None,
-        "time_to_level_s": {k: {m: (v[m]["median_s"] if v[m]["reached"] else None) for m in methods}
-                            for k, v in res["time_to_level"].items() if int(k) <= 50}}
+        "best_E_per_seed": {m: res[m]["best_per_seed"] for m in methods},
+        "lowest_level_both_reach": min((int(k) for k in both), default=None),
+        "median_ratio_plain_over_learned_at_that_level":
+            levels[str(min(int(k) for k in both))]["ratio"] if both else None,
+        "median_s_to_level": levels}
     return out, launches
 
 

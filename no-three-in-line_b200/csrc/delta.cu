@@ -32,10 +32,13 @@ namespace n3 {
 // Exact dE (and, if dbad != nullptr, this lane's badness changes for slots
 // lane + 32 t, plus the moved slots' changes in *dbad_u, *dbad_v) of a legal
 // move.  Uses the 4 centres u, v, u', v'; hist must be zeroed, is left zeroed.
+// lutf: the full signed direction table; key: this lane's slots' table keys
+// row * kLutW + column.
 template <bool BAD>
-__device__ int swap_delta_hist(const int* __restrict__ cs, int m, int u, int v, const uint16_t* __restrict__ lut,
-                               uint32_t* __restrict__ hist, int lane, int (&dbad)[kSlotsPerLane], int* dbad_u,
-                               int* dbad_v) {
+__device__ __forceinline__ int swap_delta_hist(const int* __restrict__ cs, const int (&key)[kSlotsPerLane], int m,
+                                               int u, int v, const uint16_t* __restrict__ lutf,
+                                               uint32_t* __restrict__ hist, int lane, int (&dbad)[kSlotsPerLane],
+                                               int* dbad_u, int* dbad_v) {
   const int ru = u >> 1, rv = v >> 1, cu = cs[u], cv = cs[v];
   // centre order: u, v, u', v'
   const int crow[4] = {ru, rv, ru, rv};
@@ -49,16 +52,30 @@ __device__ int swap_delta_hist(const int* __restrict__ cs, int m, int u, int v, 
 #pragma unroll
   for (int c = 0; c < 4; ++c) {
     int ids[kSlotsPerLane];
-    const int part = hist_build(cs, m, crow[c], ccol[c], u, v, lut, hist, lane, ids);
+    int part = 0;
+    {
+      const int rx = crow[c];
+      const uint16_t* base = lutf + kFullLutCentre - (rx * kLutW + ccol[c]);
+#pragma unroll
+      for (int t = 0; t < kSlotsPerLane; ++t) {
+        const int k = lane + 32 * t;
+        ids[t] = -1;
+        if (k < m && k != u && k != v && (k >> 1) != rx) {
+          const int id = base[key[t]];
+          ids[t] = id;
+          part += hist_add(hist, id);
+        }
+      }
+    }
     __syncwarp();
     tX[c] = warp_sum(part);
     const int sign = c < 2 ? -1 : 1;
     int line_id = -1;  // direction of the other moved point, for centres u and u'
     if (c == 0) {
-      line_id = dir_id(lut, rv - ru, cv - cu);
+      line_id = dir_id_full(lutf, rv - ru, cv - cu);
       j_old = hist_get(hist, line_id);
     } else if (c == 2) {
-      line_id = dir_id(lut, rv - ru, cu - cv);
+      line_id = dir_id_full(lutf, rv - ru, cu - cv);
       j_new = hist_get(hist, line_id);
     }
     if (BAD) {
@@ -131,7 +148,7 @@ __device__ int swap_delta_pairs(const int* __restrict__ cs, int m, int u, int v,
 constexpr int kDeltaWarps = 8;
 
 struct DeltaSmem {
-  static constexpr size_t lut_bytes = ((sizeof(uint16_t) * kLutSize + 15) / 16) * 16;
+  static constexpr size_t lut_bytes = kFullLutBytes;  // the full signed direction table
   static constexpr size_t bytes =
       lut_bytes + sizeof(uint32_t) * kDirWords * kDeltaWarps + sizeof(int) * kMaxM * kDeltaWarps * 2;
 };
@@ -142,7 +159,7 @@ __device__ __forceinline__ void load_lut_and_clear(unsigned char* smem, const ui
   hist_all = reinterpret_cast<uint32_t*>(smem + DeltaSmem::lut_bytes);
   cs_all = reinterpret_cast<int*>(hist_all + kDirWords * kDeltaWarps);
   aux_all = cs_all + kMaxM * kDeltaWarps;
-  for (int i = threadIdx.x; i < kLutSize; i += blockDim.x) lut[i] = g_lut[i];
+  full_lut_copy(lut, g_lut);
   for (int i = threadIdx.x; i < kDirWords * kDeltaWarps; i += blockDim.x) hist_all[i] = 0u;
   __syncthreads();
 }
@@ -168,8 +185,14 @@ __global__ void __launch_bounds__(kDeltaWarps * 32) swap_delta_kernel(const int1
   for (int mv = blockIdx.x * kDeltaWarps + warp; mv < M; mv += gridDim.x * kDeltaWarps) {
     const int b = moves[3 * mv], u = moves[3 * mv + 1], v = moves[3 * mv + 2];
     const bool in_range = b >= 0 && b < B && u >= 0 && u < m && v >= 0 && v < m;
-    if (in_range)
-      for (int s = lane; s < m; s += 32) cs[s] = cols[(size_t)b * m + s];
+    int key[kSlotsPerLane];
+#pragma unroll
+    for (int t = 0; t < kSlotsPerLane; ++t) {  // this lane's slots and their table keys
+      const int k = lane + 32 * t;
+      const int c = in_range && k < m ? (int)cols[(size_t)b * m + k] : 0;
+      if (in_range && k < m) cs[k] = c;
+      key[t] = (k >> 1) * kLutW + c;
+    }
     __syncwarp();
     if (!in_range || !legal_swap(cs, u, v)) {
       if (lane == 0) dE[mv] = N3_SENTINEL;
@@ -191,14 +214,14 @@ __global__ void __launch_bounds__(kDeltaWarps * 32) swap_delta_kernel(const int1
       int local[kSlotsPerLane];
       int du = 0, dv = 0;
       if (dbad) {
-        d = swap_delta_hist<true>(cs, m, u, v, lut, hist, lane, local, &du, &dv);
+        d = swap_delta_hist<true>(cs, key, m, u, v, lut, hist, lane, local, &du, &dv);
 #pragma unroll
         for (int t = 0; t < kSlotsPerLane; ++t) {
           const int k = lane + 32 * t;
           if (k < m) dbad[(size_t)mv * m + k] = k == u ? du : (k == v ? dv : local[t]);
         }
       } else {
-        d = swap_delta_hist<false>(cs, m, u, v, lut, hist, lane, local, &du, &dv);
+        d = swap_delta_hist<false>(cs, key, m, u, v, lut, hist, lane, local, &du, &dv);
       }
     }
     if (lane == 0) dE[mv] = d;
@@ -342,7 +365,7 @@ static int launch_swap(bool pairs, const int16_t* cols, int B, int n, const int3
   if (M == 0) return N3_OK;
   if (moves == nullptr || dE == nullptr) return set_error(N3_ERR_ARG, "null move or output pointer");
   N3_TRY(ensure_device_tables());
-  const uint16_t* lut = dir_lut_device_ptr();
+  const uint16_t* lut = dir_lut_full_device_ptr();
   const int want = (M + n3::kDeltaWarps - 1) / n3::kDeltaWarps;
   const int grid = want < sm_count() * 2 ? want : sm_count() * 2;
   if (pairs) {
