@@ -230,6 +230,71 @@ __global__ void __launch_bounds__(kSlopeWarps * 32) slope_kernel(ColSource src, 
   }
 }
 
+// Slope count only (MODE 0: scores, badness) or slope count checked against
+// the determinant counts already in `scores` (MODE 2), with 4-bit histograms
+// (slope_state4): W = blockDim.x / 32 <= 32 warps share one direction table,
+// a warp per state.  A state that overflows a 4-bit counter is recounted by
+// slope_state_halves in the same shared memory.
+constexpr int kSlope4MaxWarps = 32;
+__host__ __device__ constexpr size_t slope4_smem(int warps) {
+  return kFullLutBytes + (size_t)warps * (sizeof(uint32_t) * kDirWords4 + sizeof(int) * kMaxM * 2);
+}
+
+template <int MODE>
+__global__ void __launch_bounds__(kSlope4MaxWarps * 32, 1) slope4_kernel(ColSource src, int B, int n,
+                                                                          int32_t* __restrict__ scores,
+                                                                          int32_t* __restrict__ badness,
+                                                                          int32_t* __restrict__ mismatch,
+                                                                          uint32_t* __restrict__ error_word) {
+  static_assert(MODE == 0 || MODE == 2, "slope count only, or checked against determinant counts");
+  extern __shared__ __align__(16) unsigned char smem[];
+  const int W = blockDim.x >> 5;
+  uint16_t* lut = reinterpret_cast<uint16_t*>(smem);
+  uint32_t* hist_all = reinterpret_cast<uint32_t*>(smem + kFullLutBytes);
+  int* cs_all = reinterpret_cast<int*>(hist_all + kDirWords4 * W);
+  int* bad_all = cs_all + kMaxM * W;
+  full_lut_copy(lut, g_dir_lut_full);
+  for (int i = threadIdx.x; i < kDirWords4 * W; i += blockDim.x) hist_all[i] = 0u;
+  __syncthreads();
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int m = 2 * n;
+  int* cs = cs_all + warp * kMaxM;
+  int* bad = bad_all + warp * kMaxM;
+  uint32_t* hist = hist_all + warp * kDirWords4;
+  for (int b = blockIdx.x * W + warp; b < B; b += gridDim.x * W) {
+    const uint32_t err = load_checked(src, b, n, cs, lane);
+    if (err) {  // invalid state: no count is meaningful
+      if (lane == 0) {
+        scores[b] = -1;
+        if (error_word) atomicOr(error_word, err);
+        if (MODE != 0) atomicAdd(mismatch, 1);
+      }
+      if (badness)
+        for (int s = lane; s < m; s += 32) badness[(size_t)b * m + s] = -1;
+      __syncwarp();
+      continue;
+    }
+    bool overflow;
+    int total = slope_state4(cs, n, lut, hist, lane, bad, &overflow);
+    if (overflow) {  // uniform
+      __syncwarp();
+      total = slope_state_halves(cs, n, lut, hist, lane, bad);
+    }
+    __syncwarp();
+    if (MODE == 0) {
+      if (lane == 0) scores[b] = total / 3;
+    } else {  // scores[b] holds the determinant count of this state
+      if (lane == 0 && total != 3 * scores[b]) {
+        atomicAdd(mismatch, 1);
+        if (error_word) atomicOr(error_word, kErrMismatch);
+      }
+    }
+    if (badness)
+      for (int s = lane; s < m; s += 32) badness[(size_t)b * m + s] = bad[s];
+    __syncwarp();
+  }
+}
+
 }  // namespace n3
 
 namespace n3host {
@@ -268,8 +333,8 @@ static int check_common(int B, int n, const void* a, const void* out) {
 }
 
 int prepare_score() {
-  N3_TRY(allow_smem(reinterpret_cast<const void*>(n3::slope_kernel<0>), n3::kSlopeSmem));
-  N3_TRY(allow_smem(reinterpret_cast<const void*>(n3::slope_kernel<2>), n3::kSlopeSmem));
+  N3_TRY(allow_smem(reinterpret_cast<const void*>(n3::slope4_kernel<0>), n3::slope4_smem(n3::kSlope4MaxWarps)));
+  N3_TRY(allow_smem(reinterpret_cast<const void*>(n3::slope4_kernel<2>), n3::slope4_smem(n3::kSlope4MaxWarps)));
   N3_TRY(allow_smem(reinterpret_cast<const void*>(n3::slope_kernel<3>), n3::kSlopeSmem));
   return allow_smem(reinterpret_cast<const void*>(n3::slope_kernel<1>), n3::kSlopeSmem);
 }
@@ -298,6 +363,24 @@ static int launch_slope(const int16_t* cols, int B, int n, int32_t* scores, int3
   return check_launch("slope_kernel");
 }
 
+// The 4-bit slope kernel: one CTA per SM of W warps, W = ceil(B / SMs) up to
+// 32, so that 4096 states are one state per warp on 147 SMs.
+template <int MODE>
+static int launch_slope4(const int16_t* cols, int B, int n, int32_t* scores, int32_t* badness, int32_t* mismatch,
+                         uint32_t* error_word, cudaStream_t st) {
+  if (B == 0) return N3_OK;
+  N3_TRY(ensure_device_tables());
+  N3_TRY(allow_smem(reinterpret_cast<const void*>(n3::slope4_kernel<MODE>), n3::slope4_smem(n3::kSlope4MaxWarps)));
+  const int sms = sm_count();
+  int W = (B + sms - 1) / sms;
+  W = W < 1 ? 1 : (W > n3::kSlope4MaxWarps ? n3::kSlope4MaxWarps : W);
+  const int blocks_needed = (B + W - 1) / W;
+  const int grid = blocks_needed < sms ? blocks_needed : sms;
+  n3::slope4_kernel<MODE><<<grid, W * 32, n3::slope4_smem(W), st>>>(n3::ColSource{cols}, B, n, scores, badness,
+                                                                    mismatch, error_word);
+  return check_launch("slope4_kernel");
+}
+
 }  // namespace n3host
 
 extern "C" {
@@ -316,7 +399,7 @@ int n3_score_columns(const int16_t* cols, int B, int n, int32_t* scores, int32_t
 
 int n3_score_slope(const int16_t* cols, int B, int n, int32_t* scores, int32_t* badness, void* stream) {
   N3_TRY(n3host::check_common(B, n, cols, scores));
-  return n3host::launch_slope<0>(cols, B, n, scores, badness, nullptr, nullptr, (cudaStream_t)stream);
+  return n3host::launch_slope4<0>(cols, B, n, scores, badness, nullptr, nullptr, (cudaStream_t)stream);
 }
 
 int n3_score_checked(const int16_t* cols, int B, int n, int32_t* scores, int32_t* badness, int32_t* mismatch,
@@ -329,7 +412,8 @@ int n3_score_checked(const int16_t* cols, int B, int n, int32_t* scores, int32_t
   // own badness output costs it 70 % more time than the whole slope pass);
   // without, the forward slope count checks E at 3/4 of the cost.
   N3_TRY(n3host::launch_det(n3::ColSource{cols}, B, n, scores, nullptr, (cudaStream_t)stream));
-  if (badness) return n3host::launch_slope<2>(cols, B, n, scores, badness, mismatch, error_word, (cudaStream_t)stream);
+  if (badness)
+    return n3host::launch_slope4<2>(cols, B, n, scores, badness, mismatch, error_word, (cudaStream_t)stream);
   return n3host::launch_slope<3>(cols, B, n, scores, nullptr, mismatch, error_word, (cudaStream_t)stream);
 }
 

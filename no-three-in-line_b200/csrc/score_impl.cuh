@@ -137,6 +137,99 @@ __device__ __forceinline__ int slope_state(const int* __restrict__ cs, int n, co
   return total;
 }
 
+// The slope count with 4-bit counters (8 per word, kDirWords4 words per
+// warp): the same insertions and sums as slope_state in half the shared
+// memory, so twice the warps fit beside one direction table.  A counter that
+// would reach 16 (16 points other than the anchor on one line through it; no
+// random state comes near) sets *overflow and leaves this state's counts
+// meaningless; every touched word is still cleared, so the histogram is zero on
+// return.  The caller then recounts the state with slope_state_halves.
+constexpr int kDirWords4 = kDirCount / 8;  // 848
+__device__ __forceinline__ int slope_state4(const int* __restrict__ cs, int n, const uint16_t* __restrict__ lutf,
+                                            uint32_t* __restrict__ hist, int lane, int* __restrict__ bad_out,
+                                            bool* overflow) {
+  constexpr int kT = (kMaxM + 31) / 32;
+  const int m = 2 * n;
+  int key[kT], row[kT];
+#pragma unroll
+  for (int t = 0; t < kT; ++t) {
+    const int b = lane + 32 * t;
+    row[t] = b < m ? b >> 1 : -1;
+    key[t] = b < m ? (b >> 1) * kLutW + cs[b] : 0;
+  }
+  int total = 0;
+  bool ovf = false;
+  for (int a = 0; a < m; ++a) {
+    const int ra = a >> 1;
+    const uint16_t* base = lutf + kFullLutCentre - (ra * kLutW + cs[a]);
+    int pairs = 0;
+    int ids[kT];
+#pragma unroll
+    for (int t = 0; t < kT; ++t) {
+      ids[t] = -1;
+      if (row[t] >= 0 && row[t] != ra) {  // the row partner has the lone direction (0,1)
+        const int id = base[key[t]];
+        ids[t] = id;
+        const int sh = (id & 7) << 2;
+        const int before = (int)((atomicAdd(hist + (id >> 3), 1u << sh) >> sh) & 0xFu);
+        ovf |= before == 15;
+        pairs += before;
+      }
+    }
+    __syncwarp();
+#pragma unroll
+    for (int t = 0; t < kT; ++t)
+      if (ids[t] >= 0) hist[ids[t] >> 3] = 0u;
+    __syncwarp();
+    pairs = warp_sum(pairs);
+    if (bad_out != nullptr && lane == (a & 31)) bad_out[a] = pairs;
+    total += pairs;
+  }
+  *overflow = __any_sync(0xffffffffu, ovf);
+  return total;
+}
+
+// The exact slope count in the 4-bit histogram's space (kDirWords4 words):
+// 8-bit counters for the direction ids of each half, [0, kDirCount / 2) then
+// [kDirCount / 2, kDirCount), one pass per half.  Same results as slope_state.
+static __device__ __noinline__ int slope_state_halves(const int* __restrict__ cs, int n, const uint16_t* __restrict__ lutf,
+                                               uint32_t* __restrict__ hist, int lane, int* __restrict__ bad_out) {
+  constexpr int kT = (kMaxM + 31) / 32;
+  constexpr int kHalf = kDirCount / 2;
+  static_assert(kHalf == 4 * kDirWords4, "one half of the ids fills the 4-bit histogram as 8-bit counters");
+  const int m = 2 * n;
+  int total = 0;
+  for (int a = 0; a < m; ++a) {
+    const int ra = a >> 1;
+    const uint16_t* base = lutf + kFullLutCentre - (ra * kLutW + cs[a]);
+    int ids[kT];
+#pragma unroll
+    for (int t = 0; t < kT; ++t) {
+      const int b = lane + 32 * t;
+      ids[t] = (b < m && (b >> 1) != ra) ? (int)base[(b >> 1) * kLutW + cs[b]] : -1;
+    }
+    int pairs = 0;
+    for (int h = 0; h < 2; ++h) {
+#pragma unroll
+      for (int t = 0; t < kT; ++t) {
+        const int local = ids[t] - h * kHalf;
+        if (ids[t] >= 0 && local >= 0 && local < kHalf) pairs += hist_add(hist, local);
+      }
+      __syncwarp();
+#pragma unroll
+      for (int t = 0; t < kT; ++t) {
+        const int local = ids[t] - h * kHalf;
+        if (ids[t] >= 0 && local >= 0 && local < kHalf) hist_clear(hist, local);
+      }
+      __syncwarp();
+    }
+    pairs = warp_sum(pairs);
+    if (bad_out != nullptr && lane == (a & 31)) bad_out[a] = pairs;
+    total += pairs;
+  }
+  return total;
+}
+
 // Forward slope count of one state: for each anchor a, only the slots b > a are
 // binned by direction.  On a line holding slots p1 < .. < pk, anchor p_i sees the
 // k - i later ones, C(k - i, 2) pairs, and the sum over i is C(k, 3): the sum over

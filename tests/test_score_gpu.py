@@ -81,6 +81,32 @@ def test_degenerate_dense_collinear_states(oracle, cuda):
     assert np.array_equal(fwd.scores, ref_s) and fwd.mismatches == 0
 
 
+def test_long_lines_mixed_into_a_population(oracle, cuda):
+    """States with 16 or more points on one line through a point (the slope
+    count's 4-bit counters overflow and the state is recounted with 8-bit
+    counters over each half of the directions) spread through a batch of random
+    states, so that warps of one CTA take both paths."""
+    n = 75
+    pr, qr = state.seeded_population(n, 600)
+    r = np.arange(n)
+    dense_p = np.stack([r, r, (2 * r) % n, r, (r + 7) % n]).astype(np.int32)
+    dense_q = np.stack([(r + 1) % n, (r + 37) % n, (2 * r + 1) % n, (n - 1 - r + (r == (n - 1) // 2)) % n,
+                        (r + 8) % n]).astype(np.int32)
+    keep = [k for k in range(len(dense_p)) if np.all(dense_p[k] != dense_q[k])
+            and len(set(dense_q[k].tolist())) == n]
+    p, q = pr.copy(), qr.copy()
+    slots = [3, 97, 250, 251, 599][:len(keep)]
+    for slot, k in zip(slots, keep):
+        p[slot], q[slot] = dense_p[k], dense_q[k]
+    ref_s, ref_b = oracle.score_population(p, q, badness=True, threads=0)
+    cols = state.pq_to_columns(p, q)
+    s2, b2 = gpu.score_slope_gpu(cols)
+    assert np.array_equal(s2, ref_s) and np.array_equal(b2, ref_b)
+    chk = gpu.score_checked_gpu(cols)
+    assert np.array_equal(chk.scores, ref_s) and np.array_equal(chk.badness, ref_b) and chk.mismatches == 0
+    assert max(ref_s[slot] for slot in slots) > 10000  # a line of 74 or 75 points is among them
+
+
 def test_empty_batch_and_shape_errors(cuda):
     z = np.zeros((0, 10), np.int32)
     assert gpu.score_population_gpu(z, z).shape == (0,)
