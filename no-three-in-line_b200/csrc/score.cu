@@ -237,7 +237,7 @@ __global__ void __launch_bounds__(kSlopeWarps * 32) slope_kernel(ColSource src, 
 // slope_state_halves in the same shared memory.
 constexpr int kSlope4MaxWarps = 32;
 __host__ __device__ constexpr size_t slope4_smem(int warps) {
-  return kFullLutBytes + (size_t)warps * (sizeof(uint32_t) * kDirWords4 + sizeof(int) * kMaxM * 2);
+  return kFullLutBytes + (size_t)warps * (sizeof(uint32_t) * kHist4Words + sizeof(int) * kMaxM * 2);
 }
 
 template <int MODE>
@@ -251,16 +251,18 @@ __global__ void __launch_bounds__(kSlope4MaxWarps * 32, 1) slope4_kernel(ColSour
   const int W = blockDim.x >> 5;
   uint16_t* lut = reinterpret_cast<uint16_t*>(smem);
   uint32_t* hist_all = reinterpret_cast<uint32_t*>(smem + kFullLutBytes);
-  int* cs_all = reinterpret_cast<int*>(hist_all + kDirWords4 * W);
+  int* cs_all = reinterpret_cast<int*>(hist_all + kHist4Words * W);
   int* bad_all = cs_all + kMaxM * W;
   full_lut_copy(lut, g_dir_lut_full);
-  for (int i = threadIdx.x; i < kDirWords4 * W; i += blockDim.x) hist_all[i] = 0u;
+  for (int i = threadIdx.x; i < kHist4Words * W; i += blockDim.x) hist_all[i] = 0u;
+  __syncthreads();
+  if (threadIdx.x == 0) lut[kFullLutCentre] = (uint16_t)kDirCount;  // (0, 0): the centre's own counter
   __syncthreads();
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int m = 2 * n;
   int* cs = cs_all + warp * kMaxM;
   int* bad = bad_all + warp * kMaxM;
-  uint32_t* hist = hist_all + warp * kDirWords4;
+  uint32_t* hist = hist_all + warp * kHist4Words;
   for (int b = blockIdx.x * W + warp; b < B; b += gridDim.x * W) {
     const uint32_t err = load_checked(src, b, n, cs, lane);
     if (err) {  // invalid state: no count is meaningful

@@ -137,43 +137,44 @@ __device__ __forceinline__ int slope_state(const int* __restrict__ cs, int n, co
   return total;
 }
 
-// The slope count with 4-bit counters (8 per word, kDirWords4 words per
-// warp): the same insertions and sums as slope_state in half the shared
-// memory, so twice the warps fit beside one direction table.  A counter that
-// would reach 16 (16 points other than the anchor on one line through it; no
-// random state comes near) sets *overflow and leaves this state's counts
-// meaningless; every touched word is still cleared, so the histogram is zero on
-// return.  The caller then recounts the state with slope_state_halves.
-constexpr int kDirWords4 = kDirCount / 8;  // 848
+// The slope count with 4-bit counters (8 per word, kHist4Words words per
+// warp): the same pair sums as slope_state in half the shared memory, so twice
+// the warps fit beside one direction table.  lutf is the caller's copy of the
+// full table with the entry of (0, 0) set to kDirCount, a counter of its own
+// (the last word): every slot of the state is inserted, the centre itself into
+// that counter (adding 0, once) and its row partner into the (0, 1) class,
+// where it is alone (adding 0), so no insertion tests its row.  A counter that
+// reaches 16 wraps; by then its direction has added 0 + 1 + ... + 15 = 120
+// pairs to the centre's sum, so *overflow is set for every centre whose sum
+// reaches 120, and the caller recounts the state with slope_state_halves.
+// Every touched word is cleared, so the histogram is zero on return.
+constexpr int kDirWords4 = kDirCount / 8;     // 848
+constexpr int kHist4Words = kDirWords4 + 1;   // + the word of the centre's own counter
 __device__ __forceinline__ int slope_state4(const int* __restrict__ cs, int n, const uint16_t* __restrict__ lutf,
                                             uint32_t* __restrict__ hist, int lane, int* __restrict__ bad_out,
                                             bool* overflow) {
   constexpr int kT = (kMaxM + 31) / 32;
   const int m = 2 * n;
-  int key[kT], row[kT];
+  int key[kT];
 #pragma unroll
   for (int t = 0; t < kT; ++t) {
     const int b = lane + 32 * t;
-    row[t] = b < m ? b >> 1 : -1;
-    key[t] = b < m ? (b >> 1) * kLutW + cs[b] : 0;
+    key[t] = b < m ? (b >> 1) * kLutW + cs[b] : -1;
   }
   int total = 0;
   bool ovf = false;
   for (int a = 0; a < m; ++a) {
-    const int ra = a >> 1;
-    const uint16_t* base = lutf + kFullLutCentre - (ra * kLutW + cs[a]);
+    const uint16_t* base = lutf + kFullLutCentre - ((a >> 1) * kLutW + cs[a]);
     int pairs = 0;
     int ids[kT];
 #pragma unroll
     for (int t = 0; t < kT; ++t) {
       ids[t] = -1;
-      if (row[t] >= 0 && row[t] != ra) {  // the row partner has the lone direction (0,1)
+      if (key[t] >= 0) {
         const int id = base[key[t]];
         ids[t] = id;
         const int sh = (id & 7) << 2;
-        const int before = (int)((atomicAdd(hist + (id >> 3), 1u << sh) >> sh) & 0xFu);
-        ovf |= before == 15;
-        pairs += before;
+        pairs += (int)((atomicAdd(hist + (id >> 3), 1u << sh) >> sh) & 0xFu);
       }
     }
     __syncwarp();
@@ -182,10 +183,11 @@ __device__ __forceinline__ int slope_state4(const int* __restrict__ cs, int n, c
       if (ids[t] >= 0) hist[ids[t] >> 3] = 0u;
     __syncwarp();
     pairs = warp_sum(pairs);
+    ovf |= pairs >= 120;
     if (bad_out != nullptr && lane == (a & 31)) bad_out[a] = pairs;
     total += pairs;
   }
-  *overflow = __any_sync(0xffffffffu, ovf);
+  *overflow = ovf;  // uniform: from warp sums
   return total;
 }
 
