@@ -132,10 +132,6 @@ __global__ void __launch_bounds__(kDetWarps * 32) det_kernel(Src src, int B, int
   }
 }
 
-constexpr int kSlopeWarps = 8;  // 8 chains share one copy of the direction table per CTA
-constexpr size_t kSlopeSmem = kFullLutBytes + sizeof(uint32_t) * kDirWords * kSlopeWarps +
-                              sizeof(int) * kMaxM * kSlopeWarps * 2 + 64;
-
 // Loads one state, validating columns (range, row duplicates).  Returns the
 // device error bits for this state (warp-uniform).
 template <class Src>
@@ -154,87 +150,15 @@ __device__ __forceinline__ uint32_t load_checked(const Src& src, int b, int n, i
   return err;
 }
 
-// MODE 0: slope only (scores, badness).  MODE 1: determinant + slope, checked,
-// in this kernel.  MODE 2: slope + check against determinant counts already in
-// `scores` (written by det_kernel on the same stream).  MODE 3: forward slope
-// count of E only (slope_forward_state), compared with the determinant count in
-// `scores` (and, if `badness` is given, that badness checked to sum to 3E).
-template <int MODE>
-__global__ void __launch_bounds__(kSlopeWarps * 32) slope_kernel(ColSource src, int B, int n,
-                                                                   int32_t* __restrict__ scores,
-                                                                   int32_t* __restrict__ badness,
-                                                                   int32_t* __restrict__ mismatch,
-                                                                   uint32_t* __restrict__ error_word) {
-  extern __shared__ __align__(16) unsigned char smem[];
-  uint16_t* lut = reinterpret_cast<uint16_t*>(smem);
-  uint32_t* hist_all = reinterpret_cast<uint32_t*>(smem + kFullLutBytes);
-  int* cs_all = reinterpret_cast<int*>(hist_all + kDirWords * kSlopeWarps);
-  int* bad_all = cs_all + kMaxM * kSlopeWarps;
-  full_lut_copy(lut, g_dir_lut_full);
-  for (int i = threadIdx.x; i < kDirWords * kSlopeWarps; i += blockDim.x) hist_all[i] = 0u;
-  __syncthreads();
-  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const int m = 2 * n;
-  int* cs = cs_all + warp * kMaxM;
-  int* bad = bad_all + warp * kMaxM;
-  uint32_t* hist = hist_all + warp * kDirWords;
-  for (int b = blockIdx.x * kSlopeWarps + warp; b < B; b += gridDim.x * kSlopeWarps) {
-    const uint32_t err = load_checked(src, b, n, cs, lane);
-    if (err) {  // invalid state: no count is meaningful
-      if (lane == 0) {
-        scores[b] = -1;
-        if (error_word) atomicOr(error_word, err);
-        if (MODE != 0) atomicAdd(mismatch, 1);
-      }
-      if (badness)
-        for (int s = lane; s < m; s += 32) badness[(size_t)b * m + s] = -1;
-      __syncwarp();
-      continue;
-    }
-    if (MODE == 3) {
-      const int e_slope = warp_sum(slope_forward_state(cs, n, lut, hist, lane));
-      int bad_sum = 0;
-      if (badness)
-        for (int s = lane; s < m; s += 32) bad_sum += badness[(size_t)b * m + s];
-      bad_sum = warp_sum(bad_sum);
-      const int e_det = scores[b];
-      if (lane == 0 && (e_slope != e_det || (badness && bad_sum != 3 * e_det))) {
-        atomicAdd(mismatch, 1);
-        if (error_word) atomicOr(error_word, kErrMismatch);
-      }
-      __syncwarp();
-      continue;
-    }
-    const int total = slope_state(cs, n, lut, hist, lane, bad);
-    __syncwarp();
-    if (MODE == 0) {
-      if (lane == 0) scores[b] = total / 3;
-    } else if (MODE == 2) {  // scores[b] holds the determinant count of this state
-      if (lane == 0 && total != 3 * scores[b]) {
-        atomicAdd(mismatch, 1);
-        if (error_word) atomicOr(error_word, kErrMismatch);
-      }
-    } else {
-      const int e_det = warp_sum(det_state<false>(cs, n, lane, nullptr));
-      if (lane == 0) {
-        scores[b] = e_det;
-        if (total != 3 * e_det) {
-          atomicAdd(mismatch, 1);
-          if (error_word) atomicOr(error_word, kErrMismatch);
-        }
-      }
-    }
-    if (badness)
-      for (int s = lane; s < m; s += 32) badness[(size_t)b * m + s] = bad[s];
-    __syncwarp();
-  }
-}
-
-// Slope count only (MODE 0: scores, badness) or slope count checked against
-// the determinant counts already in `scores` (MODE 2), with 4-bit histograms
-// (slope_state4): W = blockDim.x / 32 <= 32 warps share one direction table,
-// a warp per state.  A state that overflows a 4-bit counter is recounted by
-// slope_state_halves in the same shared memory.
+// The slope count of every state with 4-bit histograms: W = blockDim.x / 32
+// <= 32 warps share one direction table, a warp per state, each state loaded
+// and validated (column range, row duplicates).  MODE 0: slope count only
+// (scores, badness).  MODE 2: slope count and badness, checked against the
+// determinant counts already in `scores` (written by det_kernel on the same
+// stream).  MODE 3: the forward slope count of E only (slope_forward_state4),
+// checked the same way (and, if `badness` is given, that badness checked to
+// sum to 3E).  A state that may have overflowed a 4-bit counter is recounted
+// by slope_state_halves in the same shared memory.
 constexpr int kSlope4MaxWarps = 32;
 __host__ __device__ constexpr size_t slope4_smem(int warps) {
   return kFullLutBytes + (size_t)warps * (sizeof(uint32_t) * kHist4Words + sizeof(int) * kMaxM * 2);
@@ -246,7 +170,7 @@ __global__ void __launch_bounds__(kSlope4MaxWarps * 32, 1) slope4_kernel(ColSour
                                                                           int32_t* __restrict__ badness,
                                                                           int32_t* __restrict__ mismatch,
                                                                           uint32_t* __restrict__ error_word) {
-  static_assert(MODE == 0 || MODE == 2, "slope count only, or checked against determinant counts");
+  static_assert(MODE == 0 || MODE == 2 || MODE == 3, "slope count only, or checked against determinant counts");
   extern __shared__ __align__(16) unsigned char smem[];
   const int W = blockDim.x >> 5;
   uint16_t* lut = reinterpret_cast<uint16_t*>(smem);
@@ -277,6 +201,24 @@ __global__ void __launch_bounds__(kSlope4MaxWarps * 32, 1) slope4_kernel(ColSour
       continue;
     }
     bool overflow;
+    if (MODE == 3) {  // forward count of E, compared with the determinant count (and badness, if given)
+      int e_slope = slope_forward_state4(cs, n, lut, hist, lane, &overflow);
+      if (overflow) {  // uniform
+        __syncwarp();
+        e_slope = slope_state_halves(cs, n, lut, hist, lane, nullptr) / 3;
+      }
+      int bad_sum = 0;
+      if (badness)
+        for (int s = lane; s < m; s += 32) bad_sum += badness[(size_t)b * m + s];
+      bad_sum = warp_sum(bad_sum);
+      const int e_det = scores[b];
+      if (lane == 0 && (e_slope != e_det || (badness && bad_sum != 3 * e_det))) {
+        atomicAdd(mismatch, 1);
+        if (error_word) atomicOr(error_word, kErrMismatch);
+      }
+      __syncwarp();
+      continue;
+    }
     int total = slope_state4(cs, n, lut, hist, lane, bad, &overflow);
     if (overflow) {  // uniform
       __syncwarp();
@@ -337,8 +279,7 @@ static int check_common(int B, int n, const void* a, const void* out) {
 int prepare_score() {
   N3_TRY(allow_smem(reinterpret_cast<const void*>(n3::slope4_kernel<0>), n3::slope4_smem(n3::kSlope4MaxWarps)));
   N3_TRY(allow_smem(reinterpret_cast<const void*>(n3::slope4_kernel<2>), n3::slope4_smem(n3::kSlope4MaxWarps)));
-  N3_TRY(allow_smem(reinterpret_cast<const void*>(n3::slope_kernel<3>), n3::kSlopeSmem));
-  return allow_smem(reinterpret_cast<const void*>(n3::slope_kernel<1>), n3::kSlopeSmem);
+  return allow_smem(reinterpret_cast<const void*>(n3::slope4_kernel<3>), n3::slope4_smem(n3::kSlope4MaxWarps));
 }
 
 template <class Src>
@@ -350,19 +291,6 @@ static int launch_det(Src src, int B, int n, int32_t* scores, int32_t* badness, 
   else
     n3::det_kernel<Src, false><<<grid, n3::kDetWarps * 32, 0, st>>>(src, B, n, scores, nullptr);
   return check_launch("det_kernel");
-}
-
-template <int MODE>
-static int launch_slope(const int16_t* cols, int B, int n, int32_t* scores, int32_t* badness, int32_t* mismatch,
-                        uint32_t* error_word, cudaStream_t st) {
-  if (B == 0) return N3_OK;
-  N3_TRY(ensure_device_tables());
-  N3_TRY(allow_smem(reinterpret_cast<const void*>(n3::slope_kernel<MODE>), n3::kSlopeSmem));
-  const int blocks_needed = (B + n3::kSlopeWarps - 1) / n3::kSlopeWarps;
-  const int grid = blocks_needed < sm_count() * 2 ? blocks_needed : sm_count() * 2;  // 2 CTAs fit per SM
-  n3::slope_kernel<MODE><<<grid, n3::kSlopeWarps * 32, n3::kSlopeSmem, st>>>(n3::ColSource{cols}, B, n, scores,
-                                                                             badness, mismatch, error_word);
-  return check_launch("slope_kernel");
 }
 
 // The 4-bit slope kernel: one CTA per SM of W warps, W = ceil(B / SMs) up to
@@ -416,7 +344,7 @@ int n3_score_checked(const int16_t* cols, int B, int n, int32_t* scores, int32_t
   N3_TRY(n3host::launch_det(n3::ColSource{cols}, B, n, scores, nullptr, (cudaStream_t)stream));
   if (badness)
     return n3host::launch_slope4<2>(cols, B, n, scores, badness, mismatch, error_word, (cudaStream_t)stream);
-  return n3host::launch_slope<3>(cols, B, n, scores, nullptr, mismatch, error_word, (cudaStream_t)stream);
+  return n3host::launch_slope4<3>(cols, B, n, scores, nullptr, mismatch, error_word, (cudaStream_t)stream);
 }
 
 }  // extern "C"

@@ -191,6 +191,50 @@ __device__ __forceinline__ int slope_state4(const int* __restrict__ cs, int n, c
   return total;
 }
 
+// The forward slope count (from each centre a only the slots b > a, so every
+// collinear triple is counted once, from its first slot) with 4-bit counters,
+// as slope_state4; returns E for the whole warp.  A centre whose forward pair
+// sum reaches 120 sets *overflow (see slope_state4).
+__device__ __forceinline__ int slope_forward_state4(const int* __restrict__ cs, int n,
+                                                    const uint16_t* __restrict__ lutf, uint32_t* __restrict__ hist,
+                                                    int lane, bool* overflow) {
+  constexpr int kT = (kMaxM + 31) / 32;
+  const int m = 2 * n;
+  int key[kT];
+#pragma unroll
+  for (int t = 0; t < kT; ++t) {
+    const int b = lane + 32 * t;
+    key[t] = b < m ? (b >> 1) * kLutW + cs[b] : -1;
+  }
+  int total = 0;
+  bool ovf = false;
+  for (int a = 0; a < m - 2; ++a) {
+    const uint16_t* base = lutf + kFullLutCentre - ((a >> 1) * kLutW + cs[a]);
+    int pairs = 0;
+    int ids[kT];
+#pragma unroll
+    for (int t = 0; t < kT; ++t) {
+      ids[t] = -1;
+      if (key[t] >= 0 && lane + 32 * t > a) {  // the row partner is alone in its direction
+        const int id = base[key[t]];
+        ids[t] = id;
+        const int sh = (id & 7) << 2;
+        pairs += (int)((atomicAdd(hist + (id >> 3), 1u << sh) >> sh) & 0xFu);
+      }
+    }
+    __syncwarp();
+#pragma unroll
+    for (int t = 0; t < kT; ++t)
+      if (ids[t] >= 0) hist[ids[t] >> 3] = 0u;
+    __syncwarp();
+    pairs = warp_sum(pairs);
+    ovf |= pairs >= 120;
+    total += pairs;
+  }
+  *overflow = ovf;
+  return total;
+}
+
 // The exact slope count in the 4-bit histogram's space (kDirWords4 words):
 // 8-bit counters for the direction ids of each half, [0, kDirCount / 2) then
 // [kDirCount / 2, kDirCount), one pass per half.  Same results as slope_state.
@@ -232,46 +276,5 @@ static __device__ __noinline__ int slope_state_halves(const int* __restrict__ cs
   return total;
 }
 
-// Forward slope count of one state: for each anchor a, only the slots b > a are
-// binned by direction.  On a line holding slots p1 < .. < pk, anchor p_i sees the
-// k - i later ones, C(k - i, 2) pairs, and the sum over i is C(k, 3): the sum over
-// anchors is E itself, from half the insertions of slope_state (no per-slot
-// badness).  Returns this lane's share; hist is left zeroed.
-__device__ __forceinline__ int slope_forward_state(const int* __restrict__ cs, int n,
-                                                   const uint16_t* __restrict__ lutf,
-                                                   uint32_t* __restrict__ hist, int lane) {
-  constexpr int kT = (kMaxM + 31) / 32;
-  const int m = 2 * n;
-  int key[kT], row[kT];
-#pragma unroll
-  for (int t = 0; t < kT; ++t) {
-    const int b = lane + 32 * t;
-    row[t] = b < m ? b >> 1 : -1;
-    key[t] = b < m ? (b >> 1) * kLutW + cs[b] : 0;
-  }
-  int pairs = 0;
-  for (int a = 0; a < m - 2; ++a) {
-    const int ra = a >> 1;
-    const uint16_t* base = lutf + kFullLutCentre - (ra * kLutW + cs[a]);
-    int ids[kT];
-#pragma unroll
-    for (int t = 0; t < kT; ++t) {
-      ids[t] = -1;
-      if (32 * t + 31 <= a) continue;  // warp-uniform: every slot of this group precedes a
-      const int b = lane + 32 * t;
-      if (b > a && row[t] >= 0 && row[t] != ra) {
-        const int id = base[key[t]];
-        ids[t] = id;
-        pairs += hist_add(hist, id);
-      }
-    }
-    __syncwarp();
-#pragma unroll
-    for (int t = 0; t < kT; ++t)
-      if (ids[t] >= 0) hist_clear(hist, ids[t]);
-    __syncwarp();
-  }
-  return pairs;
-}
 
 }  // namespace n3
