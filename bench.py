@@ -770,19 +770,24 @@ def run_b200(args):
 
     # end to end through the C ABI with host buffers: every step copies its
     # population from pinned host memory and reads its scores and flags back.
-    # The copy of step k + 1 runs on a second stream, into the other of two
-    # device buffers, while step k computes (a copy waits until the compute
-    # that last used its buffer is done).
+    # The copies run on a second stream beside the compute: the population of
+    # step k + 1 into the other of two device buffers while step k computes (a
+    # copy waits until the compute that last used its buffer is done), and the
+    # read-back of step k's scores and flags (two result buffers, so that step
+    # k + 1 writes the other) while step k + 1 computes.
     h_cols = torch.from_numpy(cols_host).pin_memory()
     h_scores = torch.empty(B, dtype=torch.int32).pin_memory()
     h_flags = torch.empty(2, dtype=torch.int32).pin_memory()
     d_bufs = [torch.empty_like(cols), torch.empty_like(cols)]
+    r_scores = [scores, torch.empty_like(scores)]
+    r_flags = [flags, torch.zeros_like(flags)]
     copy_stream = torch.cuda.Stream(device=dev)
     e2e_steps = max(3, min(args.steps, 100))
 
     def e2e_run(steps):
         ready = [torch.cuda.Event(), torch.cuda.Event()]
-        free = [torch.cuda.Event(), torch.cuda.Event()]
+        free = [torch.cuda.Event(), torch.cuda.Event()]    # step done with its input buffer and result buffers
+        read = [torch.cuda.Event(), torch.cuda.Event()]    # result buffers copied to the host
         copy_stream.wait_stream(stream)
         with torch.cuda.stream(copy_stream):
             d_bufs[0].copy_(h_cols, non_blocking=True)
@@ -796,11 +801,18 @@ def run_b200(args):
                     d_bufs[1 - b].copy_(h_cols, non_blocking=True)
                     ready[1 - b].record(copy_stream)
             stream.wait_event(ready[b])
-            _lib.check(L.n3_score_checked(d_bufs[b].data_ptr(), B, N, scores.data_ptr(), badness.data_ptr(),
-                                          flags.data_ptr(), flags.data_ptr() + 4, sptr), "n3_score_checked")
+            if k >= 2:
+                stream.wait_event(read[b])
+            _lib.check(L.n3_score_checked(d_bufs[b].data_ptr(), B, N, r_scores[b].data_ptr(), badness.data_ptr(),
+                                          r_flags[b].data_ptr(), r_flags[b].data_ptr() + 4, sptr),
+                       "n3_score_checked")
             free[b].record(stream)
-            h_scores.copy_(scores, non_blocking=True)
-            h_flags.copy_(flags, non_blocking=True)
+            with torch.cuda.stream(copy_stream):
+                copy_stream.wait_event(free[b])
+                h_scores.copy_(r_scores[b], non_blocking=True)
+                h_flags.copy_(r_flags[b], non_blocking=True)
+                read[b].record(copy_stream)
+        stream.wait_stream(copy_stream)  # the last read-back is inside the timed region
 
     e2e_run(2)
     torch.cuda.synchronize()
@@ -810,7 +822,7 @@ def run_b200(args):
     e_end.record(stream)
     torch.cuda.synchronize()
     e2e_ms = e_start.elapsed_time(e_end) / e2e_steps
-    if not np.array_equal(h_scores[:64].numpy(), ref):
+    if not np.array_equal(h_scores[:64].numpy(), ref) or int(r_flags[0][0].item()) or int(r_flags[1][0].item()):
         raise AssertionError("end-to-end scores differ from the oracle")
     t_e2e = torch.tensor([e2e_ms], dtype=torch.float64, device=dev)
     if world > 1:
@@ -876,7 +888,7 @@ def run_b200(args):
             "e2e": {"value": world * B / (e2e_ms / 1e3), "unit": UNIT,
                     "h2d_bytes_per_step": int(cols_host.nbytes),
                     "d2h_bytes_per_step": int(h_scores.numel() * 4 + h_flags.numel() * 4),
-                    "copies": "pinned host buffers; H2D of step k+1 on a second stream beside step k"},
+                    "copies": "pinned host buffers; H2D of step k+1 and read-back of step k on a second stream beside the compute"},
             "gpu_launches": args.steps * (2 if args.mode == "checked" else 1),
             "roofline": {"bound": "int32 pipes (FMA pipe for products, ALU pipe for compares)",
                          "kernel": "n3::det_kernel<ColSource,false> (the larger of the checked step's two "
