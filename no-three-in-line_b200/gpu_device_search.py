@@ -94,8 +94,15 @@ def elite_key(score: int, badness: np.ndarray) -> tuple[int, int, int]:
 
 
 def rank_elites(scores: np.ndarray, badness: np.ndarray) -> np.ndarray:
-    """gpu_device_search.py:185-197: stable order by (E, max badness, sum of squared badness)."""
-    return np.asarray(sorted(range(len(scores)), key=lambda i: elite_key(scores[i], badness[i])), dtype=np.int32)
+    """gpu_device_search.py:185-197: stable order by (E, max badness, sum of
+    squared badness), ties in index order.  The three keys of every row are
+    formed at once (int64) and ordered by one stable lexicographic sort, the
+    same order as the reference's Python sort by elite_key."""
+    scores = np.asarray(scores).astype(np.int64).reshape(-1)
+    if len(scores) == 0:
+        return np.zeros(0, dtype=np.int32)
+    values = np.asarray(badness).astype(np.int64).reshape(len(scores), -1)
+    return np.lexsort((np.einsum("ij,ij->i", values, values), values.max(axis=1), scores)).astype(np.int32)
 
 
 def mutate_population_device(parent_p, parent_q, *, population: int, active_strength: int, max_strength: int,

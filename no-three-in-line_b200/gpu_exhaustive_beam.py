@@ -71,6 +71,15 @@ def _signature(p: np.ndarray, q: np.ndarray) -> bytes:
     return values.astype(np.int16, copy=False).tobytes()
 
 
+def _signatures(p: np.ndarray, q: np.ndarray) -> list[bytes]:
+    """_signature of every row pair (p[k], q[k]), the rows sorted all at once."""
+    p, q = np.asarray(p), np.asarray(q)
+    values = np.stack((np.minimum(p, q), np.maximum(p, q)), axis=2)  # each row's pair sorted
+    width = values.shape[1] * 4  # bytes of one row's int16 signature
+    whole = values.astype(np.int16).tobytes()
+    return [whole[k * width:(k + 1) * width] for k in range(len(values))]
+
+
 class _Buffers:
     """Device buffers of one search, sized for elite_size + 1 elites (the
     reference's retention can keep one elite more than elite_size when
@@ -206,7 +215,7 @@ def gpu_exhaustive_beam_search(
         pp = buf.pp[:prospects].cpu().numpy()
         pq = buf.pq[:prospects].cpu().numpy()
         p_pos = buf.p_pos[:prospects].cpu().numpy()
-        sigs = [_signature(pp[k], pq[k]) for k in range(prospects)]
+        sigs = _signatures(pp, pq)
         ranked = [int(k) for k in rank_elites(p_score, p_bad)]
         diverse_order = [int(k) for k in np.argsort(np.where(p_pos >= 0, p_pos, np.iinfo(np.int32).max),
                                                     kind="stable")[:int(np.count_nonzero(p_pos >= 0))]]
