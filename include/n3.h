@@ -415,6 +415,15 @@ int n3_beam_mutate(const int32_t* parent_p, const int32_t* parent_q, const int32
                    int max_strength, int bad_bias, uint64_t seed, int generation, int32_t* child_p,
                    int32_t* child_q, void* stream);
 
+/* Canonical P/Q of B row/column 2-factors given as raw rows p[b][r], q[b][r]
+ * (host pointers, int32 [B][n]; the two columns of each row in either order):
+ * P is the perfect matching that augmenting paths find with the rows in order
+ * and each row's columns ascending, Q the other column of each row.  Host code,
+ * no GPU.  N3_ERR_ARG if a state is not a 2-factor.
+ * Replaces: state.points_to_permutations (src/no_three_75/state.py:47-85) as the
+ * beam searches use it on raw rows (gpu_device_search.py:178-182). */
+int n3_normalize_pairs(const int32_t* p, const int32_t* q, int B, int n, int32_t* p_out, int32_t* q_out);
+
 /* Python's random.Random(seed) (MT19937 seeded by init_by_array over the 32-bit
  * words of |seed|), used by the reference for its diversity shuffle
  * (gpu_device_search.py:280, 343).  state: device uint32[625] (624 words and

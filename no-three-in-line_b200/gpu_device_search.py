@@ -29,7 +29,7 @@ from typing import Callable
 import numpy as np
 
 from . import _lib
-from .state import PairPermutations, points_to_permutations
+from .state import PairPermutations
 
 _P = ctypes.c_void_p
 _I = ctypes.c_int
@@ -52,6 +52,7 @@ _lib.register("n3_beam_mutate", [_P, _P, _P] + [_I] * 7 + [ctypes.c_uint64, _I, 
 _lib.register("n3_py_random_seed", [_P, ctypes.c_uint64, _P])
 _lib.register("n3_py_random_shuffle", [_P, _P, _I, _P])
 _lib.register("n3_py_shuffle_steps", [_P, _I, _P, _P])
+_lib.register("n3_normalize_pairs", [_P, _P, _I, _I, _P, _P])
 _lib.register("n3_beam_init", [ctypes.POINTER(BeamDesc), _I, _P])
 _lib.register("n3_beam_generation", [ctypes.POINTER(BeamDesc), _I, _P])
 
@@ -80,11 +81,25 @@ class GpuSearchResult:
     seed: int
 
 
+def normalize_rows(p, q) -> tuple[np.ndarray, np.ndarray]:
+    """Canonical P/Q of every state given as raw rows p[b], q[b] (the columns
+    of each row in either order): points_to_permutations of each, by the
+    library's host routine n3_normalize_pairs (the same augmenting-path search,
+    so the same result).  ValueError if a state is not a row/column 2-factor."""
+    p = np.ascontiguousarray(np.atleast_2d(p), dtype=np.int32)
+    q = np.ascontiguousarray(np.atleast_2d(q), dtype=np.int32)
+    if p.shape != q.shape:
+        raise ValueError("P and Q rows must have the same shape")
+    po, qo = np.empty_like(p), np.empty_like(q)
+    _lib.call("n3_normalize_pairs", p.ctypes.data, q.ctypes.data, p.shape[0], p.shape[1], po.ctypes.data,
+              qo.ctypes.data)
+    return po, qo
+
+
 def _normalize_raw(p: np.ndarray, q: np.ndarray) -> PairPermutations:
     """gpu_device_search.py:178-182: raw P/Q rows back to a canonical state."""
-    n = p.shape[0]
-    points = [(row, int(p[row])) for row in range(n)] + [(row, int(q[row])) for row in range(n)]
-    return points_to_permutations(points, n)
+    po, qo = normalize_rows(p, q)
+    return PairPermutations(tuple(int(x) for x in po[0]), tuple(int(x) for x in qo[0]))
 
 
 def elite_key(score: int, badness: np.ndarray) -> tuple[int, int, int]:
@@ -270,7 +285,8 @@ def gpu_device_beam_search(
             ep = beam.elite_p[:count].cpu().numpy()
             eq = beam.elite_q[:count].cpu().numpy()
             scores = beam.elite_scores[:count].cpu().numpy()
-            normalized = [np.column_stack((s.P, s.Q)) for s in (_normalize_raw(p, q) for p, q in zip(ep, eq))]
+            npp, nqq = normalize_rows(ep, eq)
+            normalized = [np.column_stack((a, c)) for a, c in zip(npp, nqq)]
             best_state = _normalize_raw(beam.best_p.cpu().numpy(), beam.best_q.cpu().numpy())
             callback(GpuSearchSnapshot(generation, time.perf_counter() - started,
                                        evaluations + population * completed, int(st[6]), int(st[1]),

@@ -31,7 +31,8 @@ from typing import Callable
 import numpy as np
 
 from . import _lib
-from .gpu_device_search import GpuSearchResult, GpuSearchSnapshot, _normalize_raw, elite_key, rank_elites
+from .gpu_device_search import (GpuSearchResult, GpuSearchSnapshot, _normalize_raw, elite_key, normalize_rows,
+                                 rank_elites)
 from .state import PairPermutations
 
 _P = ctypes.c_void_p
@@ -269,11 +270,8 @@ def gpu_exhaustive_beam_search(
             best_score, best_key = generation_best, generation_key
             best_p, best_q = pp[order_in_prospects[0]].copy(), pq[order_in_prospects[0]].copy()
         if callback is not None and (improved or generation % max(1, report_every) == 0):
-            raw_p, raw_q = pp[order_in_prospects], pq[order_in_prospects]
-            normalized = []
-            for p, q in zip(raw_p, raw_q):
-                s = _normalize_raw(p, q)
-                normalized.append(np.column_stack((s.P, s.Q)))
+            npp, nqq = normalize_rows(pp[order_in_prospects], pq[order_in_prospects])
+            normalized = [np.column_stack((a, c)) for a, c in zip(npp, nqq)]
             callback(GpuSearchSnapshot(generation, time.perf_counter() - started, evaluations, generation_best,
                                        best_score, tuple(map(int, elite_scores)), np.asarray(normalized, np.int32),
                                        _normalize_raw(best_p, best_q)))
