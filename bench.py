@@ -892,7 +892,7 @@ def run_b200(args):
             "gpu_launches": args.steps * (2 if args.mode == "checked" else 1),
             "roofline": {"bound": "int32 pipes (FMA pipe for products, ALU pipe for compares)",
                          "kernel": "n3::det_kernel<ColSource,false> (the larger of the checked step's two "
-                                   "launches; the other is n3::slope_kernel<2>), timed alone",
+                                   "launches; the other is n3::slope4_kernel<2>), timed alone",
                          "kernel_launch_us": det_launch_s * 1e6,
                          "kernel_tests_per_s": kernel_tests,
                          "achieved": achieved, "peak": peak, "unit": "Gop/s", "frac": achieved / peak,
