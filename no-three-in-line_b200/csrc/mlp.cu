@@ -210,7 +210,8 @@ __global__ void __launch_bounds__(kCand) candidates_kernel(const CandArgs A) {
 // Chain part of layer 1 for every chain: c1[c][n] = b1[n] + sum_k W1[n][12 + k] badn[c][k]
 // (k < 150).  One thread per output column n, kChainTile chains per CTA (their
 // badness rows staged in shared memory, zero-padded to 160; 2048 chains make 293
-// CTAs, two per SM; 16 chains per CTA measured slower).  W1's chain columns pass through shared memory in chunks of
+// CTAs, two per SM; 16 chains per CTA, and 28 chains x 128 columns per CTA on 148
+// CTAs, measured slower).  W1's chain columns pass through shared memory in chunks of
 // 32, read row-contiguously (coalesced, the next chunk in flight while this one
 // is used) and stored transposed with a 257-float stride (no bank conflicts
 // either way).  Columns up to 171 stay inside the 192-wide rows.  Deterministic:
