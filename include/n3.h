@@ -81,10 +81,11 @@ int n3_score_slope(const int16_t* cols, int B, int n, int32_t* scores, int32_t* 
 /* Fused, cross-checked scoring: determinant count and slope count per state,
  * plus the column-range / duplicate-point checks.  scores = determinant E,
  * badness = slope badness, or NULL: then the slope side counts E alone, each
- * collinear triple once from its first slot (3/4 of the time).  *mismatch (device int32, accumulated, caller zeroes it) counts states whose
- * two counts differ or whose badness does not sum to 3E; *error_word (device uint32, OR-ed, caller zeroes it, may be NULL)
- * collects the device error bits (1: column range, 2: duplicate point,
- * 4: mismatch).  The reference runs this audit on the host
+ * collinear triple once from its first slot (about 2/3 of the slope side's
+ * time).  *mismatch (device int32, accumulated, caller zeroes it) counts
+ * states whose two counts differ or whose badness does not sum to 3E;
+ * *error_word (device uint32, OR-ed, caller zeroes it, may be NULL) collects
+ * the device error bits (1: column range, 2: duplicate point, 4: mismatch).  The reference runs this audit on the host
  * (src/no_three_75/gpu.py:131 exact_match, src/no_three_75/tempering.py:193-204). */
 int n3_score_checked(const int16_t* cols, int B, int n, int32_t* scores, int32_t* badness,
                      int32_t* mismatch, uint32_t* error_word, void* stream);
