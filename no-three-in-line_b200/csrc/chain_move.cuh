@@ -83,7 +83,8 @@ struct Team {
   }
 };
 
-// hist_build_full for a team: slot k = t + 32 WPC j, j < kSlots; KEYED: the
+// Direction histogram of centre (rx, cx) on the full signed table, by a team:
+// slot k = t + 32 WPC j, j < kSlots, except skip0, skip1 and row rx; KEYED: the
 // slots' table keys come from tm.key instead of the columns in cs.
 template <int WPC, bool KEYED = false>
 __device__ __forceinline__ int team_hist_build(const Team<WPC>& tm, const int* __restrict__ cs, int m, int rx, int cx,

@@ -47,27 +47,6 @@ __device__ __forceinline__ void hist_clear(uint32_t* hist, int id) { hist[id >> 
 
 constexpr int kSlotsPerLane = (kMaxM + 31) / 32;  // 5
 
-// Direction histogram around centre X = (rx, cx) over the slots of the state in
-// smem `cs` (m slots) except skip0, skip1 and except points in X's row (their
-// direction (0,1) is unique).  ids[t] receives the id of slot lane + 32 t
-// (-1 if not inserted).  Returns this lane's share of sum_dir C(count, 2).
-__device__ __forceinline__ int hist_build(const int* __restrict__ cs, int m, int rx, int cx, int skip0, int skip1,
-                                          const uint16_t* __restrict__ lut, uint32_t* __restrict__ hist, int lane,
-                                          int (&ids)[kSlotsPerLane]) {
-  int pairs = 0;
-#pragma unroll
-  for (int t = 0; t < kSlotsPerLane; ++t) {
-    const int k = lane + 32 * t;
-    ids[t] = -1;
-    if (k < m && k != skip0 && k != skip1 && (k >> 1) != rx) {
-      const int id = dir_id(lut, (k >> 1) - rx, cs[k] - cx);
-      ids[t] = id;
-      pairs += hist_add(hist, id);
-    }
-  }
-  return pairs;
-}
-
 // Full direction table (signed dx, no normalisation at lookup), kept in shared
 // memory by the kernels that evaluate moves: entry (dx + kMaxN - 1) * kLutW +
 // dy + kMaxN - 1 holds the id of (dx, dy); (0, 0) holds 0 and is never read.
@@ -87,25 +66,6 @@ __device__ __forceinline__ void full_lut_copy(uint16_t* __restrict__ dst, const 
 
 __device__ __forceinline__ int dir_id_full(const uint16_t* __restrict__ lutf, int dx, int dy) {
   return lutf[dx * kLutW + dy + kFullLutCentre];
-}
-
-// hist_build over the full table: same insertions, same result.
-__device__ __forceinline__ int hist_build_full(const int* __restrict__ cs, int m, int rx, int cx, int skip0,
-                                               int skip1, const uint16_t* __restrict__ lutf,
-                                               uint32_t* __restrict__ hist, int lane, int (&ids)[kSlotsPerLane]) {
-  const uint16_t* base = lutf + kFullLutCentre - (rx * kLutW + cx);
-  int pairs = 0;
-#pragma unroll
-  for (int t = 0; t < kSlotsPerLane; ++t) {
-    const int k = lane + 32 * t;
-    ids[t] = -1;
-    if (k < m && k != skip0 && k != skip1 && (k >> 1) != rx) {
-      const int id = base[(k >> 1) * kLutW + cs[k]];
-      ids[t] = id;
-      pairs += hist_add(hist, id);
-    }
-  }
-  return pairs;
 }
 
 __device__ __forceinline__ void hist_release(uint32_t* hist, const int (&ids)[kSlotsPerLane]) {

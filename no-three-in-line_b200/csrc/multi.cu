@@ -36,9 +36,10 @@ __device__ __forceinline__ void lane_keys(const int* __restrict__ cs, int m, int
   }
 }
 
-// hist_build_full over A: slots whose bit t is set in `skip` (this lane's slot
-// lane + 32 t is a moved one) are left out, and so are the points in row rx.
-// key: lane_keys of the state.
+// Direction histogram of centre (rx, cx) over A, on the full signed table:
+// slots whose bit t is set in `skip` (this lane's slot lane + 32 t is a moved
+// one) are left out, and so are the points in row rx.  key: lane_keys of the
+// state.
 __device__ __forceinline__ int hist_build_excl(const int (&key)[kT], int m, int rx, int cx, uint32_t skip,
                                                const uint16_t* __restrict__ lutf, uint32_t* __restrict__ hist,
                                                int lane, int (&ids)[kT]) {
