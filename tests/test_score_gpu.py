@@ -104,6 +104,8 @@ def test_long_lines_mixed_into_a_population(oracle, cuda):
     assert np.array_equal(s2, ref_s) and np.array_equal(b2, ref_b)
     chk = gpu.score_checked_gpu(cols)
     assert np.array_equal(chk.scores, ref_s) and np.array_equal(chk.badness, ref_b) and chk.mismatches == 0
+    fwd = gpu.score_checked_gpu(cols, badness=False)  # the forward count's own overflow path
+    assert np.array_equal(fwd.scores, ref_s) and fwd.mismatches == 0
     assert max(ref_s[slot] for slot in slots) > 10000  # a line of 74 or 75 points is among them
 
 
