@@ -82,6 +82,8 @@ def parse():
     ap.add_argument("--learned-moves", type=str, default="1",
                     help="time-to-target: comma-separated moves per learned step to compare (1 = one move per "
                          "step); learned: the first value is the moves per step")
+    ap.add_argument("--learned-threads", type=int, default=0, choices=(0, 32, 64),
+                    help="learned: threads per chain of the exact moves (0 = the library's default)")
     return ap.parse_args()
 
 
@@ -431,7 +433,7 @@ def run_chain_mode(args):
         per_step, unit, what = 2048 * 150 * 10, "deltas/s", "exact swap deltas (proposals)"
     else:
         moves = int(args.learned_moves.split(",")[0])
-        lp = learned.LearnedProposal(ch, seed=1, moves=moves)
+        lp = learned.LearnedProposal(ch, seed=1, moves=moves, threads_per_chain=args.learned_threads)
         lp.run(50, exchange_every=50, train_every=10, block=50)
         step = lambda: lp.run(50, exchange_every=50, train_every=10, block=50, warm=False)  # noqa: E731
         per_step, unit, what = 2048 * 128 * 50, "candidates/s", "MLP-scored candidates"
@@ -447,7 +449,9 @@ def run_chain_mode(args):
             "scaling": "weak", "vs_baseline": None, "dtype": "int32" if args.mode == "tempering" else "bf16",
             "data": "synthetic: random_state(75, Random(91001+c)) chain starts",
             "config": {"workload": f"n=75, 2048 chains, 32 ladders x 64 temperatures (0.05..5.0): {what}",
-                       "mode": args.mode, **({"moves_per_step": moves} if args.mode == "learned" else {}),
+                       "mode": args.mode,
+                       **({"moves_per_step": moves, "threads_per_chain": args.learned_threads}
+                          if args.mode == "learned" else {}),
                        "anneal_sweeps": args.anneal_sweeps},
             "mean_E_at_start": e_start, "best_E": int(ch.best_energy.min().item())}
     print(json.dumps(line), flush=True)

@@ -264,6 +264,12 @@ int n3_mlp_infer(const n3_mlp* mlp, int tiles, void* stream);
  * advances the step counter.  temps: the ladder's L temperatures (device). */
 int n3_mlp_step(const n3_chains* chains, const n3_mlp* mlp, const float* temps, uint64_t seed, int moves,
                 void* stream);
+/* The same step with the width of the team that works on one chain chosen by
+ * the caller: threads_per_chain 32 (one warp) or 64 (two warps sharing the
+ * chain's histogram); 0 takes the default.  No counterpart in the reference.
+ * Results do not depend on the width. */
+int n3_mlp_step_team(const n3_chains* chains, const n3_mlp* mlp, const float* temps, uint64_t seed, int moves,
+                     int threads_per_chain, void* stream);
 /* One Adam step on a batch drawn from the ring slots recorded so far (all
  * counters live on the device, so the call is graph-capturable); scratch
  * holds n3_mlp_scratch_floats(batch) floats, grads/adam_m/adam_v

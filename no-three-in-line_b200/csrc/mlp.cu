@@ -553,7 +553,10 @@ __global__ void __launch_bounds__(kInferThreads, 1) infer_kernel(const InferArgs
 // Learned step: sample one candidate per chain from softmax(-pred / T), score
 // it exactly, Metropolis-accept with the chain's threshold row, update the
 // state and badness, and push the (features, exact dE) tuple to the ring.
-// One warp per chain, state in shared memory (as in the tempering kernel).
+// One team of WPC warps per chain (1 or 2), state in shared memory (as in the
+// tempering kernel).  Every warp of a team runs the same draw on the same
+// registers, so the team needs no broadcast; the exact move splits its slots
+// over the team.
 // ---------------------------------------------------------------------------
 struct StepArgs {
   n3_chains ch;
@@ -572,33 +575,39 @@ struct StepArgs {
   int moves;              // moves drawn per step (without replacement)
 };
 
-constexpr int kStepWarps = 14;  // 2048 chains -> 147 CTAs, one per SM
+constexpr int kStepChains = 14;  // chains per CTA: 2048 chains -> 147 CTAs, one per SM
 
-__global__ void __launch_bounds__(kStepWarps * 32, 1) learned_step_kernel(const StepArgs A) {
+template <int WPC>
+__global__ void __launch_bounds__(kStepChains * 32 * WPC, 1) learned_step_kernel(const StepArgs A) {
+  constexpr int TT = Team<WPC>::kThreads;
   extern __shared__ __align__(16) unsigned char smem[];
   const n3_chains& ch = A.ch;
   uint16_t* lut = reinterpret_cast<uint16_t*>(smem);
   uint32_t* hist_all = reinterpret_cast<uint32_t*>(smem + kFullLutBytes);
-  int* cs_all = reinterpret_cast<int*>(hist_all + kStepWarps * kDirWords);
-  int* bs_all = cs_all + kStepWarps * kMaxM;
+  int* cs_all = reinterpret_cast<int*>(hist_all + kStepChains * kDirWords);
+  int* bs_all = cs_all + kStepChains * kMaxM;
+  int* team_red = bs_all + kStepChains * kMaxM;  // 2 WPC ints per chain (WPC > 1)
+  int* cand_all = team_red + kStepChains * 4;    // this step's candidate codes and predictions
+  float* pred_all = reinterpret_cast<float*>(cand_all + kStepChains * kCand);
   full_lut_copy(lut, A.lut);
-  for (int i = threadIdx.x; i < kStepWarps * kDirWords / 4; i += blockDim.x)
+  for (int i = threadIdx.x; i < kStepChains * kDirWords / 4; i += blockDim.x)
     reinterpret_cast<uint4*>(hist_all)[i] = make_uint4(0u, 0u, 0u, 0u);
   __syncthreads();
-  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const int c = blockIdx.x * kStepWarps + warp;
-  if (c >= ch.n_chains) return;  // no block-level barrier follows
+  const int team = threadIdx.x / TT;  // this chain's index in the CTA
+  Team<WPC> tm{(int)threadIdx.x % TT, 1 + team, team_red + 2 * WPC * team, 0, {}};
+  const int lane = tm.t & 31;
+  const int c = blockIdx.x * kStepChains + team;
+  if (c >= ch.n_chains) return;  // the whole team leaves; no block-level barrier follows
   const int L = ch.ladder_size;
   const int n = ch.ladder_n[c / L], m = 2 * n;
-  int* cs = cs_all + warp * kMaxM;
-  int* bs = bs_all + warp * kMaxM;
-  uint32_t* hist = hist_all + warp * kDirWords;
-  for (int s = lane; s < m; s += 32) {
+  int* cs = cs_all + team * kMaxM;
+  int* bs = bs_all + team * kMaxM;
+  uint32_t* hist = hist_all + team * kDirWords;
+  for (int s = tm.t; s < m; s += TT) {
     cs[s] = ch.cols[(size_t)c * kMaxM + s];
     bs[s] = ch.badness[(size_t)c * kMaxM + s];
   }
-  Team<1> tm{lane, 0, nullptr, 0, {}};
-  team_load_keys(tm, cs, m);  // the slots' table keys, kept in registers across the moves
+  team_load_keys(tm, cs, m);  // the thread's own slots' table keys, kept in registers across the moves
   const int temp = ch.temp_of[c];
   const float T = A.temps[temp];
   // softmax(-pred / T) over the legal candidates, sampled by inverse CDF;
@@ -608,17 +617,28 @@ __global__ void __launch_bounds__(kStepWarps * 32, 1) learned_step_kernel(const 
   // so a draw needs one warp scan of the lane totals.
   constexpr int kPer = kCand / 32;
   static_assert(kPer == 4, "four candidates per lane");
-  const int4 cw4 = reinterpret_cast<const int4*>(A.cand + (size_t)c * kCand)[lane];
-  const float4 pr4 = reinterpret_cast<const float4*>(A.pred + (size_t)c * kCand)[lane];
-  const int cwv[kPer] = {cw4.x, cw4.y, cw4.z, cw4.w};
-  const float prv[kPer] = {pr4.x, pr4.y, pr4.z, pr4.w};
+  // The codes and predictions also go to shared memory, where a draw reads the
+  // picked one (registers hold only the weights).
+  int* cand_c = cand_all + team * kCand;
+  float* pred_c = pred_all + team * kCand;
   float w[kPer];
   float mx = -INFINITY;
+  {
+    const int4 cw4 = reinterpret_cast<const int4*>(A.cand + (size_t)c * kCand)[lane];
+    const float4 pr4 = reinterpret_cast<const float4*>(A.pred + (size_t)c * kCand)[lane];
+    if (tm.t < 32) {
+      reinterpret_cast<int4*>(cand_c)[lane] = cw4;
+      reinterpret_cast<float4*>(pred_c)[lane] = pr4;
+    }
+    const int cwv[kPer] = {cw4.x, cw4.y, cw4.z, cw4.w};
+    const float prv[kPer] = {pr4.x, pr4.y, pr4.z, pr4.w};
 #pragma unroll
-  for (int q = 0; q < kPer; ++q) {
-    w[q] = cwv[q] < 0 ? -prv[q] / T : -INFINITY;
-    mx = fmaxf(mx, w[q]);
+    for (int q = 0; q < kPer; ++q) {
+      w[q] = cwv[q] < 0 ? -prv[q] / T : -INFINITY;
+      mx = fmaxf(mx, w[q]);
+    }
   }
+  tm.sync();  // the state and the candidates are read by the whole team from here on
 #pragma unroll
   for (int o = 16; o; o >>= 1) mx = fmaxf(mx, __shfl_xor_sync(0xffffffffu, mx, o));
 #pragma unroll
@@ -670,16 +690,8 @@ __global__ void __launch_bounds__(kStepWarps * 32, 1) learned_step_kernel(const 
       owner = 31 - __clz(hit);
       q_pick = __shfl_sync(0xffffffffu, q_last, owner);
     }
-    int cw_mine = cwv[0];
-    float p_mine = prv[0];
-#pragma unroll
-    for (int q = 1; q < kPer; ++q)
-      if (q == q_pick) {
-        cw_mine = cwv[q];
-        p_mine = prv[q];
-      }
-    const int cw = __shfl_sync(0xffffffffu, cw_mine, owner);
-    const float p = __shfl_sync(0xffffffffu, p_mine, owner);
+    const int cw = cand_c[kPer * owner + q_pick];
+    const float p = pred_c[kPer * owner + q_pick];
     if (lane == owner) {  // without replacement
 #pragma unroll
       for (int q = 0; q < kPer; ++q)
@@ -687,23 +699,24 @@ __global__ void __launch_bounds__(kStepWarps * 32, 1) learned_step_kernel(const 
     }
     const int u = cw & 0xFF, v = (cw >> 8) & 0xFF;
     if (k > 0 && !legal_swap(cs, u, v)) continue;  // an earlier move of this step made it illegal
-    // tuple: features of the state before the move (lane i writes feature i)
+    // tuple: features of the state before the move (thread i writes feature i).
+    // These reads of cs and bs come before the move's first team barrier, and
+    // the move writes the state only after later ones.
     const uint64_t tuple = (step * (uint64_t)ch.n_chains + (uint64_t)c) * (uint64_t)A.moves + (uint64_t)k;
     const int64_t slot = (int64_t)(tuple % (uint64_t)A.rb_cap);
-    if (lane < kCandFeat) {
-      const int which = lane & 3;
+    if (tm.t < kCandFeat) {
+      const int which = tm.t & 3;
       const int sidx = which == 0 ? u : which == 1 ? v : which == 2 ? (u ^ 1) : (v ^ 1);
-      const float f = lane < 4 ? (float)bs[sidx] * (1.0f / 16.0f)
-                               : (float)(lane < 8 ? (sidx >> 1) : cs[sidx]) * (1.0f / (float)n);
-      A.rb_feat[slot * kCandFeat + lane] = bf16_bits(f);
+      const float f = tm.t < 4 ? (float)bs[sidx] * (1.0f / 16.0f)
+                               : (float)(tm.t < 8 ? (sidx >> 1) : cs[sidx]) * (1.0f / (float)n);
+      A.rb_feat[slot * kCandFeat + tm.t] = bf16_bits(f);
     }
-    for (int s = lane; s < kChainFeat; s += 32)
+    for (int s = tm.t; s < kChainFeat; s += TT)
       A.rb_bad[slot * kChainFeat + s] = (uint8_t)(s < m ? min(bs[s], 255) : 0);
-    __syncwarp();
     int dE = 0;
-    const int acc = team_move<1, false, false, false, true>(tm, cs, bs, m, lut, hist, u, v, r.y, thr, ch.acc_width, E,
-                                                            err, &dE);
-    if (lane == 0) A.rb_dE[slot] = (int16_t)max(-32768, min(32767, dE));
+    const int acc = team_move<WPC, false, false, false, true>(tm, cs, bs, m, lut, hist, u, v, r.y, thr, ch.acc_width,
+                                                              E, err, &dE);
+    if (tm.t == 0) A.rb_dE[slot] = (int16_t)max(-32768, min(32767, dE));
     n_acc += acc ? 1u : 0u;
     st_abs += fabsf(p - (float)dE);
     st_n += 1.0f;
@@ -713,14 +726,14 @@ __global__ void __launch_bounds__(kStepWarps * 32, 1) learned_step_kernel(const 
     }
     if (acc && E < bestE) {
       bestE = E;
-      for (int s = lane; s < m; s += 32) ch.best_cols[(size_t)c * kMaxM + s] = (int16_t)cs[s];
+      for (int s = tm.t; s < m; s += TT) ch.best_cols[(size_t)c * kMaxM + s] = (int16_t)cs[s];
     }
   }
-  for (int s = lane; s < m; s += 32) {
+  for (int s = tm.t; s < m; s += TT) {
     ch.cols[(size_t)c * kMaxM + s] = (int16_t)cs[s];
     ch.badness[(size_t)c * kMaxM + s] = bs[s];
   }
-  if (lane == 0) {
+  if (tm.t == 0) {
     ch.energy[c] = E;
     ch.best_energy[c] = bestE;
     ch.accepted[c] += n_acc;
@@ -1015,14 +1028,21 @@ static int launch_pack(const n3_mlp* M, cudaStream_t st) {
   return check_launch("mlp pack_kernel");
 }
 
-static size_t step_smem() {
-  return n3::kFullLutBytes +
-         kStepWarps * (sizeof(uint32_t) * n3::kDirWords + 2 * sizeof(int) * n3::kMaxM);
+static size_t step_smem() {  // the team scratch is sized for the widest team (2 warps)
+  return n3::kFullLutBytes + kStepChains * (sizeof(uint32_t) * n3::kDirWords + 2 * sizeof(int) * n3::kMaxM +
+                                            4 * sizeof(int) + kCand * (sizeof(int) + sizeof(float)));
+}
+
+// Threads per chain of the learned step when the caller leaves it open.
+static int default_step_threads(int n_chains) {
+  (void)n_chains;
+  return 32;
 }
 
 int prepare_mlp() {
   N3_TRY(allow_smem(reinterpret_cast<const void*>(infer_kernel), kInferSmem));
-  return allow_smem(reinterpret_cast<const void*>(learned_step_kernel), step_smem());
+  N3_TRY(allow_smem(reinterpret_cast<const void*>(learned_step_kernel<1>), step_smem()));
+  return allow_smem(reinterpret_cast<const void*>(learned_step_kernel<2>), step_smem());
 }
 
 }  // namespace n3host
@@ -1151,13 +1171,16 @@ int n3_mlp_infer(const n3_mlp* M, int tiles, void* stream) {
   return n3host::check_launch("infer_kernel");
 }
 
-int n3_mlp_step(const n3_chains* ch, const n3_mlp* M, const float* temps, uint64_t seed, int moves, void* stream) {
+int n3_mlp_step_team(const n3_chains* ch, const n3_mlp* M, const float* temps, uint64_t seed, int moves,
+                     int threads_per_chain, void* stream) {
   using namespace n3::mlp;
   if (!ch || !M || !temps) return n3host::set_error(N3_ERR_ARG, "null descriptor");
   if (moves < 1 || moves > kCand) return n3host::set_error(N3_ERR_RANGE, "moves per step %d outside [1, 128]", moves);
+  if (threads_per_chain == 0) threads_per_chain = n3host::default_step_threads(ch->n_chains);
+  if (threads_per_chain != 32 && threads_per_chain != 64)
+    return n3host::set_error(N3_ERR_RANGE, "threads per chain %d: the learned step takes 32 or 64", threads_per_chain);
   N3_TRY(n3host::ensure_device_tables());
   const size_t smem = n3host::step_smem();
-  N3_TRY(n3host::allow_smem(reinterpret_cast<const void*>(learned_step_kernel), smem));
   StepArgs A;
   A.ch = *ch;
   A.lut = n3host::dir_lut_full_device_ptr();
@@ -1173,11 +1196,21 @@ int n3_mlp_step(const n3_chains* ch, const n3_mlp* M, const float* temps, uint64
   A.rb_cap = M->rb_capacity;
   A.stats = M->stats;
   A.moves = moves;
-  const int grid = (ch->n_chains + kStepWarps - 1) / kStepWarps;
-  learned_step_kernel<<<grid, kStepWarps * 32, smem, (cudaStream_t)stream>>>(A);
+  const int grid = (ch->n_chains + kStepChains - 1) / kStepChains;
+  if (threads_per_chain == 64) {
+    N3_TRY(n3host::allow_smem(reinterpret_cast<const void*>(learned_step_kernel<2>), smem));
+    learned_step_kernel<2><<<grid, kStepChains * 64, smem, (cudaStream_t)stream>>>(A);
+  } else {
+    N3_TRY(n3host::allow_smem(reinterpret_cast<const void*>(learned_step_kernel<1>), smem));
+    learned_step_kernel<1><<<grid, kStepChains * 32, smem, (cudaStream_t)stream>>>(A);
+  }
   N3_TRY(n3host::check_launch("learned_step_kernel"));
   bump_kernel<<<1, 1, 0, (cudaStream_t)stream>>>(M->counters, 0);
   return n3host::check_launch("bump_kernel");
+}
+
+int n3_mlp_step(const n3_chains* ch, const n3_mlp* M, const float* temps, uint64_t seed, int moves, void* stream) {
+  return n3_mlp_step_team(ch, M, temps, seed, moves, 0, stream);
 }
 
 int n3_mlp_train(const n3_mlp* M, int n_chains, int batch, float lr, uint64_t seed, float* scratch, float* grads,

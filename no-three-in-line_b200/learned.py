@@ -47,6 +47,8 @@ _lib.register("n3_mlp_candidates", [ctypes.POINTER(N3Chains), ctypes.POINTER(N3M
 _lib.register("n3_mlp_infer", [ctypes.POINTER(N3Mlp), ctypes.c_int, _P])
 _lib.register("n3_mlp_step", [ctypes.POINTER(N3Chains), ctypes.POINTER(N3Mlp), _P, ctypes.c_uint64, ctypes.c_int,
                               _P])
+_lib.register("n3_mlp_step_team", [ctypes.POINTER(N3Chains), ctypes.POINTER(N3Mlp), _P, ctypes.c_uint64,
+                                   ctypes.c_int, ctypes.c_int, _P])
 _lib.register("n3_mlp_train", [ctypes.POINTER(N3Mlp), ctypes.c_int, ctypes.c_int, ctypes.c_float, ctypes.c_uint64,
                                _P, _P, _P, _P, _P])
 
@@ -105,11 +107,15 @@ class LearnedProposal:
 
     def __init__(self, chains: TemperingChains, *, seed: int = 1, ring_capacity: int = 1 << 21,
                  batch: int = 4096, lr: float = 1e-3, params: np.ndarray | None = None, moves: int = 1,
-                 bad_bias: int = 0):
+                 bad_bias: int = 0, threads_per_chain: int = 0):
         t = _lib.torch()
         if not 0 <= bad_bias <= 100:
             raise ValueError("bad_bias must lie in [0,100]")
+        if threads_per_chain not in (0, 32, 64):
+            raise ValueError("threads_per_chain must be 0 (the default), 32 or 64")
         self.bad_bias = int(bad_bias)
+        # width of the team that makes one chain's exact moves (0: the library's default)
+        self.threads_per_chain = int(threads_per_chain)
         self.ch = chains
         dev = chains.device
         C = chains.cols.shape[0]
@@ -169,8 +175,9 @@ class LearnedProposal:
         """One learned step on every chain."""
         self.propose_scores(stream)
         cd = self.ch._descriptor()
-        _lib.check(_lib.lib().n3_mlp_step(ctypes.byref(cd), ctypes.byref(self._desc), self.temps.data_ptr(),
-                                          self.seed, self.moves, _lib.stream_ptr(stream)), "n3_mlp_step")
+        _lib.check(_lib.lib().n3_mlp_step_team(ctypes.byref(cd), ctypes.byref(self._desc), self.temps.data_ptr(),
+                                               self.seed, self.moves, self.threads_per_chain,
+                                               _lib.stream_ptr(stream)), "n3_mlp_step_team")
         self.ch._moved(False)
 
     def train(self, stream=None):

@@ -88,3 +88,20 @@ def test_beam_entry_points_check_arguments_on_the_host():
     assert L.n3_py_random_shuffle(None, None, 3, None) == _lib.N3_ERR_ARG
     assert L.n3_py_shuffle_steps(None, 3, None, None) == _lib.N3_ERR_ARG
     assert L.n3_py_shuffle_steps(ctypes.c_void_p(16), 65537, ctypes.c_void_p(16), None) == _lib.N3_ERR_RANGE
+
+
+def test_learned_step_checks_its_team_width_on_the_host():
+    from no_three_in_line_b200 import _lib, learned
+    from no_three_in_line_b200.tempering import N3Chains
+
+    L = _lib.lib()
+    ch, M, temps = N3Chains(), learned.N3Mlp(), ctypes.c_void_p(16)
+    assert L.n3_mlp_step_team(ctypes.byref(ch), ctypes.byref(M), temps, 1, 1, 48, None) == _lib.N3_ERR_RANGE
+    assert "48" in _lib.last_error()
+    assert L.n3_mlp_step_team(ctypes.byref(ch), ctypes.byref(M), temps, 1, 0, 32, None) == _lib.N3_ERR_RANGE
+    assert L.n3_mlp_step_team(None, ctypes.byref(M), temps, 1, 1, 32, None) == _lib.N3_ERR_ARG
+    # the Python wrapper refuses other widths before it allocates anything
+    import pytest
+
+    with pytest.raises(ValueError):
+        learned.LearnedProposal.__init__(object.__new__(learned.LearnedProposal), None, threads_per_chain=48)

@@ -189,3 +189,24 @@ def test_several_moves_per_step_keep_energies_exact(cuda):
     assert int(ch.error_word.item()) == 0
     st = lp.read_stats()
     assert st.proposals > 64 * 201 * 3 and st.accepted > 0
+
+
+@pytest.mark.parametrize("moves", [1, 4])
+def test_team_width_does_not_change_the_learned_run(cuda, moves):
+    """One warp or a team of two per chain: the same draws, the same exact
+    moves, the same ring-buffer tuples, bit for bit (64 chains: the last CTA
+    of 14 chains is partly empty)."""
+    runs = []
+    for tpc in (32, 64):
+        ch = make(chains=64, L=16, seed=31)
+        lp = learned.LearnedProposal(ch, seed=31, ring_capacity=1 << 14, batch=256, moves=moves,
+                                     threads_per_chain=tpc)
+        lp.run(100, exchange_every=50, train_every=0, block=50, graph=tpc == 64, warm=False)
+        ch.validate()
+        assert int(ch.error_word.item()) == 0
+        runs.append([x.cpu().numpy() for x in (ch.cols, ch.energy, ch.best_energy, ch.best_cols, ch.badness_dev,
+                                               ch.accepted_dev, lp.rb_feat, lp.rb_bad, lp.rb_dE)])
+        assert int(lp.read_stats().accepted) > 0
+    for a, b in zip(*runs):
+        assert np.array_equal(a, b)
+
