@@ -266,8 +266,9 @@ int n3_mlp_step(const n3_chains* chains, const n3_mlp* mlp, const float* temps, 
                 void* stream);
 /* The same step with the width of the team that works on one chain chosen by
  * the caller: threads_per_chain 32 (one warp) or 64 (two warps sharing the
- * chain's histogram); 0 takes the default.  No counterpart in the reference.
- * Results do not depend on the width. */
+ * chain's histogram); 0 takes the default (64 for several moves per step, 32
+ * for one).  No counterpart in the reference.  Results do not depend on the
+ * width.  A ring buffer capacity below 1 is rejected with N3_ERR_ARG. */
 int n3_mlp_step_team(const n3_chains* chains, const n3_mlp* mlp, const float* temps, uint64_t seed, int moves,
                      int threads_per_chain, void* stream);
 /* One Adam step on a batch drawn from the ring slots recorded so far (all

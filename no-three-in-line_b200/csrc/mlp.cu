@@ -207,73 +207,6 @@ __global__ void __launch_bounds__(kCand) candidates_kernel(const CandArgs A) {
   A.cand[(size_t)c * kCand + j] = u | (v << 8) | (legal ? (1 << 31) : 0);
 }
 
-// Chain part of layer 1 for every chain: c1[c][n] = b1[n] + sum_k W1[n][12 + k] badn[c][k]
-// (k < 150).  One thread per output column n, kChainTile chains per CTA (their
-// badness rows staged in shared memory, zero-padded to 160; 2048 chains make 293
-// CTAs, two per SM; 16 chains per CTA, and 28 chains x 128 columns per CTA on 148
-// CTAs, measured slower).  W1's chain columns pass through shared memory in chunks of
-// 32, read row-contiguously (coalesced, the next chunk in flight while this one
-// is used) and stored transposed with a 257-float stride (no bank conflicts
-// either way).  Columns up to 171 stay inside the 192-wide rows.  Deterministic:
-// one thread sums each output in a fixed order.
-constexpr int kChainTile = 7;
-constexpr int kChainPad = 160;
-constexpr int kWStride = kH + 1;
-__global__ void __launch_bounds__(kH) chain_part_kernel(int C, const float* __restrict__ badn,
-                                                        const float* __restrict__ P, float* __restrict__ c1) {
-  __shared__ __align__(16) float xs[kChainTile][kChainPad];
-  __shared__ float ws[32][kWStride];
-  const int c0 = blockIdx.x * kChainTile;
-  for (int i = threadIdx.x; i < kChainTile * kChainPad; i += blockDim.x) {
-    const int cc = i / kChainPad, k = i % kChainPad;
-    xs[cc][k] = (c0 + cc < C && k < kChainFeat) ? badn[(size_t)(c0 + cc) * kChainFeat + k] : 0.f;
-  }
-  const int nn = threadIdx.x;
-  float acc[kChainTile];
-#pragma unroll
-  for (int cc = 0; cc < kChainTile; ++cc) acc[cc] = 0.f;
-  // element i = thread + 256 r of a chunk: row i / 8, columns k0 + 4 (i % 8) ..
-  auto fetch = [&](int k0, float4 (&v)[8]) {
-#pragma unroll
-    for (int r = 0; r < 8; ++r) {
-      const int i = threadIdx.x + kH * r;
-      v[r] = *reinterpret_cast<const float4*>(P + oW1 + (size_t)(i >> 3) * kIn + kCandFeat + k0 + 4 * (i & 7));
-    }
-  };
-  float4 v[8];
-  fetch(0, v);
-#pragma unroll 1
-  for (int k0 = 0; k0 < kChainPad; k0 += 32) {
-    __syncthreads();  // the previous chunk has been consumed (and, first time, xs is in place)
-#pragma unroll
-    for (int r = 0; r < 8; ++r) {
-      const int i = threadIdx.x + kH * r, row = i >> 3, kq = 4 * (i & 7);
-      ws[kq][row] = v[r].x;
-      ws[kq + 1][row] = v[r].y;
-      ws[kq + 2][row] = v[r].z;
-      ws[kq + 3][row] = v[r].w;
-    }
-    __syncthreads();
-    if (k0 + 32 < kChainPad) fetch(k0 + 32, v);
-#pragma unroll
-    for (int k = 0; k < 32; k += 4) {
-      const float w0 = ws[k][nn], w1 = ws[k + 1][nn], w2 = ws[k + 2][nn], w3 = ws[k + 3][nn];
-#pragma unroll
-      for (int cc = 0; cc < kChainTile; ++cc) {
-        const float4 x = *reinterpret_cast<const float4*>(&xs[cc][k0 + k]);
-        acc[cc] = fmaf(w0, x.x, acc[cc]);
-        acc[cc] = fmaf(w1, x.y, acc[cc]);
-        acc[cc] = fmaf(w2, x.z, acc[cc]);
-        acc[cc] = fmaf(w3, x.w, acc[cc]);
-      }
-    }
-  }
-  const float bias = P[oB1 + nn];
-#pragma unroll
-  for (int cc = 0; cc < kChainTile; ++cc)
-    if (c0 + cc < C) c1[(size_t)(c0 + cc) * kH + nn] = acc[cc] + bias;
-}
-
 // ---------------------------------------------------------------------------
 // Tensor-core inference: one persistent CTA per SM, 4 warps, one chain tile
 // (128 candidates) per iteration.
@@ -644,13 +577,17 @@ __global__ void __launch_bounds__(kStepChains * 32 * WPC, 1) learned_step_kernel
 #pragma unroll
   for (int q = 0; q < kPer; ++q) w[q] = w[q] > -INFINITY ? __expf(w[q] - mx) : 0.f;
   const uint64_t step = *A.step;
-  const uint32_t* thr = ch.acc_thresh + (size_t)temp * ch.acc_width;
   int E = ch.energy[c];
   int bestE = ch.best_energy[c];
-  uint32_t err = 0, n_acc = 0;
-  float st_abs = 0.f, st_n = 0.f, st_acc = 0.f, st_dE = 0.f;  // this chain's statistics (lane-uniform)
+  uint32_t err = 0, n_acc = 0, n_scored = 0;
+  int sum_dE_acc = 0;  // with n_acc, n_scored and st_abs: this chain's statistics (team-uniform)
+  float st_abs = 0.f;
   // the moves' Philox blocks 32 at a time: lane l makes move k0 + l's, move k takes lane k % 32's
   U4 batch = {0u, 0u, 0u, 0u};
+  // ring slot of move k: tuple (step C + c) moves + k modulo the capacity,
+  // from one 64-bit remainder per chain and step
+  const int64_t slot0 =
+      (int64_t)(((step * (uint64_t)ch.n_chains + (uint64_t)c) * (uint64_t)A.moves) % (uint64_t)A.rb_cap);
   for (int k = 0; k < A.moves; ++k) {
     const int j = k & 31;
     if (j == 0)
@@ -702,8 +639,11 @@ __global__ void __launch_bounds__(kStepChains * 32 * WPC, 1) learned_step_kernel
     // tuple: features of the state before the move (thread i writes feature i).
     // These reads of cs and bs come before the move's first team barrier, and
     // the move writes the state only after later ones.
-    const uint64_t tuple = (step * (uint64_t)ch.n_chains + (uint64_t)c) * (uint64_t)A.moves + (uint64_t)k;
-    const int64_t slot = (int64_t)(tuple % (uint64_t)A.rb_cap);
+    int64_t slot = slot0 + k;
+    if (slot >= A.rb_cap) {
+      slot -= A.rb_cap;
+      if (slot >= A.rb_cap) slot %= A.rb_cap;
+    }
     if (tm.t < kCandFeat) {
       const int which = tm.t & 3;
       const int sidx = which == 0 ? u : which == 1 ? v : which == 2 ? (u ^ 1) : (v ^ 1);
@@ -714,16 +654,14 @@ __global__ void __launch_bounds__(kStepChains * 32 * WPC, 1) learned_step_kernel
     for (int s = tm.t; s < kChainFeat; s += TT)
       A.rb_bad[slot * kChainFeat + s] = (uint8_t)(s < m ? min(bs[s], 255) : 0);
     int dE = 0;
+    const uint32_t* thr = ch.acc_thresh + (size_t)temp * ch.acc_width;  // formed here: fewer live registers
     const int acc = team_move<WPC, false, false, false, true>(tm, cs, bs, m, lut, hist, u, v, r.y, thr, ch.acc_width,
                                                               E, err, &dE);
     if (tm.t == 0) A.rb_dE[slot] = (int16_t)max(-32768, min(32767, dE));
     n_acc += acc ? 1u : 0u;
     st_abs += fabsf(p - (float)dE);
-    st_n += 1.0f;
-    if (acc) {
-      st_acc += 1.0f;
-      st_dE += (float)dE;
-    }
+    n_scored += 1u;
+    if (acc) sum_dE_acc += dE;
     if (acc && E < bestE) {
       bestE = E;
       for (int s = tm.t; s < m; s += TT) ch.best_cols[(size_t)c * kMaxM + s] = (int16_t)cs[s];
@@ -741,9 +679,9 @@ __global__ void __launch_bounds__(kStepChains * 32 * WPC, 1) learned_step_kernel
     if (ch.global_best) atomicMin(ch.global_best, E);
     // one set of statistics atomics per chain and step, not per move
     atomicAdd(A.stats + 0, st_abs);
-    atomicAdd(A.stats + 1, st_n);
-    atomicAdd(A.stats + 2, st_acc);
-    atomicAdd(A.stats + 3, st_dE);
+    atomicAdd(A.stats + 1, (float)n_scored);
+    atomicAdd(A.stats + 2, (float)n_acc);
+    atomicAdd(A.stats + 3, (float)sum_dE_acc);
   }
 }
 
@@ -789,12 +727,13 @@ __global__ void gather_kernel(const uint16_t* __restrict__ rb_feat, const uint8_
 
 
 // out = H2 . w3 + b3, d = 2 (out - y) / B, dZ2 = d w3 (Z2 > 0), loss += (out - y)^2
-// Training GEMMs on the tensor cores (tcgen05, kind::f16): C (M x N, fp32) =
+// GEMMs on the tensor cores (tcgen05, kind::f16): C (M x N, fp32) =
 // sum_k A(m, k) B(k, n) for fp32 operands given by element strides (A(m, k) at
 // A[m sam + k sak], B(k, n) at Bm[k sbk + n sbn]), with the epilogues of the
 // training step: EPI 0 store (or add, with a K split over gridDim.z: the
 // weight gradients), EPI 1 Z = acc + bias, H = relu(Z) (the forward layers),
-// EPI 2 acc masked by Z > 0 (back through a ReLU).
+// EPI 2 acc masked by Z > 0 (back through a ReLU); and EPI 3 acc + bias (the
+// chain part of layer 1 before inference).
 //
 // A CTA of 4 warps owns a 128 x kTcN output tile.  Per K slice of 64 it rounds
 // the operands to bf16 while staging them into 128B-swizzled K-major shared
@@ -934,6 +873,8 @@ __global__ void __launch_bounds__(128) tc_gemm_kernel(int M, int N, int K, const
           const float z = x + bias[nn];
           aux[o] = z;
           C[o] = fmaxf(z, 0.f);
+        } else if (EPI == 3) {
+          C[o] = x + bias[nn];
         } else {
           C[o] = aux[o] > 0.f ? x : 0.f;
         }
@@ -1033,14 +974,14 @@ static size_t step_smem() {  // the team scratch is sized for the widest team (2
                                             4 * sizeof(int) + kCand * (sizeof(int) + sizeof(float)));
 }
 
-// Threads per chain of the learned step when the caller leaves it open.
-static int default_step_threads(int n_chains) {
-  (void)n_chains;
-  return 32;
-}
+// Threads per chain of the learned step when the caller leaves it open: two
+// warps for several moves per step (2048 chains x 16 moves: 6.50 against
+// 6.68 ms per 50 steps), one for a single move (4.31 against 4.33 ms).
+static int default_step_threads(int moves) { return moves > 1 ? 64 : 32; }
 
 int prepare_mlp() {
   N3_TRY(allow_smem(reinterpret_cast<const void*>(infer_kernel), kInferSmem));
+  N3_TRY(allow_smem(reinterpret_cast<const void*>(tc_gemm_kernel<3>), kTcSmem));
   N3_TRY(allow_smem(reinterpret_cast<const void*>(learned_step_kernel<1>), step_smem()));
   return allow_smem(reinterpret_cast<const void*>(learned_step_kernel<2>), step_smem());
 }
@@ -1146,10 +1087,17 @@ int n3_mlp_candidates(const n3_chains* ch, const n3_mlp* M, uint64_t seed, int b
   cudaStream_t st = (cudaStream_t)stream;
   candidates_kernel<<<ch->n_chains, kCand, 0, st>>>(A);
   N3_TRY(n3host::check_launch("candidates_kernel"));
-  // chain part of layer 1 for every chain: c1 = badn W1b^T + b1
+  // Chain part of layer 1 for every chain, c1 = badn W1b^T + b1 (W1b: the 150
+  // chain columns of W1, B(k, n) = W1[n * 192 + 12 + k]), on the tensor cores
+  // with bf16 operands and fp32 accumulation, as the training forward computes
+  // the same product.  2048 chains: 16 x 4 CTAs of 128 x 64 outputs, K = 150
+  // in three slices.
   const int C = ch->n_chains;
-  chain_part_kernel<<<(C + kChainTile - 1) / kChainTile, kH, 0, st>>>(C, M->badn, M->params, M->c1);
-  return n3host::check_launch("chain_part_kernel");
+  N3_TRY(n3host::allow_smem(reinterpret_cast<const void*>(tc_gemm_kernel<3>), kTcSmem));
+  tc_gemm_kernel<3><<<dim3(kH / kTcN, (C + 127) / 128, 1), 128, kTcSmem, st>>>(
+      C, kH, kChainFeat, M->badn, kChainFeat, 1, M->params + oW1 + kCandFeat, 1, kIn, M->c1, kH, M->params + oB1,
+      nullptr, M->error_word);
+  return n3host::check_launch("chain part (tc_gemm_kernel<3>)");
 }
 
 int n3_mlp_infer(const n3_mlp* M, int tiles, void* stream) {
@@ -1176,7 +1124,8 @@ int n3_mlp_step_team(const n3_chains* ch, const n3_mlp* M, const float* temps, u
   using namespace n3::mlp;
   if (!ch || !M || !temps) return n3host::set_error(N3_ERR_ARG, "null descriptor");
   if (moves < 1 || moves > kCand) return n3host::set_error(N3_ERR_RANGE, "moves per step %d outside [1, 128]", moves);
-  if (threads_per_chain == 0) threads_per_chain = n3host::default_step_threads(ch->n_chains);
+  if (M->rb_capacity < 1) return n3host::set_error(N3_ERR_ARG, "ring buffer capacity %lld", (long long)M->rb_capacity);
+  if (threads_per_chain == 0) threads_per_chain = n3host::default_step_threads(moves);
   if (threads_per_chain != 32 && threads_per_chain != 64)
     return n3host::set_error(N3_ERR_RANGE, "threads per chain %d: the learned step takes 32 or 64", threads_per_chain);
   N3_TRY(n3host::ensure_device_tables());

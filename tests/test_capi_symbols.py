@@ -96,6 +96,9 @@ def test_learned_step_checks_its_team_width_on_the_host():
 
     L = _lib.lib()
     ch, M, temps = N3Chains(), learned.N3Mlp(), ctypes.c_void_p(16)
+    assert L.n3_mlp_step_team(ctypes.byref(ch), ctypes.byref(M), temps, 1, 1, 32, None) == _lib.N3_ERR_ARG
+    assert "capacity" in _lib.last_error()  # an empty ring buffer
+    M.rb_capacity = 1024
     assert L.n3_mlp_step_team(ctypes.byref(ch), ctypes.byref(M), temps, 1, 1, 48, None) == _lib.N3_ERR_RANGE
     assert "48" in _lib.last_error()
     assert L.n3_mlp_step_team(ctypes.byref(ch), ctypes.byref(M), temps, 1, 0, 32, None) == _lib.N3_ERR_RANGE

@@ -56,7 +56,8 @@ def test_inference_matches_bf16_reference(cuda):
     c1_dev = lp.c1.cpu().numpy()
     for c in list(range(0, cols.shape[0], 13)) + [cols.shape[0] - 1]:
         x_chain = bad[c] / 16.0
-        c1 = b1 + W1[:, 12:162] @ x_chain
+        # the chain part runs on the tensor cores: bf16 operands, fp32 accumulation
+        c1 = b1 + bf16(W1[:, 12:162]) @ bf16(x_chain)
         assert np.allclose(c1_dev[c], c1, rtol=1e-5, atol=1e-5)
         F = np.zeros((128, 16))
         F[:, 12:14] = 1.0  # constant columns that carry the chain part (hi, lo) into layer 1
