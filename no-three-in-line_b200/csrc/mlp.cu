@@ -11,7 +11,8 @@
 //   [162..191] zero
 // Layer 1 is split accordingly: W1 = [W1a | W1b].  The 150 chain features are
 // shared by all 128 candidates of a chain, so the chain part c1 = W1b x + b1 is
-// computed once per chain (a GEMM after candidates_kernel) and enters the
+// computed once per chain (a tcgen05 GEMM after candidates_kernel, bf16
+// operands as in the training forward) and enters the
 // per-candidate K = 16 tensor-core product through two constant-1 columns of
 // A1 (k = 12, 13) against c1 split into bf16 high and low parts (B columns
 // 12, 13; c1 = hi + lo to about 2^-17 relative).  Inference per chain is one
