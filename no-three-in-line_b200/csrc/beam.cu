@@ -208,8 +208,9 @@ __global__ void __launch_bounds__(kMutThreads) mutate_kernel(const MutArgs A) {
 // --------------------------------------------------------------------------
 // Children's scores by exact deltas: warp per child, the parent's columns and
 // badness in shared memory, then each recorded swap applied with its exact dE
-// and the exact update of every badness (move_exact_t<true>, the tempering
-// move without the Metropolis test).  E and badness equal a full recount.
+// and the exact update of every badness (team_move<1, true>: the tempering
+// move by one warp, without the Metropolis test).  E and badness equal a full
+// recount.
 // --------------------------------------------------------------------------
 constexpr int kDeltaWarps = 22;
 constexpr size_t kDeltaSmem = kFullLutBytes + kDeltaWarps * (sizeof(uint32_t) * kDirWords + 2 * sizeof(int) * kMaxM);

@@ -237,24 +237,6 @@ __device__ __forceinline__ int team_move(Team<WPC>& tm, int* __restrict__ cs, in
   return 1;
 }
 
-// The move evaluated by one warp (lane = its lane index).
-template <bool FORCE, bool UMB = false, bool EARLY = false>
-__device__ __forceinline__ int move_exact_t(int* __restrict__ cs, int* __restrict__ bs, int m,
-                                            const uint16_t* __restrict__ lutf, uint32_t* __restrict__ hist, int lane,
-                                            int u, int v, uint32_t z, const uint32_t* __restrict__ thr, int W, int& E,
-                                            uint32_t& err, int* dE_out, int64_t umb_q = 0,
-                                            const uint32_t* __restrict__ frac = nullptr) {
-  Team<1> tm{lane, 0, nullptr, 0, {}};
-  return team_move<1, FORCE, UMB, EARLY>(tm, cs, bs, m, lutf, hist, u, v, z, thr, W, E, err, dE_out, umb_q, frac);
-}
-
-__device__ __forceinline__ int move_exact(int* __restrict__ cs, int* __restrict__ bs, int m,
-                                          const uint16_t* __restrict__ lutf, uint32_t* __restrict__ hist, int lane,
-                                          int u, int v, uint32_t z, const uint32_t* __restrict__ thr, int W, int& E,
-                                          uint32_t& err, int* dE_out) {
-  return move_exact_t<false>(cs, bs, m, lutf, hist, lane, u, v, z, thr, W, E, err, dE_out);
-}
-
 // Slot of a badness-weighted draw (tempering.py:52-54): the first slot whose
 // running badness sum exceeds `target` (target < 3E = the sum of all badness),
 // and at most m - 1.  Lane l sums slots 5l .. 5l + 4 (stride-5 shared-memory
